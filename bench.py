@@ -1,0 +1,368 @@
+#!/usr/bin/env python
+"""Benchmark of the compact-hashing neighbour search on B200.
+
+Workload (one step = one full search, structure build included): 1,048,576 float32 points
+uniform in [-1,1]^3 (torch.manual_seed(0)), non-periodic, per-point support
+h_i = h0*U(0.9,1.1) with h0 = cbrt(3*50*dx^3/(4*pi)), dx = 2/102 (about 50 neighbours),
+symmetric mode, CSR output -- 51,798,992 pairs per step.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
+
+Prints one JSON line.  `value` is pairs/s with inputs resident in HBM and L2 flushed (a 256 MiB
+write) between timed steps, timed with CUDA events on the launching stream (max over ranks
+under torchrun; every rank runs an independent replica, "replicas only").  `e2e` is the same
+metric through the public API with the inputs copied from pinned host memory and the whole
+CSR result copied back every step.  `roofline` covers the dominant kernel (the emitting
+candidate walk), `cpu_baseline` the reference's own CPU operators on this host.
+"""
+import argparse
+import json
+import os
+import re
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+REPO = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, REPO)
+
+METRIC = "neighbor pairs/s, 3D 1M pts; batched/served vs per-call; p50/p99 ms"
+WORKLOAD = "3d_1m_uniform_symmetric_csr"
+N_POINTS = 1 << 20
+L2_FLUSH_BYTES = 256 << 20
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=100)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    return ap.parse_args()
+
+
+def make_workload():
+    import numpy as np
+    import torch
+    torch.manual_seed(0)
+    pos = torch.rand(N_POINTS, 3) * 2 - 1
+    dx = 2 / 102
+    h0 = (3 * 50 * dx ** 3 / (4 * np.pi)) ** (1 / 3)
+    sup = h0 * (0.9 + 0.2 * torch.rand(N_POINTS))
+    return pos.contiguous(), sup.to(torch.float32).contiguous()
+
+
+def config(pairs):
+    return {"workload": WORKLOAD, "n_points": N_POINTS, "dim": 3, "mode": "symmetric", "format": "csr",
+            "periodic": [False, False, False], "hashMapLength": 4096, "pairs_per_step": pairs,
+            "l2": "flushed between timed steps (256 MiB device write)", "parallelism": "replicas"}
+
+
+def measured_peak():
+    p = os.path.join(REPO, "MEASURED_PEAKS.json")
+    try:
+        with open(p) as f:
+            return float(json.load(f)["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+def ncu_traffic():
+    """dram bytes per launch of the emitting walk from the committed ncu summary, if any."""
+    p = os.path.join(REPO, "profiles", "walk_emit_3d_1m.txt")
+    try:
+        with open(p) as f:
+            m = re.search(r"dram_bytes_per_launch_full_size:\s*([0-9.eE+]+)", f.read())
+        return float(m.group(1)) if m else None
+    except OSError:
+        return None
+
+
+class Clocks:
+    """nvidia-smi sampling during the timed region."""
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+         "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+         "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+        self.path = None
+
+    def start(self):
+        try:
+            fd, self.path = tempfile.mkstemp(suffix=".csv")
+            os.close(fd)
+            self.proc = subprocess.Popen(["nvidia-smi", f"--query-gpu={self.Q}", "--format=csv,noheader,nounits",
+                                          "-i", str(self.index), "-lms", "100"], stdout=open(self.path, "w"),
+                                         stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return None
+        time.sleep(0.15)
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        sm, smax, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        with open(self.path) as f:
+            for line in f:
+                parts = [p.strip() for p in line.split(",")]
+                if len(parts) < 9:
+                    continue
+                try:
+                    sm.append(float(parts[1]))
+                    smax.append(float(parts[2]))
+                except ValueError:
+                    continue
+                for n, v in zip(names, parts[5:9]):
+                    if v.lower() == "active":
+                        reasons.add(n)
+        os.unlink(self.path)
+        if not sm:
+            return None
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": max(smax), "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def cpu_baseline_reference(pos, sup, budget_s=25.0):
+    """The reference's own CPU operators (oracle/_ref) through its driver, on all host threads."""
+    import torch
+    from oracle import ref_pipeline
+    torch.set_num_threads(os.cpu_count() or 1)
+    cores = torch.get_num_threads()
+    lo, hi, per = [-1.0] * 3, [1.0] * 3, [False] * 3
+    t0 = time.perf_counter()
+    out = ref_pipeline.radius_search(pos, sup, None, None, lo, hi, per, "symmetric", 4096, "csr")
+    t1 = time.perf_counter()
+    pairs = int(out[0].numel())
+    reps = max(1, min(3, int(budget_s / max(t1 - t0, 1e-3)) - 1))
+    times = []
+    for _ in range(reps):
+        s = time.perf_counter()
+        ref_pipeline.radius_search(pos, sup, None, None, lo, hi, per, "symmetric", 4096, "csr")
+        times.append(time.perf_counter() - s)
+    t = statistics.median(times)
+    return {"value": pairs / t, "unit": "pairs/s", "cores": cores, "kind": "reference",
+            "sample": f"the full workload ({pairs} pairs), 1 warm-up + median of {reps} runs, "
+                      f"torch.set_num_threads({cores})", "seconds_per_search": t}, pairs
+
+
+def cpu_baseline_port(pos, sup, max_queries=131072):
+    """The C restatement (oracle/compact_oracle.c) on a query subset, OpenMP over host threads."""
+    from oracle import compact
+    q = pos[:max_queries].numpy()
+    hq = sup[:max_queries].numpy()
+    t0 = time.perf_counter()
+    r = compact.radius_search(q, hq, pos.numpy(), sup.numpy(), [-1] * 3, [1] * 3, [False] * 3, "symmetric", 4096)
+    t = time.perf_counter() - t0
+    return {"value": len(r.col) / t, "unit": "pairs/s", "cores": compact.num_threads(), "kind": "port",
+            "sample": f"first {max_queries} queries against all {pos.shape[0]} points, one run"}
+
+
+def run_reference(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return 0
+    import torch
+    from oracle import ref_pipeline
+    pos, sup = make_workload()
+    if not ref_pipeline.available():
+        print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref (the reference's CPU operators) is not "
+                                                               "built; run oracle/build_ref.py where the reference "
+                                                               "checkout exists"}))
+        return 0
+    torch.set_num_threads(os.cpu_count() or 1)
+    cores = torch.get_num_threads()
+    lo, hi, per = [-1.0] * 3, [1.0] * 3, [False] * 3
+    # size each step so that warm-up + steps stay within ~3 minutes
+    t0 = time.perf_counter()
+    out = ref_pipeline.radius_search(pos, sup, None, None, lo, hi, per, "symmetric", 4096, "csr")
+    full_t = time.perf_counter() - t0
+    full_pairs = int(out[0].numel())
+    total_steps = args.steps + args.warmup
+    frac = min(1.0, 170.0 / max(total_steps * full_t, 1e-9))
+    nq = max(1024, int(N_POINTS * frac)) if frac < 1.0 else N_POINTS
+    if nq >= N_POINTS:
+        q, hq, r, hr, sample = pos, sup, None, None, f"the full workload ({full_pairs} pairs) per step"
+    else:
+        q, hq, r, hr = pos[:nq], sup[:nq], pos, sup
+        sample = f"first {nq} queries against all {N_POINTS} points per step (time-bounded)"
+    for _ in range(args.warmup):
+        ref_pipeline.radius_search(q, hq, r, hr, lo, hi, per, "symmetric", 4096, "csr")
+    times, pairs = [], 0
+    for _ in range(args.steps):
+        s = time.perf_counter()
+        o = ref_pipeline.radius_search(q, hq, r, hr, lo, hi, per, "symmetric", 4096, "csr")
+        times.append(time.perf_counter() - s)
+        pairs = int(o[0].numel())
+    tot = sum(times)
+    value = pairs * len(times) / tot
+    line = {"metric": METRIC, "value": value, "unit": "pairs/s", "n_gpus": args.gpus, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": 1e3 * tot / len(times), "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic", "impl": "reference",
+            "config": config(pairs),
+            "p50_ms": 1e3 * statistics.median(times), "p99_ms": 1e3 * sorted(times)[min(len(times) - 1,
+                                                                                     int(0.99 * len(times)))],
+            "cpu_baseline": {"value": value, "unit": "pairs/s", "cores": cores, "kind": "reference",
+                             "sample": sample},
+            "e2e": {"value": value, "unit": "pairs/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line))
+    return 0
+
+
+def run_b200(args):
+    import torch
+    import torch.distributed as dist
+
+    import torchcompactradius_b200 as tcr
+    from torchcompactradius_b200 import _lib
+    from torchcompactradius_b200.search import compact_search
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    if world > 1:
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=120), device_id=dev)
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+
+    def max_over_ranks(v):
+        if world == 1:
+            return v
+        t = torch.tensor([v], dtype=torch.float64, device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    pos_h, sup_h = make_workload()
+    pos_pin, sup_pin = pos_h.pin_memory(), sup_h.pin_memory()
+    pos_d, sup_d = pos_h.to(dev), sup_h.to(dev)
+    dom = tcr.DomainDescription(torch.tensor([-1.0] * 3), torch.tensor([1.0] * 3), torch.tensor([False] * 3), 3)
+    lib = _lib.load()
+    flush = torch.empty(L2_FLUSH_BYTES, dtype=torch.uint8, device=dev)
+    stream = torch.cuda.current_stream(dev)
+
+    def device_step(events=None):
+        (col, indptr, entries), _ = compact_search(pos_d, sup_d, pos_d, sup_d, [-1.0] * 3, [1.0] * 3, 0,
+                                                   "symmetric", 4096, "csr", True, events=events)
+        return col, indptr, entries
+
+    for _ in range(args.warmup):
+        col, indptr, entries = device_step()
+    pairs = int(col.numel())
+    torch.cuda.synchronize()
+
+    # ---- device-resident timing -----------------------------------------------------------
+    clk = Clocks(local)
+    clk.start()
+    barrier()
+    torch.cuda.synchronize()
+    launches0 = lib.tcr_kernel_launches()
+    step_ms, emit_ms, count_ms, build_ms = [], [], [], []
+    for k in range(args.steps):
+        flush.fill_(k & 0xff)  # L2 flush outside the step's events
+        ev = {}
+        s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        s.record(stream)
+        device_step(ev)
+        e.record(stream)
+        e.synchronize()
+        step_ms.append(s.elapsed_time(e))
+        build_ms.append(ev["build"][0].elapsed_time(ev["build"][1]))
+        count_ms.append(ev["count"][0].elapsed_time(ev["count"][1]))
+        emit_ms.append(ev["emit"][0].elapsed_time(ev["emit"][1]))
+    torch.cuda.synchronize()
+    barrier()
+    launches = lib.tcr_kernel_launches() - launches0
+    clocks = clk.stop()
+    total_ms = max_over_ranks(sum(step_ms))
+    value = pairs * args.steps * world / (total_ms / 1e3)
+
+    # ---- end to end through the public API (pinned host in, host out) ----------------------
+    nq = N_POINTS
+    out_idx = torch.empty(pairs, dtype=torch.int64, pin_memory=True)
+    out_ptr = torch.empty(nq + 1, dtype=torch.int32, pin_memory=True)
+    out_ent = torch.empty(nq, dtype=torch.int64, pin_memory=True)
+    e2e_ms = []
+    barrier()
+    for k in range(max(3, min(args.steps, 30))):
+        flush.fill_(k & 0xff)
+        s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        s.record(stream)
+        p = pos_pin.to(dev, non_blocking=True)
+        h = sup_pin.to(dev, non_blocking=True)
+        adj = tcr.radiusSearch(tcr.PointCloud(p, h), mode="symmetric", domain=dom, hashMapLength=4096,
+                               algorithm="compact", format="csr")
+        out_idx.copy_(adj.indices, non_blocking=True)
+        out_ptr.copy_(adj.indptr, non_blocking=True)
+        out_ent.copy_(adj.rowEntries, non_blocking=True)
+        e.record(stream)
+        e.synchronize()
+        e2e_ms.append(s.elapsed_time(e))
+    barrier()
+    e2e_total = max_over_ranks(sum(e2e_ms))
+    e2e_value = pairs * len(e2e_ms) * world / (e2e_total / 1e3)
+    ok = torch.equal(out_ptr, indptr.cpu()) and int(out_ent.sum()) == pairs
+
+    # ---- roofline of the dominant kernel (the emitting walk) ------------------------------
+    peak, peak_kind = measured_peak()
+    emit_bytes = 16 * N_POINTS + 8 * pairs  # inputs read once (4d+4 B/pt) + int64 CSR indices
+    emit_s = statistics.mean(emit_ms) / 1e3
+    achieved = emit_bytes / emit_s / 1e9
+    search_bytes = 16 * N_POINTS + 8 * pairs + 4 * (N_POINTS + 1) + 8 * N_POINTS
+    traffic = ncu_traffic()
+    line = {
+        "metric": METRIC, "value": value, "unit": "pairs/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32", "data": "synthetic", "impl": "b200", "config": config(pairs),
+        "p50_ms": statistics.median(step_ms), "p99_ms": sorted(step_ms)[min(len(step_ms) - 1,
+                                                                         int(0.99 * len(step_ms)))],
+        "phases_ms": {"build": statistics.mean(build_ms), "count": statistics.mean(count_ms),
+                      "emit": statistics.mean(emit_ms)},
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                     "traffic": traffic, "kernel": "walk_kernel<3,false,true> + stray_kernel<true> (emit)",
+                     "algorithmic_bytes_per_launch": emit_bytes, "peak_kind": peak_kind,
+                     "search_frac": search_bytes / (statistics.mean(step_ms) / 1e3) / 1e9 / peak},
+        "e2e": {"value": e2e_value, "unit": "pairs/s", "h2d_bytes_per_step": 16 * N_POINTS,
+                "d2h_bytes_per_step": 8 * pairs + 4 * (N_POINTS + 1) + 8 * N_POINTS,
+                "ms_per_step": e2e_total / len(e2e_ms), "output_checked": bool(ok)},
+        "gpu_launches": int(launches),
+        "clocks": clocks,
+    }
+    if world > 1:
+        dist.destroy_process_group()
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        try:
+            cb, ref_pairs = cpu_baseline_reference(pos_h, sup_h)
+            cb["pairs_match"] = ref_pairs == pairs
+        except Exception as ex:  # the compiled reference is missing: time the C restatement instead
+            cb = cpu_baseline_port(pos_h, sup_h)
+            cb["note"] = f"reference operators unavailable: {ex}"
+        line["cpu_baseline"] = cb
+    if rank == 0:
+        print(json.dumps(line))
+    return 0
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        return run_reference(args)
+    return run_b200(args)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -1,0 +1,131 @@
+/*
+ * tcr_b200.h -- C ABI of the B200 (sm_100a) compact-hashing neighbour search.
+ *
+ * Plain pointers and sizes only: every array argument is a device pointer unless stated
+ * otherwise, every `stream` is a cudaStream_t passed as void*, and every function returns
+ * TCR_OK (0) or a negative TCR_ERR_* code with a message in tcr_last_error().  Nothing here
+ * allocates device memory: callers pass buffers of the sizes tcr_search_sizes() reports.
+ *
+ * The reference (wi-re/torchCompactRadius) exposes this path as torch operators registered in
+ * src/torchCompactRadius/cppSrc/cppWrapper.cpp:38-59 and driven from Python by
+ * compactHashing/cppSearch.py:12-98 (searchNeighbors_cpp) and :179-244 (neighborSearch_cpp).
+ * Each entry point below names the reference interface it replaces.
+ */
+#ifndef TCR_B200_H
+#define TCR_B200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define TCR_ABI_VERSION 1
+
+#define TCR_OK 0
+#define TCR_ERR_INVALID (-1) /* bad argument or workspace too small */
+#define TCR_ERR_CUDA (-2)    /* a CUDA call failed */
+
+/* Support modes (reference cppSrc/common.h:68-70 enum supportMode; thresholds
+ * neighborhoodDynamic.h:63-69): gather h_i, scatter h_j, symmetric (h_i+h_j)/2,
+ * superSymmetric max(h_i, h_j). */
+#define TCR_GATHER 0
+#define TCR_SCATTER 1
+#define TCR_SYMMETRIC 2
+#define TCR_SUPERSYMMETRIC 3
+
+/* One search.  Positions are row-major float32 [n, dim]; supports float32 [n].  The domain
+ * (DomainDescription, reference util.py:280-292) is given by value on the host. */
+typedef struct tcr_search_desc {
+    int32_t dim;             /* 1, 2 or 3 */
+    int32_t mode;            /* TCR_GATHER .. TCR_SUPERSYMMETRIC */
+    int32_t periodic_mask;   /* bit d set: dimension d is periodic */
+    int32_t self_search;     /* 1: the query cloud is the reference cloud (same positions) */
+    float domain_min[3];
+    float domain_max[3];
+    int64_t hash_map_length; /* the reference's hashMapLength; selects hash buckets exactly as
+                                cppSrc/neighborhood.h:73-96 does */
+    int64_t n_query;
+    int64_t n_ref;
+    const float* query_pos;  /* device [n_query*dim] */
+    const float* query_sup;  /* device [n_query]; may be NULL for TCR_SCATTER */
+    const float* ref_pos;    /* device [n_ref*dim] */
+    const float* ref_sup;    /* device [n_ref]; may be NULL for TCR_GATHER */
+} tcr_search_desc;
+
+/* Message of the last failing call on this thread. */
+const char* tcr_last_error(void);
+
+/* TCR_ABI_VERSION of the loaded library. */
+int tcr_version(void);
+
+/* sizeof(tcr_search_desc) as compiled into the library, for FFI layout checks. */
+int64_t tcr_desc_bytes(void);
+
+/* Total number of CUDA kernels this library has launched in this process (launch accounting
+ * for benchmarks; no reference counterpart). */
+int64_t tcr_kernel_launches(void);
+
+/* Byte sizes of the persistent structure (reference-side cell table and hash map, kept for
+ * reuse like the reference's CompactHashMap, compactHashing/datastructure.py:8-31) and of the
+ * per-search scratch.  Host-only; no device work. */
+int tcr_search_sizes(int64_t n_query, int64_t n_ref, int32_t dim, int64_t* structure_bytes,
+                     int64_t* scratch_bytes);
+
+/* Layout of the structure buffer, so a caller can view its parts (the fields of the reference's
+ * CompactHashMap, datastructure.py:8-31, are derived from them).  Host-only.  offsets[k] is the
+ * byte offset of field k (TCR_STRUCT_*), except offsets[TCR_STRUCT_MAP_CAPACITY], which is the
+ * number of 64-bit slots of the linear-index map.  Field contents:
+ *   GRID          float hmax, float hCell, int32 cellCount[3], int32 exact_only, int32 error, ...
+ *   NUM_CELLS     int32 number of occupied cells C
+ *   SORTED_POINTS float4 [n_ref] wrapped reference positions in cell order, .w = support
+ *   SORT_INDEX    int32 [n_ref] original index of each sorted point
+ *   CELL_START    int32 [C+1] first sorted point of each cell (cells in linear-index order)
+ *   CELL_LIN      int32 [C] linear cell index (cellTable.py:31)
+ *   CELL_COORDS   int32 [3*C] integer cell coordinates
+ *   CELL_BUCKET   int32 [C] reference hash of the coordinates mod hashMapLength
+ *   MAP           uint64 [cap] open-addressing map (lin << 32 | cell), empty = ~0 */
+#define TCR_STRUCT_GRID 0
+#define TCR_STRUCT_NUM_CELLS 1
+#define TCR_STRUCT_SORTED_POINTS 2
+#define TCR_STRUCT_SORT_INDEX 3
+#define TCR_STRUCT_CELL_START 4
+#define TCR_STRUCT_CELL_LIN 5
+#define TCR_STRUCT_CELL_COORDS 6
+#define TCR_STRUCT_CELL_BUCKET 7
+#define TCR_STRUCT_MAP 8
+#define TCR_STRUCT_MAP_CAPACITY 9
+#define TCR_STRUCT_NFIELDS 10
+int tcr_structure_offsets(int64_t n_ref, int64_t* offsets, int32_t n);
+
+/* Builds the search structure over the reference cloud: grid support (cellTable.py:40-81),
+ * cell size (util.py:28-79 compute_h), periodic wraps, sort by linear cell index, cell table
+ * and hash map.  Replaces buildCompactHashMap_compat (compactHashing/hashTable.py:159-234)
+ * together with the computeHashIndices operator (cppSrc/hashing.h:37-39, cppWrapper.cpp:45).
+ * The query supports of `d` enter the grid support for gather/symmetric modes, as in the
+ * reference. */
+int tcr_build_structure(const tcr_search_desc* d, void* structure, int64_t structure_bytes, void* scratch,
+                        int64_t scratch_bytes, void* stream);
+
+/* Counts the neighbours of every query and scans them.  Replaces the countNeighbors operator
+ * (cppSrc/neighborhood.h:140-146, cppWrapper.cpp:39) plus the cumsum of cppSearch.py:81-84.
+ * offsets: device int64 [n_query+1] (exclusive scan, offsets[n_query] = total pairs).
+ * indptr_out (device int32 [n_query+1]) and row_entries_out (device int64 [n_query]) are the
+ * SparseCSR fields of util.py:321-358 and may be NULL.  info_out (host, 4 x int64, may be
+ * NULL) receives {total pairs, grid error flag, queries walked serially, exact-only mode}
+ * asynchronously on `stream`. */
+int tcr_count(const tcr_search_desc* d, const void* structure, void* scratch, int64_t scratch_bytes,
+              int64_t* offsets, int32_t* indptr_out, int64_t* row_entries_out, int64_t* info_out, void* stream);
+
+/* Writes the neighbour pairs at the offsets of tcr_count (same scratch, same descriptor).
+ * Replaces the buildNeighborList operator (cppSrc/neighborhood.h:155-162, cppWrapper.cpp:40)
+ * and the j = sortIndex[j] unsort of cppSearch.py:97: col_out receives original reference
+ * indices, row_out (NULL for CSR) original query indices, both int64 [total]. */
+int tcr_emit(const tcr_search_desc* d, const void* structure, void* scratch, int64_t scratch_bytes,
+             const int64_t* offsets, int64_t* row_out, int64_t* col_out, void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* TCR_B200_H */

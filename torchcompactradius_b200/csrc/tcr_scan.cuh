@@ -1,0 +1,124 @@
+// tcr_scan.cuh -- device-wide exclusive prefix sums built from a block scan.
+//
+// Three launches: per-tile reduction, a single-CTA scan of the tile totals, and a per-tile scan
+// that adds the tile's prefix.  Input and output are functors so that producers (flags, counts)
+// and consumers (cell tables, offsets) fuse into the scan instead of round-tripping through HBM.
+#pragma once
+#include <cstdint>
+#include <cuda_runtime.h>
+
+#include "tcr_common.cuh"
+
+namespace tcr {
+
+constexpr int kScanThreads = 256;
+constexpr int kScanItems = 8;
+constexpr int kScanTile = kScanThreads * kScanItems;
+
+template <typename T>
+__device__ __forceinline__ T warp_inclusive_scan(T v) {
+    const unsigned lane = threadIdx.x & 31;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        T n = __shfl_up_sync(0xffffffffu, v, o);
+        if (lane >= (unsigned)o) v += n;
+    }
+    return v;
+}
+
+// Block-wide exclusive scan of one value per thread; returns the exclusive prefix and writes
+// the block total.  smem must hold NWARPS entries.
+template <typename T, int NTHREADS>
+__device__ __forceinline__ T block_exclusive_scan(T v, T* smem, T& total) {
+    constexpr int NW = NTHREADS / 32;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    T inc = warp_inclusive_scan(v);
+    if (lane == 31) smem[warp] = inc;
+    __syncthreads();
+    if (warp == 0) {
+        T s = lane < NW ? smem[lane] : T(0);
+        T si = warp_inclusive_scan(s);
+        if (lane < NW) smem[lane] = si - s;
+        if (lane == NW - 1) smem[NW] = si;
+    }
+    __syncthreads();
+    T excl = inc - v + smem[warp];
+    total = smem[NW];
+    __syncthreads();
+    return excl;
+}
+
+// Pass 1: tile totals.  In(i) returns the value of element i (0 for i >= n).
+template <typename T, typename In>
+__global__ void __launch_bounds__(kScanThreads) scan_reduce_kernel(In in, int64_t n, T* tile_sums) {
+    __shared__ T sm[kScanThreads / 32 + 1];
+    const int64_t base = (int64_t)blockIdx.x * kScanTile;
+    T s = 0;
+#pragma unroll
+    for (int k = 0; k < kScanItems; ++k) {
+        int64_t i = base + (int64_t)k * kScanThreads + threadIdx.x;
+        if (i < n) s += in(i);
+    }
+    T total;
+    block_exclusive_scan<T, kScanThreads>(s, sm, total);
+    if (threadIdx.x == 0) tile_sums[blockIdx.x] = total;
+}
+
+// Pass 2: one CTA scans the tile totals in place (exclusive) and stores the grand total.
+template <typename T>
+__global__ void __launch_bounds__(1024) scan_tiles_kernel(T* tile_sums, int64_t ntiles, T* grand_total) {
+    __shared__ T sm[1024 / 32 + 1];
+    T carry = 0;
+    for (int64_t b = 0; b < ntiles; b += 1024) {
+        int64_t i = b + threadIdx.x;
+        T v = i < ntiles ? tile_sums[i] : T(0);
+        T total;
+        T ex = block_exclusive_scan<T, 1024>(v, sm, total);
+        if (i < ntiles) tile_sums[i] = ex + carry;
+        carry += total;
+    }
+    if (threadIdx.x == 0 && grand_total) *grand_total = carry;
+}
+
+// Pass 3: per-tile exclusive scan; Out(i, exclusive_prefix, value) consumes each element.
+// Elements are processed in blocked order (thread t owns kScanItems consecutive elements).
+template <typename T, typename In, typename Out>
+__global__ void __launch_bounds__(kScanThreads) scan_apply_kernel(In in, Out out, int64_t n, const T* tile_sums) {
+    __shared__ T sm[kScanThreads / 32 + 1];
+    const int64_t base = (int64_t)blockIdx.x * kScanTile + (int64_t)threadIdx.x * kScanItems;
+    T v[kScanItems];
+    T s = 0;
+#pragma unroll
+    for (int k = 0; k < kScanItems; ++k) {
+        int64_t i = base + k;
+        v[k] = i < n ? in(i) : T(0);
+        s += v[k];
+    }
+    T total;
+    T ex = block_exclusive_scan<T, kScanThreads>(s, sm, total) + tile_sums[blockIdx.x];
+#pragma unroll
+    for (int k = 0; k < kScanItems; ++k) {
+        int64_t i = base + k;
+        if (i < n) out(i, ex, v[k]);
+        ex += v[k];
+    }
+}
+
+inline int64_t scan_tiles(int64_t n) { return (n + kScanTile - 1) / kScanTile; }
+
+// Host launcher.  tile_sums must hold scan_tiles(n) elements; grand_total may be null.
+template <typename T, typename In, typename Out>
+cudaError_t device_exclusive_scan(In in, Out out, int64_t n, T* tile_sums, T* grand_total, cudaStream_t st) {
+    int64_t nt = scan_tiles(n);
+    if (nt == 0) {
+        if (grand_total) return cudaMemsetAsync(grand_total, 0, sizeof(T), st);
+        return cudaSuccess;
+    }
+    scan_reduce_kernel<T><<<(unsigned)nt, kScanThreads, 0, st>>>(in, n, tile_sums);
+    scan_tiles_kernel<T><<<1, 1024, 0, st>>>(tile_sums, nt, grand_total);
+    scan_apply_kernel<T><<<(unsigned)nt, kScanThreads, 0, st>>>(in, out, n, tile_sums);
+    note_launches(3);
+    return cudaGetLastError();
+}
+
+}  // namespace tcr

@@ -1,0 +1,934 @@
+// tcr_search.cu -- compact-hashing fixed-radius neighbour search for sm_100a, with a C ABI.
+//
+// Pipeline (one CUDA stream, no host synchronisation inside a phase):
+//   build:  support max-reduction -> grid parameters (compute_h) -> wrap + pack reference points
+//           into float4 (x, y, z, h) and int32 linear cell keys -> stable radix sort ->
+//           run-length cell table (begin, coords, bucket) + open-addressing lin -> cell map.
+//   count:  query packing (self search reuses the reference order) -> query groups (cells) ->
+//           work units of <= 32 queries -> warp-per-unit candidate walk over the 3^d stencil with
+//           broadcast query positions and ballot counting -> device scan -> offsets.
+//   emit:   the same walk writing int64 (row, col) pairs at the scanned offsets.
+// The candidate set of every query is the reference's (cppSrc/neighborhood.h:73-132): the
+// stencil cells of its own cell, found by linear index inside the bucket of the stencil cell's
+// hash; the pair test is the reference's float test (tcr_common.cuh).
+#include <cstdio>
+#include <cstring>
+#include <cstdarg>
+#include <algorithm>
+
+#include "tcr_common.cuh"
+#include "tcr_scan.cuh"
+#include "tcr_sort.cuh"
+#include "../../include/tcr_b200.h"
+
+namespace tcr {
+
+// ------------------------------------------------------------------------------------------
+// error reporting
+static thread_local char g_err[512];
+static int set_error(int code, const char* fmt, ...) {
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(g_err, sizeof(g_err), fmt, ap);
+    va_end(ap);
+    return code;
+}
+#define TCR_CUDA(call)                                                                         \
+    do {                                                                                       \
+        cudaError_t e_ = (call);                                                               \
+        if (e_ != cudaSuccess)                                                                 \
+            return set_error(TCR_ERR_CUDA, "%s:%d %s", __FILE__, __LINE__, cudaGetErrorString(e_)); \
+    } while (0)
+
+// ------------------------------------------------------------------------------------------
+// workspace layout
+static inline int64_t align256(int64_t x) { return (x + 255) & ~int64_t(255); }
+static inline int64_t next_pow2(int64_t x) {
+    int64_t p = 1;
+    while (p < x) p <<= 1;
+    return p;
+}
+static inline int64_t hash_capacity(int64_t n_ref) { return std::max<int64_t>(1024, next_pow2(2 * std::max<int64_t>(n_ref, 1))); }
+
+struct Carve {
+    char* base;
+    int64_t off;
+    template <typename T>
+    T* take(int64_t count) {
+        T* p = base ? reinterpret_cast<T*>(base + off) : nullptr;
+        off += align256(count * (int64_t)sizeof(T));
+        return p;
+    }
+};
+
+// Persistent structure (reference side); kept alive for reuse.
+struct Structure {
+    GridParams* grid;       // [1]
+    float4* rsorted;        // [nr] wrapped reference points in cell order, .w = support
+    int32_t* rsidx;         // [nr] original index of each sorted point
+    int32_t* cell_start;    // [nr+1]
+    int32_t* cell_lin;      // [nr]
+    int32_t* cell_coords;   // [3*nr]
+    int32_t* cell_bucket;   // [nr] ref hash of the cell's coordinates mod hashMapLength
+    int32_t* num_cells;     // [1]
+    unsigned long long* map;  // [H] (lin << 32 | cell), empty = ~0
+    int64_t map_cap;
+};
+
+static Structure carve_structure(void* buf, int64_t nr, int64_t* bytes) {
+    Carve c{(char*)buf, 0};
+    Structure s;
+    s.grid = c.take<GridParams>(1);
+    s.num_cells = c.take<int32_t>(1);
+    s.rsorted = c.take<float4>(nr);
+    s.rsidx = c.take<int32_t>(nr);
+    s.cell_start = c.take<int32_t>(nr + 1);
+    s.cell_lin = c.take<int32_t>(nr);
+    s.cell_coords = c.take<int32_t>(3 * nr);
+    s.cell_bucket = c.take<int32_t>(nr);
+    s.map_cap = hash_capacity(nr);
+    s.map = c.take<unsigned long long>(s.map_cap);
+    if (bytes) *bytes = c.off;
+    return s;
+}
+
+// Per-search scratch.
+struct Scratch {
+    float4* pack;           // [max(nq,nr)] packed input points before sorting
+    SortWorkspace sort;
+    int64_t* scan_tiles64;  // [scan_tiles(max)]
+    int32_t* scan_tiles32;  // [scan_tiles(max)]
+    float4* qsorted;        // [nq]
+    int32_t* qsidx;         // [nq]
+    int32_t* qgroup_start;  // [nq+1]
+    int32_t* qgroup_coords; // [3*nq]
+    int32_t* num_qgroups;   // [1]
+    int32_t* unit_group;    // [nq]
+    int32_t* unit_t0;       // [nq]
+    int32_t* num_units;     // [1]
+    int32_t* counts;        // [nq]
+    int32_t* stray;         // [nq]
+    int32_t* num_stray;     // [1]
+    int32_t* work;          // [4] work counters
+    int64_t* total;         // [1]
+    int64_t* info;          // [4] total pairs, grid error, stray queries, exact-only mode
+};
+
+static Scratch carve_scratch(void* buf, int64_t nq, int64_t nr, int64_t* bytes) {
+    Carve c{(char*)buf, 0};
+    Scratch s;
+    int64_t nmax = std::max<int64_t>(std::max<int64_t>(nq, nr), 1);
+    s.sort.state = c.take<SortState>(1);
+    s.num_qgroups = c.take<int32_t>(1);
+    s.num_units = c.take<int32_t>(1);
+    s.num_stray = c.take<int32_t>(1);
+    s.work = c.take<int32_t>(4);
+    s.total = c.take<int64_t>(1);
+    s.info = c.take<int64_t>(4);
+    s.pack = c.take<float4>(nmax);
+    s.sort.keys[0] = c.take<uint32_t>(nmax);
+    s.sort.keys[1] = c.take<uint32_t>(nmax);
+    s.sort.vals[0] = c.take<int32_t>(nmax);
+    s.sort.vals[1] = c.take<int32_t>(nmax);
+    s.sort.hist = c.take<int32_t>(sort_hist_elems(nmax));
+    s.sort.tile_sums = c.take<int32_t>(scan_tiles(sort_hist_elems(nmax)));
+    s.scan_tiles64 = c.take<int64_t>(scan_tiles(nmax + 1));
+    s.scan_tiles32 = c.take<int32_t>(scan_tiles(nmax + 1));
+    int64_t q = std::max<int64_t>(nq, 1);
+    s.qsorted = c.take<float4>(q);
+    s.qsidx = c.take<int32_t>(q);
+    s.qgroup_start = c.take<int32_t>(q + 1);
+    s.qgroup_coords = c.take<int32_t>(3 * q);
+    s.unit_group = c.take<int32_t>(q);
+    s.unit_t0 = c.take<int32_t>(q);
+    s.counts = c.take<int32_t>(q);
+    s.stray = c.take<int32_t>(q);
+    if (bytes) *bytes = c.off;
+    return s;
+}
+
+// ------------------------------------------------------------------------------------------
+// build kernels
+
+
+// computeGridSupport (cellTable.py:40-81): max over the supports the mode uses; also tracks
+// min |h| and non-finite values for the exact-mode decision.
+__global__ void support_reduce_kernel(const float* a, int64_t na, const float* b, int64_t nb, GridParams* g) {
+    uint32_t kmax = 0, kmin = 0xffffffffu;
+    int nonfinite = 0;
+    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < na + nb; i += stride) {
+        float h = i < na ? a[i] : b[i - na];
+        kmax = max(kmax, float_key(h));
+        kmin = min(kmin, float_key(fabsf(h)));
+        nonfinite |= !isfinite(h);
+    }
+#pragma unroll
+    for (int o = 16; o; o >>= 1) {
+        kmax = max(kmax, __shfl_xor_sync(0xffffffffu, kmax, o));
+        kmin = min(kmin, __shfl_xor_sync(0xffffffffu, kmin, o));
+        nonfinite |= __shfl_xor_sync(0xffffffffu, nonfinite, o);
+    }
+    if ((threadIdx.x & 31) == 0) {
+        atomicMax(&g->hmax_key, kmax);
+        atomicMin(&g->hmin_abs_key, kmin);
+        if (nonfinite) atomicOr(&g->nonfinite, 1);
+    }
+}
+
+__global__ void sort_state_init_kernel(SortState* st) {
+    st->key_min = 0xffffffffu;
+    st->key_max = 0;
+    st->sel[0] = 0;
+}
+
+__global__ void grid_init_kernel(GridParams* g, SortState* st) {
+    g->hmax_key = 0;
+    g->hmin_abs_key = 0xffffffffu;
+    g->nonfinite = 0;
+    g->error = 0;
+    st->key_min = 0xffffffffu;
+    st->key_max = 0;
+    st->sel[0] = 0;
+}
+
+// util.py:28-79 compute_h and cellTable.py:27-29, float32 throughout.
+__global__ void grid_params_kernel(SearchParams sp, GridParams* g, SortState* st) {
+    const float grow = 1.00010001659393310546875f;  // fl32(1e-4 + 1)
+    float hmax = key_float(g->hmax_key);
+    float ext[3], nc[3], h[3];
+    bool any = false;
+    for (int d = 0; d < sp.dim; ++d) {
+        ext[d] = __fsub_rn(sp.dmax[d], sp.dmin[d]);
+        nc[d] = floorf(__fdiv_rn(ext[d], hmax));
+        h[d] = __fdiv_rn(ext[d], nc[d]);
+    }
+    for (int d = 0; d < sp.dim; ++d) any |= __fsub_rn(__fdiv_rn(ext[d], h[d]), nc[d]) > 0.0f;
+    if (any)
+        for (int d = 0; d < sp.dim; ++d) {
+            nc[d] = __fsub_rn(nc[d], 1.0f);
+            h[d] = __fdiv_rn(ext[d], nc[d]);
+        }
+    any = false;
+    for (int d = 0; d < sp.dim; ++d) {
+        float r = __fdiv_rn(ext[d], h[d]);
+        any |= ceilf(r) > r;
+    }
+    if (any)
+        for (int d = 0; d < sp.dim; ++d) h[d] = __fmul_rn(h[d], grow);
+    float hc = h[0];
+    for (int d = 1; d < sp.dim; ++d) {
+        float v = h[d];
+        if (hc != hc) break;
+        if (v != v || v > hc) hc = v;  // torch.max propagates NaN
+    }
+    g->hmax = hmax;
+    g->hcell = hc;
+    for (int d = 0; d < 3; ++d) g->count[d] = d < sp.dim ? (int32_t)ceilf(__fdiv_rn(ext[d], hc)) : 1;
+    float hmin_abs = key_float(g->hmin_abs_key);
+    g->always_exact = (g->nonfinite || !(hmin_abs >= 1e-18f) || !(fabsf(hmax) <= 1e18f)) ? 1 : 0;
+    int err = 0;
+    if (!(hc > 0.0f) || !isfinite(hc)) err = 1;  // no valid grid (support larger than the domain, NaN, ...)
+    for (int d = 0; d < sp.dim; ++d)
+        if (((sp.periodic_mask >> d) & 1) && g->count[d] <= 0) err = 1;
+    g->error = err;
+    if (err) st->key_min = st->key_max = 0;  // no radix pass runs on keys that were never written
+}
+
+__device__ __forceinline__ float4 load_point(const float* x, const float* h, int64_t i, int dim) {
+    float4 v = make_float4(0.f, 0.f, 0.f, h ? h[i] : 0.0f);
+    const float* p = x + i * dim;
+    v.x = p[0];
+    if (dim > 1) v.y = p[1];
+    if (dim > 2) v.z = p[2];
+    return v;
+}
+
+__device__ __forceinline__ float4 wrap_point(const SearchParams& sp, float4 v, int times) {
+    for (int d = 0; d < sp.dim; ++d)
+        if ((sp.periodic_mask >> d) & 1) {
+            float c = comp(v, d);
+            for (int t = 0; t < times; ++t) c = wrap_coord(c, sp.dmin[d], sp.ext[d]);
+            if (d == 0) v.x = c; else if (d == 1) v.y = c; else v.z = c;
+        }
+    return v;
+}
+
+__device__ __forceinline__ void point_cell(const SearchParams& sp, const GridParams* g, const float4& v, int32_t* c) {
+    const float hc = g->hcell;
+    c[0] = cell_coord(v.x, sp.dmin[0], hc);
+    c[1] = sp.dim > 1 ? cell_coord(v.y, sp.dmin[1], hc) : 0;
+    c[2] = sp.dim > 2 ? cell_coord(v.z, sp.dmin[2], hc) : 0;
+}
+
+// Wrap (twice for the reference cloud, cppSearch.py:221 after neighborhood.py:203; once for a
+// query cloud), pack to float4 and emit the signed-order linear key.
+__global__ void pack_points_kernel(SearchParams sp, const GridParams* g, const float* x, const float* h, int64_t n,
+                                   int wraps, float4* pack, uint32_t* keys, int32_t* vals, SortState* st) {
+    if (g->error) return;
+    uint32_t kmin = 0xffffffffu, kmax = 0;
+    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
+        float4 v = wrap_point(sp, load_point(x, h, i, sp.dim), wraps);
+        int32_t c[3];
+        point_cell(sp, g, v, c);
+        uint32_t key = (uint32_t)linear_index(sp.dim, c, g->count) ^ 0x80000000u;
+        pack[i] = v;
+        keys[i] = key;
+        vals[i] = (int32_t)i;
+        kmin = min(kmin, key);
+        kmax = max(kmax, key);
+    }
+#pragma unroll
+    for (int o = 16; o; o >>= 1) {
+        kmin = min(kmin, __shfl_xor_sync(0xffffffffu, kmin, o));
+        kmax = max(kmax, __shfl_xor_sync(0xffffffffu, kmax, o));
+    }
+    if ((threadIdx.x & 31) == 0) {
+        atomicMin(&st->key_min, kmin);
+        atomicMax(&st->key_max, kmax);
+    }
+}
+
+__device__ __forceinline__ uint32_t mix32(uint32_t x) {
+    x ^= x >> 16;
+    x *= 0x85ebca6bu;
+    x ^= x >> 13;
+    x *= 0xc2b2ae35u;
+    x ^= x >> 16;
+    return x;
+}
+
+__device__ __forceinline__ void map_insert(unsigned long long* map, int64_t cap, int32_t lin, int32_t cell) {
+    const unsigned long long entry = ((unsigned long long)(uint32_t)lin << 32) | (uint32_t)cell;
+    uint64_t slot = mix32((uint32_t)lin) & (cap - 1);
+    for (int64_t probe = 0; probe < cap; ++probe) {
+        unsigned long long prev = atomicCAS(&map[slot], ~0ull, entry);
+        if (prev == ~0ull || (uint32_t)(prev >> 32) == (uint32_t)lin) return;
+        slot = (slot + 1) & (cap - 1);
+    }
+}
+
+__device__ __forceinline__ int32_t map_find(const unsigned long long* __restrict__ map, int64_t cap, int32_t lin) {
+    uint64_t slot = mix32((uint32_t)lin) & (cap - 1);
+    for (int64_t probe = 0; probe < cap; ++probe) {
+        unsigned long long e = __ldg(&map[slot]);
+        if (e == ~0ull) return -1;
+        if ((uint32_t)(e >> 32) == (uint32_t)lin) return (int32_t)(uint32_t)e;
+        slot = (slot + 1) & (cap - 1);
+    }
+    return -1;
+}
+
+// Gathers sorted points and flags run starts (unique_consecutive, hashTable.py:193).
+struct RunFlagIn {
+    const GridParams* g;
+    const uint32_t* keys0;
+    const uint32_t* keys1;
+    const SortState* st;
+    __device__ int32_t operator()(int64_t i) const {
+        if (g->error) return 0;
+        const uint32_t* k = st->sel[4] ? keys1 : keys0;
+        return (i == 0 || k[i] != k[i - 1]) ? 1 : 0;
+    }
+};
+
+// Writes one cell record per run start: begin, lin, coords of the run's first point, bucket.
+struct CellOut {
+    SearchParams sp;
+    const GridParams* g;
+    const uint32_t* keys0;
+    const uint32_t* keys1;
+    const SortState* st;
+    const float4* rsorted;
+    int32_t* cell_start;
+    int32_t* cell_lin;
+    int32_t* cell_coords;
+    int32_t* cell_bucket;
+    unsigned long long* map;
+    int64_t map_cap;
+    __device__ void operator()(int64_t i, int32_t ex, int32_t flag) const {
+        if (!flag) return;
+        const uint32_t* k = st->sel[4] ? keys1 : keys0;
+        const int32_t cell = ex;
+        const int32_t lin = (int32_t)(k[i] ^ 0x80000000u);
+        int32_t c[3];
+        point_cell(sp, g, rsorted[i], c);
+        cell_start[cell] = (int32_t)i;
+        cell_lin[cell] = lin;
+        cell_coords[3 * cell + 0] = c[0];
+        cell_coords[3 * cell + 1] = c[1];
+        cell_coords[3 * cell + 2] = c[2];
+        cell_bucket[cell] = (int32_t)ref_hash(sp.dim, c, sp.hash_len);
+        map_insert(map, map_cap, lin, cell);
+    }
+};
+
+__global__ void gather_sorted_kernel(const GridParams* g, const float4* pack, const int32_t* vals0,
+                                     const int32_t* vals1, const SortState* st, int64_t n, float4* sorted,
+                                     int32_t* sidx) {
+    if (g->error) return;
+    const int32_t* v = st->sel[4] ? vals1 : vals0;
+    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
+        int32_t p = v[i];
+        sorted[i] = pack[p];
+        sidx[i] = p;
+    }
+}
+
+__global__ void finish_cells_kernel(int32_t* cell_start, const int32_t* num_cells, int64_t n) {
+    cell_start[*num_cells] = (int32_t)n;
+}
+
+// ------------------------------------------------------------------------------------------
+// query side
+
+// Self search: query i is reference i, so the reference order and cells group the queries.
+// Positions are the once-wrapped query coordinates (only periodic dims differ from rsorted).
+__global__ void pack_self_queries_kernel(SearchParams sp, const GridParams* g, const float* x, const float* h,
+                                         const int32_t* rsidx, int64_t n, float4* qsorted, int32_t* qsidx) {
+    if (g->error) return;
+    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < n; t += stride) {
+        int32_t i = rsidx[t];
+        qsorted[t] = wrap_point(sp, load_point(x, h, i, sp.dim), 1);
+        qsidx[t] = i;
+    }
+}
+
+struct QueryGroupOut {
+    SearchParams sp;
+    const GridParams* g;
+    const float4* qsorted;
+    int32_t* group_start;
+    int32_t* group_coords;
+    __device__ void operator()(int64_t i, int32_t ex, int32_t flag) const {
+        if (!flag) return;
+        int32_t c[3];
+        point_cell(sp, g, qsorted[i], c);
+        group_start[ex] = (int32_t)i;
+        group_coords[3 * ex + 0] = c[0];
+        group_coords[3 * ex + 1] = c[1];
+        group_coords[3 * ex + 2] = c[2];
+    }
+};
+
+constexpr int kUnit = 32;  // queries per work unit (one warp)
+
+// Group count comes from a device scalar; the scan kernels are launched over the upper bound
+// and read the true count through the functor.
+struct BoundedUnitCountIn {
+    const int32_t* group_start;
+    const int32_t* num_groups;
+    __device__ int32_t operator()(int64_t g) const {
+        if (g >= *num_groups) return 0;
+        int32_t n = group_start[g + 1] - group_start[g];
+        return (n + kUnit - 1) / kUnit;
+    }
+};
+struct BoundedUnitOut {
+    const int32_t* group_start;
+    const int32_t* num_groups;
+    int32_t* unit_group;
+    int32_t* unit_t0;
+    __device__ void operator()(int64_t g, int32_t ex, int32_t nunits) const {
+        if (g >= *num_groups) return;
+        int32_t s = group_start[g];
+        for (int32_t u = 0; u < nunits; ++u) {
+            unit_group[ex + u] = (int32_t)g;
+            unit_t0[ex + u] = s + u * kUnit;
+        }
+    }
+};
+
+// ------------------------------------------------------------------------------------------
+// the candidate walk
+
+struct WalkArgs {
+    SearchParams sp;
+    const GridParams* g;
+    const float4* __restrict__ rsorted;
+    const int32_t* __restrict__ rsidx;
+    const int32_t* __restrict__ cell_start;
+    const int32_t* __restrict__ cell_coords;
+    const int32_t* __restrict__ cell_bucket;
+    const unsigned long long* __restrict__ map;
+    int64_t map_cap;
+    const float4* __restrict__ qsorted;
+    const int32_t* __restrict__ qsidx;
+    const int32_t* __restrict__ group_start;
+    const int32_t* __restrict__ group_coords;
+    const int32_t* __restrict__ unit_group;
+    const int32_t* __restrict__ unit_t0;
+    const int32_t* __restrict__ num_units;
+    int32_t* work;
+    int32_t* stray;
+    int32_t* num_stray;
+    int32_t* counts;             // count pass output [nq] (original query order)
+    const int64_t* offsets;      // emit pass input [nq+1]
+    int64_t* row_out;            // emit: COO rows or null
+    int64_t* col_out;            // emit: columns
+};
+
+// Looks up stencil cell `o` (getOffsets order, last coordinate fastest) around cell gc with the
+// reference's semantics; returns the sorted range or an empty one.
+__device__ __forceinline__ void stencil_lookup(const WalkArgs& a, const int32_t* gc, int o, int32_t& beg,
+                                               int32_t& cnt) {
+    const SearchParams& sp = a.sp;
+    int32_t c[3] = {0, 0, 0};
+    int rem = o;
+    for (int d = sp.dim - 1; d >= 0; --d) {
+        int32_t off = rem % 3 - 1;
+        rem /= 3;
+        int32_t v = gc[d] + off;
+        if ((sp.periodic_mask >> d) & 1) v = pymod(v, a.g->count[d]);
+        c[d] = v;
+    }
+    beg = 0;
+    cnt = 0;
+    int32_t lin = linear_index(sp.dim, c, a.g->count);
+    int32_t cell = map_find(a.map, a.map_cap, lin);
+    if (cell < 0) return;
+    // queryHashMap matches the linear index inside bucket hash(c) only.
+    if ((uint32_t)__ldg(&a.cell_bucket[cell]) != ref_hash(sp.dim, c, sp.hash_len)) return;
+    beg = __ldg(&a.cell_start[cell]);
+    cnt = __ldg(&a.cell_start[cell + 1]) - beg;
+}
+
+template <int DIM>
+__device__ __forceinline__ bool same_cell(const int32_t* a, const int32_t* b) {
+    bool s = a[0] == b[0];
+    if (DIM > 1) s &= a[1] == b[1];
+    if (DIM > 2) s &= a[2] == b[2];
+    return s;
+}
+
+constexpr int kWalkWarps = 8;
+
+template <int DIM, bool PERIODIC, bool EMIT>
+__global__ void __launch_bounds__(kWalkWarps * 32) walk_kernel(WalkArgs a) {
+    if (a.g->error) return;
+    __shared__ int32_t s_pre[kWalkWarps][33];
+    __shared__ int32_t s_beg[kWalkWarps][32];
+    __shared__ float4 s_q[kWalkWarps][32];
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    const unsigned lt = (1u << lane) - 1u;
+    const int S = DIM == 1 ? 3 : (DIM == 2 ? 9 : 27);
+    const bool exact_all = a.g->always_exact != 0;
+    const int mode = a.sp.mode;
+    const ExactCtx xc = exact_ctx(a.sp);
+    const int32_t nunits = *a.num_units;
+    for (;;) {
+        int32_t unit = 0;
+        if (lane == 0) unit = atomicAdd(&a.work[EMIT ? 1 : 0], 1);
+        unit = __shfl_sync(0xffffffffu, unit, 0);
+        if (unit >= nunits) break;
+        const int32_t grp = a.unit_group[unit];
+        const int32_t t0 = a.unit_t0[unit];
+        const int32_t nb = min(kUnit, a.group_start[grp + 1] - t0);
+        int32_t gc[3] = {a.group_coords[3 * grp], a.group_coords[3 * grp + 1], a.group_coords[3 * grp + 2]};
+        // stencil lookups, one lane per stencil cell
+        int32_t beg = 0, cnt = 0;
+        if (lane < S) stencil_lookup(a, gc, lane, beg, cnt);
+        int32_t inc = warp_inclusive_scan(cnt);
+        s_pre[w][lane + 1] = inc;
+        if (lane == 0) s_pre[w][0] = 0;
+        s_beg[w][lane] = beg;
+        const int32_t M = __shfl_sync(0xffffffffu, inc, 31);
+        // queries of this unit
+        bool active = false;
+        int32_t qorig = 0;
+        float4 qv = make_float4(__int_as_float(0x7fc00000), 0.f, 0.f, 0.f);
+        if (lane < nb) {
+            const int32_t t = t0 + lane;
+            qv = a.qsorted[t];
+            qorig = a.qsidx[t];
+            int32_t qc[3];
+            point_cell(a.sp, a.g, qv, qc);
+            active = same_cell<DIM>(qc, gc);
+            if (!active && !EMIT) {  // own cell differs from the group's (aliasing or wrap rounding): serial path
+                int32_t k = atomicAdd(a.num_stray, 1);
+                a.stray[k] = t;
+            }
+        }
+        s_q[w][lane] = qv;
+        const unsigned amask = __ballot_sync(0xffffffffu, active);
+        int64_t obase = 0;
+        if (EMIT && active) obase = a.offsets[qorig];
+        int32_t qcount = 0;
+        __syncwarp();
+        for (int32_t base = 0; base < M; base += 32) {
+            const int32_t k = base + lane;
+            const bool valid = k < M;
+            float4 cv = make_float4(__int_as_float(0x7fc00000), 0.f, 0.f, 0.f);
+            int32_t j = 0;
+            if (valid) {
+                // stencil cell holding candidate k: last r with pre[r] <= k
+                int lo = 0, hi = S;  // pre[lo] <= k < pre[hi]
+                while (hi - lo > 1) {
+                    int mid = (lo + hi) >> 1;
+                    if (s_pre[w][mid] <= k) lo = mid; else hi = mid;
+                }
+                j = s_beg[w][lo] + (k - s_pre[w][lo]);
+                cv = __ldg(&a.rsorted[j]);
+            }
+            unsigned todo = amask;
+            while (todo) {
+                const int qi = __ffs(todo) - 1;
+                todo &= todo - 1;
+                const float4 q = s_q[w][qi];
+                const float thr = mode_threshold(mode, q.w, cv.w);
+                bool in, unc;
+                fast_pair_test<DIM, PERIODIC>(a.sp, q, thr, cv, in, unc);
+                unc = (unc || exact_all) && valid;
+                if (__any_sync(0xffffffffu, unc)) {
+                    if (unc) in = exact_pair_test(xc, q, q.w, cv, cv.w);
+                }
+                in = in && valid;
+                const unsigned b = __ballot_sync(0xffffffffu, in);
+                if (EMIT) {
+                    const int64_t qb = __shfl_sync(0xffffffffu, obase, qi);
+                    const int32_t qrow = __shfl_sync(0xffffffffu, qorig, qi);
+                    if (in) {
+                        const int64_t pos = qb + __popc(b & lt);
+                        a.col_out[pos] = (int64_t)__ldg(&a.rsidx[j]);
+                        if (a.row_out) a.row_out[pos] = (int64_t)qrow;
+                    }
+                    if (lane == qi) obase += __popc(b);
+                } else {
+                    if (lane == qi) qcount += __popc(b);
+                }
+            }
+        }
+        if (!EMIT && active) a.counts[qorig] = qcount;
+        __syncwarp();
+    }
+}
+
+// Serial walk for queries whose own cell differs from their group's (one thread per query).
+template <bool EMIT>
+__global__ void stray_kernel(WalkArgs a) {
+    if (a.g->error) return;
+    const int32_t ns = *a.num_stray;
+    const int S = a.sp.dim == 1 ? 3 : (a.sp.dim == 2 ? 9 : 27);
+    const ExactCtx xc = exact_ctx(a.sp);
+    for (int32_t s = blockIdx.x * blockDim.x + threadIdx.x; s < ns; s += gridDim.x * blockDim.x) {
+        const int32_t t = a.stray[s];
+        const float4 q = a.qsorted[t];
+        const int32_t qorig = a.qsidx[t];
+        int32_t qc[3];
+        point_cell(a.sp, a.g, q, qc);
+        int64_t pos = EMIT ? a.offsets[qorig] : 0;
+        int32_t n = 0;
+        for (int o = 0; o < S; ++o) {
+            int32_t beg, cnt;
+            stencil_lookup(a, qc, o, beg, cnt);
+            for (int32_t j = beg; j < beg + cnt; ++j) {
+                const float4 cv = a.rsorted[j];
+                if (exact_pair_test(xc, q, q.w, cv, cv.w)) {
+                    if (EMIT) {
+                        a.col_out[pos] = (int64_t)a.rsidx[j];
+                        if (a.row_out) a.row_out[pos] = qorig;
+                        ++pos;
+                    } else {
+                        ++n;
+                    }
+                }
+            }
+        }
+        if (!EMIT) a.counts[qorig] = n;
+    }
+}
+
+// counts -> offsets (int64, nq+1), optional CSR indptr (int32) and rowEntries (int64).
+struct CountIn {
+    const int32_t* counts;
+    int64_t n;
+    __device__ int64_t operator()(int64_t i) const { return i < n ? (int64_t)counts[i] : 0; }
+};
+struct OffsetOut {
+    int64_t n;
+    int64_t* offsets;
+    int32_t* indptr;
+    int64_t* entries;
+    __device__ void operator()(int64_t i, int64_t ex, int64_t v) const {
+        offsets[i] = ex;
+        if (indptr) indptr[i] = (int32_t)ex;
+        if (entries && i < n) entries[i] = v;
+    }
+};
+
+__global__ void info_kernel(const GridParams* g, const int64_t* total, const int32_t* num_stray, int64_t* info) {
+    info[0] = *total;
+    info[1] = g->error;
+    info[2] = *num_stray;
+    info[3] = g->always_exact;
+}
+
+// ------------------------------------------------------------------------------------------
+// host orchestration
+
+static SearchParams make_params(const tcr_search_desc* d) {
+    SearchParams sp;
+    memset(&sp, 0, sizeof(sp));
+    sp.dim = d->dim;
+    sp.mode = d->mode;
+    sp.periodic_mask = d->periodic_mask;
+    sp.hash_len = (uint32_t)d->hash_map_length;
+    for (int k = 0; k < 3; ++k) {
+        sp.dmin[k] = k < d->dim ? d->domain_min[k] : 0.f;
+        sp.dmax[k] = k < d->dim ? d->domain_max[k] : 1.f;
+        sp.ext[k] = sp.dmax[k] - sp.dmin[k];
+    }
+    sp.n_query = d->n_query;
+    sp.n_ref = d->n_ref;
+    return sp;
+}
+
+// need_ref_sup: the structure build reads reference supports; the query phases take them from
+// the structure and only need the query supports.
+static int validate(const tcr_search_desc* d, bool need_ref_sup = true) {
+    if (!d) return set_error(TCR_ERR_INVALID, "null descriptor");
+    if (d->dim < 1 || d->dim > 3) return set_error(TCR_ERR_INVALID, "dim must be 1, 2 or 3 (got %d)", d->dim);
+    if (d->mode < 0 || d->mode > 3) return set_error(TCR_ERR_INVALID, "invalid mode %d", d->mode);
+    if (d->hash_map_length <= 0 || d->hash_map_length > 0xffffffffLL)
+        return set_error(TCR_ERR_INVALID, "hashMapLength must be in [1, 2^32)");
+    if (d->n_query < 0 || d->n_ref < 0 || d->n_query > 0x7fffffffLL || d->n_ref > 0x7ffffff0LL)
+        return set_error(TCR_ERR_INVALID, "point counts must be in [0, 2^31)");
+    if ((d->n_query && !d->query_pos) || (d->n_ref && !d->ref_pos))
+        return set_error(TCR_ERR_INVALID, "missing positions");
+    if ((d->mode == kGather || d->mode == kSymmetric || d->mode == kSuperSymmetric) && d->n_query && !d->query_sup)
+        return set_error(TCR_ERR_INVALID, "this mode needs query supports");
+    if (need_ref_sup && (d->mode == kScatter || d->mode == kSymmetric || d->mode == kSuperSymmetric) && d->n_ref &&
+        !d->ref_sup)
+        return set_error(TCR_ERR_INVALID, "this mode needs reference supports");
+    if (d->self_search && d->n_query != d->n_ref)
+        return set_error(TCR_ERR_INVALID, "self search needs one cloud");
+    return TCR_OK;
+}
+
+static inline unsigned grid_for(int64_t n, int threads, int max_blocks = 148 * 16) {
+    int64_t b = (n + threads - 1) / threads;
+    return (unsigned)std::max<int64_t>(1, std::min<int64_t>(b, max_blocks));
+}
+
+static WalkArgs make_walk(const SearchParams& sp, const Structure& S, const Scratch& W, bool self) {
+    WalkArgs a;
+    memset(&a, 0, sizeof(a));
+    a.sp = sp;
+    a.g = S.grid;
+    a.rsorted = S.rsorted;
+    a.rsidx = S.rsidx;
+    a.cell_start = S.cell_start;
+    a.cell_coords = S.cell_coords;
+    a.cell_bucket = S.cell_bucket;
+    a.map = S.map;
+    a.map_cap = S.map_cap;
+    a.qsorted = W.qsorted;
+    a.qsidx = W.qsidx;
+    a.group_start = self ? S.cell_start : W.qgroup_start;
+    a.group_coords = self ? S.cell_coords : W.qgroup_coords;
+    a.unit_group = W.unit_group;
+    a.unit_t0 = W.unit_t0;
+    a.num_units = W.num_units;
+    a.work = W.work;
+    a.stray = W.stray;
+    a.num_stray = W.num_stray;
+    a.counts = W.counts;
+    return a;
+}
+
+template <bool EMIT>
+static cudaError_t launch_walk(const WalkArgs& a, int dim, bool periodic, int64_t nq, cudaStream_t st) {
+    int dev = 0, nsm = 148;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+    const int64_t max_units = (nq + kUnit - 1) / kUnit + 1;
+    unsigned blocks = (unsigned)std::max<int64_t>(1, std::min<int64_t>((int64_t)nsm * 8, (max_units + kWalkWarps - 1) / kWalkWarps));
+    dim3 grid(blocks), block(kWalkWarps * 32);
+#define TCR_WALK(D, P) walk_kernel<D, P, EMIT><<<grid, block, 0, st>>>(a)
+    if (dim == 1) { if (periodic) TCR_WALK(1, true); else TCR_WALK(1, false); }
+    else if (dim == 2) { if (periodic) TCR_WALK(2, true); else TCR_WALK(2, false); }
+    else { if (periodic) TCR_WALK(3, true); else TCR_WALK(3, false); }
+#undef TCR_WALK
+    note_launches(1);
+    stray_kernel<EMIT><<<grid_for(nq, 128, nsm * 4), 128, 0, st>>>(a);
+    note_launches(1);
+    return cudaGetLastError();
+}
+
+}  // namespace tcr
+
+using namespace tcr;
+
+extern "C" {
+
+const char* tcr_last_error(void) { return g_err; }
+
+int tcr_version(void) { return TCR_ABI_VERSION; }
+
+int64_t tcr_desc_bytes(void) { return (int64_t)sizeof(tcr_search_desc); }
+
+int64_t tcr_kernel_launches(void) { return (int64_t)__atomic_load_n(&g_launches, __ATOMIC_RELAXED); }
+
+int tcr_search_sizes(int64_t n_query, int64_t n_ref, int32_t dim, int64_t* structure_bytes, int64_t* scratch_bytes) {
+    if (dim < 1 || dim > 3 || n_query < 0 || n_ref < 0) return set_error(TCR_ERR_INVALID, "invalid sizes");
+    if (structure_bytes) carve_structure(nullptr, n_ref, structure_bytes);
+    if (scratch_bytes) carve_scratch(nullptr, n_query, n_ref, scratch_bytes);
+    return TCR_OK;
+}
+
+int tcr_structure_offsets(int64_t n_ref, int64_t* offsets, int32_t n) {
+    if (n_ref < 0 || !offsets || n < TCR_STRUCT_NFIELDS) return set_error(TCR_ERR_INVALID, "invalid arguments");
+    char* const base = reinterpret_cast<char*>(256);  // any non-null base; offsets are relative
+    Structure s = carve_structure(base, n_ref, nullptr);
+    auto off = [&](const void* p) { return (int64_t)((const char*)p - base); };
+    offsets[TCR_STRUCT_GRID] = off(s.grid);
+    offsets[TCR_STRUCT_NUM_CELLS] = off(s.num_cells);
+    offsets[TCR_STRUCT_SORTED_POINTS] = off(s.rsorted);
+    offsets[TCR_STRUCT_SORT_INDEX] = off(s.rsidx);
+    offsets[TCR_STRUCT_CELL_START] = off(s.cell_start);
+    offsets[TCR_STRUCT_CELL_LIN] = off(s.cell_lin);
+    offsets[TCR_STRUCT_CELL_COORDS] = off(s.cell_coords);
+    offsets[TCR_STRUCT_CELL_BUCKET] = off(s.cell_bucket);
+    offsets[TCR_STRUCT_MAP] = off(s.map);
+    offsets[TCR_STRUCT_MAP_CAPACITY] = s.map_cap;
+    return TCR_OK;
+}
+
+int tcr_build_structure(const tcr_search_desc* d, void* structure, int64_t structure_bytes, void* scratch,
+                        int64_t scratch_bytes, void* stream) {
+    int rc = validate(d);
+    if (rc) return rc;
+    int64_t need_s = 0, need_w = 0;
+    carve_structure(nullptr, d->n_ref, &need_s);
+    carve_scratch(nullptr, d->n_query, d->n_ref, &need_w);
+    if (!structure || !scratch || structure_bytes < need_s || scratch_bytes < need_w)
+        return set_error(TCR_ERR_INVALID, "workspace too small (structure %lld/%lld, scratch %lld/%lld)",
+                         (long long)structure_bytes, (long long)need_s, (long long)scratch_bytes, (long long)need_w);
+    cudaStream_t st = (cudaStream_t)stream;
+    const SearchParams sp = make_params(d);
+    Structure S = carve_structure(structure, d->n_ref, nullptr);
+    Scratch W = carve_scratch(scratch, d->n_query, d->n_ref, nullptr);
+    const int64_t nr = d->n_ref, nq = d->n_query;
+    grid_init_kernel<<<1, 1, 0, st>>>(S.grid, W.sort.state);
+    note_launches(1);
+    // computeGridSupport: which supports set hMax depends on the mode
+    const float* sa = nullptr; int64_t na = 0;
+    const float* sb = nullptr; int64_t nb = 0;
+    if (d->mode == kScatter) { sa = d->ref_sup; na = nr; }
+    else if (d->mode == kGather) { sa = d->query_sup; na = nq; }
+    else { sa = d->ref_sup; na = nr; sb = d->query_sup; nb = nq; }
+    if (na + nb > 0) support_reduce_kernel<<<grid_for(na + nb, 256), 256, 0, st>>>(sa, na, sb, nb, S.grid);
+    note_launches(1);
+    grid_params_kernel<<<1, 1, 0, st>>>(sp, S.grid, W.sort.state);
+    note_launches(1);
+    TCR_CUDA(cudaMemsetAsync(S.map, 0xff, sizeof(unsigned long long) * S.map_cap, st));
+    TCR_CUDA(cudaMemsetAsync(S.num_cells, 0, sizeof(int32_t), st));
+    if (nr > 0) {
+        pack_points_kernel<<<grid_for(nr, 256), 256, 0, st>>>(sp, S.grid, d->ref_pos, d->ref_sup, nr, 2, W.pack,
+                                                              W.sort.keys[0], W.sort.vals[0], W.sort.state);
+        note_launches(1);
+        TCR_CUDA(radix_sort_pairs(W.sort, nr, st));
+        gather_sorted_kernel<<<grid_for(nr, 256), 256, 0, st>>>(S.grid, W.pack, W.sort.vals[0], W.sort.vals[1], W.sort.state,
+                                                                nr, S.rsorted, S.rsidx);
+        note_launches(1);
+        CellOut co{sp, S.grid, W.sort.keys[0], W.sort.keys[1], W.sort.state, S.rsorted, S.cell_start, S.cell_lin,
+                   S.cell_coords, S.cell_bucket, S.map, S.map_cap};
+        RunFlagIn fi{S.grid, W.sort.keys[0], W.sort.keys[1], W.sort.state};
+        TCR_CUDA(device_exclusive_scan<int32_t>(fi, co, nr, W.scan_tiles32, S.num_cells, st));
+    }
+    finish_cells_kernel<<<1, 1, 0, st>>>(S.cell_start, S.num_cells, nr);
+    note_launches(1);
+    TCR_CUDA(cudaGetLastError());
+    return TCR_OK;
+}
+
+int tcr_count(const tcr_search_desc* d, const void* structure, void* scratch, int64_t scratch_bytes,
+              int64_t* offsets, int32_t* indptr_out, int64_t* row_entries_out, int64_t* info_out, void* stream) {
+    int rc = validate(d, false);
+    if (rc) return rc;
+    int64_t need_w = 0;
+    carve_scratch(nullptr, d->n_query, d->n_ref, &need_w);
+    if (!structure || !scratch || scratch_bytes < need_w || !offsets)
+        return set_error(TCR_ERR_INVALID, "workspace too small or offsets missing");
+    cudaStream_t st = (cudaStream_t)stream;
+    const SearchParams sp = make_params(d);
+    Structure S = carve_structure(const_cast<void*>(structure), d->n_ref, nullptr);
+    Scratch W = carve_scratch(scratch, d->n_query, d->n_ref, nullptr);
+    const int64_t nq = d->n_query;
+    const bool self = d->self_search != 0;
+    TCR_CUDA(cudaMemsetAsync(W.work, 0, sizeof(int32_t) * 4, st));
+    TCR_CUDA(cudaMemsetAsync(W.num_stray, 0, sizeof(int32_t), st));
+    TCR_CUDA(cudaMemsetAsync(W.num_units, 0, sizeof(int32_t), st));
+    if (nq > 0) {
+        TCR_CUDA(cudaMemsetAsync(W.counts, 0, sizeof(int32_t) * nq, st));
+        const int32_t* gstart;
+        const int32_t* ngroups;
+        if (self) {
+            pack_self_queries_kernel<<<grid_for(nq, 256), 256, 0, st>>>(sp, S.grid, d->query_pos, d->query_sup,
+                                                                        S.rsidx, nq, W.qsorted, W.qsidx);
+            note_launches(1);
+            gstart = S.cell_start;
+            ngroups = S.num_cells;
+        } else {
+            // sort the queries by their own cells
+            sort_state_init_kernel<<<1, 1, 0, st>>>(W.sort.state);
+            note_launches(1);
+            pack_points_kernel<<<grid_for(nq, 256), 256, 0, st>>>(sp, S.grid, d->query_pos, d->query_sup, nq, 1,
+                                                                  W.pack, W.sort.keys[0], W.sort.vals[0],
+                                                                  W.sort.state);
+            note_launches(1);
+            TCR_CUDA(radix_sort_pairs(W.sort, nq, st));
+            gather_sorted_kernel<<<grid_for(nq, 256), 256, 0, st>>>(S.grid, W.pack, W.sort.vals[0], W.sort.vals[1],
+                                                                    W.sort.state, nq, W.qsorted, W.qsidx);
+            note_launches(1);
+            QueryGroupOut qo{sp, S.grid, W.qsorted, W.qgroup_start, W.qgroup_coords};
+            RunFlagIn fi{S.grid, W.sort.keys[0], W.sort.keys[1], W.sort.state};
+            TCR_CUDA(device_exclusive_scan<int32_t>(fi, qo, nq, W.scan_tiles32, W.num_qgroups, st));
+            finish_cells_kernel<<<1, 1, 0, st>>>(W.qgroup_start, W.num_qgroups, nq);
+            note_launches(1);
+            gstart = W.qgroup_start;
+            ngroups = W.num_qgroups;
+        }
+        BoundedUnitCountIn ui{gstart, ngroups};
+        BoundedUnitOut uo{gstart, ngroups, W.unit_group, W.unit_t0};
+        TCR_CUDA(device_exclusive_scan<int32_t>(ui, uo, nq, W.scan_tiles32, W.num_units, st));
+        WalkArgs a = make_walk(sp, S, W, self);
+        TCR_CUDA(launch_walk<false>(a, d->dim, d->periodic_mask != 0, nq, st));
+    }
+    CountIn ci{W.counts, nq};
+    OffsetOut oo{nq, offsets, indptr_out, row_entries_out};
+    TCR_CUDA(device_exclusive_scan<int64_t>(ci, oo, nq + 1, W.scan_tiles64, W.total, st));
+    info_kernel<<<1, 1, 0, st>>>(S.grid, W.total, W.num_stray, W.info);
+    note_launches(1);
+    if (info_out) TCR_CUDA(cudaMemcpyAsync(info_out, W.info, 4 * sizeof(int64_t), cudaMemcpyDeviceToHost, st));
+    return TCR_OK;
+}
+
+int tcr_emit(const tcr_search_desc* d, const void* structure, void* scratch, int64_t scratch_bytes,
+             const int64_t* offsets, int64_t* row_out, int64_t* col_out, void* stream) {
+    int rc = validate(d, false);
+    if (rc) return rc;
+    int64_t need_w = 0;
+    carve_scratch(nullptr, d->n_query, d->n_ref, &need_w);
+    if (!structure || !scratch || scratch_bytes < need_w || !offsets)
+        return set_error(TCR_ERR_INVALID, "workspace too small or offsets missing");
+    cudaStream_t st = (cudaStream_t)stream;
+    const SearchParams sp = make_params(d);
+    Structure S = carve_structure(const_cast<void*>(structure), d->n_ref, nullptr);
+    Scratch W = carve_scratch(scratch, d->n_query, d->n_ref, nullptr);
+    const int64_t nq = d->n_query;
+    if (nq <= 0) return TCR_OK;
+    WalkArgs a = make_walk(sp, S, W, d->self_search != 0);
+    a.offsets = offsets;
+    a.row_out = row_out;
+    a.col_out = col_out;
+    // the count pass already collected the stray queries; the emit walk must not re-append them
+    TCR_CUDA(cudaMemsetAsync(W.work + 1, 0, sizeof(int32_t), st));
+    TCR_CUDA(launch_walk<true>(a, d->dim, d->periodic_mask != 0, nq, st));
+    return TCR_OK;
+}
+
+}  // extern "C"
