@@ -124,6 +124,25 @@ int tcr_count(const tcr_search_desc* d, const void* structure, void* scratch, in
 int tcr_emit(const tcr_search_desc* d, const void* structure, void* scratch, int64_t scratch_bytes,
              const int64_t* offsets, int64_t* row_out, int64_t* col_out, void* stream);
 
+/* One whole search -- tcr_build_structure, tcr_count and tcr_emit -- that allocates nothing.
+ * No counterpart in the reference: it exists for callers that cannot allocate device memory at
+ * search time (a host that gives the search a fixed arena at start-up and forbids cudaMalloc
+ * afterwards, e.g. because cudaMalloc can synchronise the device inside a real-time loop, or a
+ * plugin host whose allocator the search cannot reach).  The structure and scratch live in a
+ * 32 MiB file-scope device array that every GPU loading this library holds until exit, which
+ * bounds a search to about 180K points (the exact limit is the byte size of structure plus
+ * scratch; larger searches are rejected with TCR_ERR_INVALID before any device work).
+ * The caller passes its inputs in `d` and its outputs: offsets (device int64 [n_query+1]),
+ * optional indptr_out / row_entries_out as in tcr_count, row_out (NULL for CSR) and col_out of
+ * pair_capacity entries.  The call synchronises `stream` once to learn the pair count
+ * (*total_out); if it exceeds pair_capacity nothing is emitted and TCR_ERR_INVALID is returned,
+ * so the caller can retry with a larger output.
+ * The first call on a device looks the array up with cudaGetSymbolAddress; make that first call
+ * before any stream capture.  All calls share the one array: calls whose work overlaps on the GPU
+ * (other streams, other host threads) race and must be serialised by the caller. */
+int tcr_search_noalloc(const tcr_search_desc* d, int64_t* offsets, int32_t* indptr_out, int64_t* row_entries_out,
+                       int64_t* row_out, int64_t* col_out, int64_t pair_capacity, int64_t* total_out, void* stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -49,6 +49,7 @@ SIGNATURES = {
     "tcr_build_structure": (ctypes.c_int, [_desc_p, _vp, _i64, _vp, _i64, _vp]),
     "tcr_count": (ctypes.c_int, [_desc_p, _vp, _vp, _i64, _vp, _vp, _vp, _vp, _vp]),
     "tcr_emit": (ctypes.c_int, [_desc_p, _vp, _vp, _i64, _vp, _vp, _vp, _vp]),
+    "tcr_search_noalloc": (ctypes.c_int, [_desc_p, _vp, _vp, _vp, _vp, _vp, _i64, ctypes.POINTER(_i64), _vp]),
 }
 
 

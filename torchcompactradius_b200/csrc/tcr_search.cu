@@ -15,6 +15,7 @@
 #include <cstring>
 #include <cstdarg>
 #include <algorithm>
+#include <mutex>
 
 #include "tcr_common.cuh"
 #include "tcr_scan.cuh"
@@ -932,3 +933,84 @@ int tcr_emit(const tcr_search_desc* d, const void* structure, void* scratch, int
 }
 
 }  // extern "C"
+
+// ------------------------------------------------------------------------------------------
+// Search without any device allocation.
+//
+// Some callers cannot allocate device memory at search time: a host application that hands the
+// search a fixed memory arena at start-up and forbids cudaMalloc afterwards (cudaMalloc can
+// synchronise the device and stall a real-time loop), or a plugin host whose allocator the
+// search cannot reach.  tcr_search_noalloc serves them: the structure and the scratch of one
+// whole search live in the file-scope device array below, so the caller passes only its inputs
+// and its output buffers.  The array is kTcrStaticScratchBytes (32 MiB) on every GPU that loads
+// this library, held until the process exits.
+namespace tcr {
+constexpr int64_t kTcrStaticScratchBytes = 32ll << 20;
+static __device__ __align__(256) unsigned char g_static_scratch[kTcrStaticScratchBytes];
+
+constexpr int kMaxDevices = 64;
+static void* g_static_ptr[kMaxDevices] = {nullptr};
+static int g_static_err[kMaxDevices] = {0};
+static std::once_flag g_static_once[kMaxDevices];
+
+// Device address of g_static_scratch on the current device.  In host code the symbol's name is
+// only a host-side stand-in, so the address is asked from the runtime, once per device, with that
+// device current.
+static int static_scratch_address(void** out) {
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return set_error(TCR_ERR_CUDA, "cudaGetDevice: %s", cudaGetErrorString(e));
+    if (dev < 0 || dev >= kMaxDevices) return set_error(TCR_ERR_INVALID, "device ordinal %d out of range", dev);
+    std::call_once(g_static_once[dev], [dev]() {
+        void* p = nullptr;
+        cudaError_t r = cudaGetSymbolAddress(&p, g_static_scratch);
+        if (r == cudaSuccess) g_static_ptr[dev] = p;
+        else g_static_err[dev] = (int)r;
+    });
+    if (!g_static_ptr[dev])
+        return set_error(TCR_ERR_CUDA, "cudaGetSymbolAddress(static scratch) failed on device %d: %s", dev,
+                         cudaGetErrorString((cudaError_t)g_static_err[dev]));
+    *out = g_static_ptr[dev];
+    return TCR_OK;
+}
+}  // namespace tcr
+
+extern "C" int tcr_search_noalloc(const tcr_search_desc* d, int64_t* offsets, int32_t* indptr_out,
+                                  int64_t* row_entries_out, int64_t* row_out, int64_t* col_out,
+                                  int64_t pair_capacity, int64_t* total_out, void* stream) {
+    using namespace tcr;
+    int rc = validate(d);
+    if (rc) return rc;
+    if (!offsets || (pair_capacity > 0 && !col_out) || pair_capacity < 0)
+        return set_error(TCR_ERR_INVALID, "offsets and a column buffer of pair_capacity entries are required");
+    int64_t s_bytes = 0, w_bytes = 0;
+    carve_structure(nullptr, d->n_ref, &s_bytes);
+    carve_scratch(nullptr, d->n_query, d->n_ref, &w_bytes);
+    if (s_bytes + w_bytes > kTcrStaticScratchBytes)
+        return set_error(TCR_ERR_INVALID,
+                         "tcr_search_noalloc: %lld query and %lld reference points need %lld bytes of scratch, "
+                         "more than the static %lld bytes (about 180K points); use tcr_build_structure/"
+                         "tcr_count/tcr_emit with caller-allocated buffers",
+                         (long long)d->n_query, (long long)d->n_ref, (long long)(s_bytes + w_bytes),
+                         (long long)kTcrStaticScratchBytes);
+    void* base = nullptr;
+    rc = static_scratch_address(&base);
+    if (rc) return rc;
+    void* structure = base;
+    void* scratch = static_cast<char*>(base) + s_bytes;
+    // Every kernel below initialises what it reads (counters, map, sort state), so the contents a
+    // previous call left in the array do not matter.
+    rc = tcr_build_structure(d, structure, s_bytes, scratch, w_bytes, stream);
+    if (rc) return rc;
+    int64_t info[4] = {0, 0, 0, 0};
+    rc = tcr_count(d, structure, scratch, w_bytes, offsets, indptr_out, row_entries_out, info, stream);
+    if (rc) return rc;
+    TCR_CUDA(cudaStreamSynchronize((cudaStream_t)stream));
+    if (total_out) *total_out = info[0];
+    if (info[1]) return set_error(TCR_ERR_INVALID, "no valid cell grid for this domain and support");
+    if (info[0] > pair_capacity)
+        return set_error(TCR_ERR_INVALID, "tcr_search_noalloc: %lld pairs do not fit the %lld-entry output",
+                         (long long)info[0], (long long)pair_capacity);
+    if (info[0] == 0) return TCR_OK;
+    return tcr_emit(d, structure, scratch, w_bytes, offsets, row_out, col_out, stream);
+}
