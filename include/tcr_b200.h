@@ -20,7 +20,7 @@
 extern "C" {
 #endif
 
-#define TCR_ABI_VERSION 1
+#define TCR_ABI_VERSION 4
 
 #define TCR_OK 0
 #define TCR_ERR_INVALID (-1) /* bad argument or workspace too small */
@@ -109,20 +109,30 @@ int tcr_build_structure(const tcr_search_desc* d, void* structure, int64_t struc
 
 /* Counts the neighbours of every query and scans them.  Replaces the countNeighbors operator
  * (cppSrc/neighborhood.h:140-146, cppWrapper.cpp:39) plus the cumsum of cppSearch.py:81-84.
+ * Every (query, candidate) pair is tested once here: each work unit (<= 32 queries of one cell
+ * with <= 768 candidates) writes a record of its hit masks and candidate indices to `stage`
+ * (device int32, stage_capacity words) for tcr_emit to expand into place.  Units that do not fit
+ * (or every unit when stage is NULL / capacity 0) are tested again by tcr_emit.
  * offsets: device int64 [n_query+1] (exclusive scan, offsets[n_query] = total pairs).
  * indptr_out (device int32 [n_query+1]) and row_entries_out (device int64 [n_query]) are the
- * SparseCSR fields of util.py:321-358 and may be NULL.  info_out (host, 4 x int64, may be
- * NULL) receives {total pairs, grid error flag, queries walked serially, exact-only mode}
- * asynchronously on `stream`. */
-int tcr_count(const tcr_search_desc* d, const void* structure, void* scratch, int64_t scratch_bytes,
-              int64_t* offsets, int32_t* indptr_out, int64_t* row_entries_out, int64_t* info_out, void* stream);
+ * SparseCSR fields of util.py:321-358 and may be NULL.  info_out (host, 8 x int64, may be NULL)
+ * receives, asynchronously on `stream`: {total pairs, grid error flag, queries walked serially,
+ * exact-only mode, staging words the units asked for, units left for tcr_emit to re-test, 0, 0};
+ * a caller sizes the next search's staging list from entry 4. */
+int tcr_count(const tcr_search_desc* d, const void* structure, void* scratch, int64_t scratch_bytes, int32_t* stage,
+              int64_t stage_capacity, int64_t* offsets, int32_t* indptr_out, int64_t* row_entries_out,
+              int64_t* info_out, void* stream);
 
-/* Writes the neighbour pairs at the offsets of tcr_count (same scratch, same descriptor).
+/* Writes the neighbour pairs at the offsets of tcr_count (same scratch, stage and descriptor).
  * Replaces the buildNeighborList operator (cppSrc/neighborhood.h:155-162, cppWrapper.cpp:40)
  * and the j = sortIndex[j] unsort of cppSearch.py:97: col_out receives original reference
- * indices, row_out (NULL for CSR) original query indices, both int64 [total]. */
+ * indices, row_out (NULL for CSR) original query indices, int64 [out_capacity] each.  It may be
+ * enqueued right after tcr_count without waiting for the total: pairs at positions >=
+ * out_capacity are dropped, so a caller that guessed too small a buffer reads the total from
+ * tcr_count's info and calls tcr_emit again with a large enough one. */
 int tcr_emit(const tcr_search_desc* d, const void* structure, void* scratch, int64_t scratch_bytes,
-             const int64_t* offsets, int64_t* row_out, int64_t* col_out, void* stream);
+             const int32_t* stage, const int64_t* offsets, int64_t* row_out, int64_t* col_out, int64_t out_capacity,
+             void* stream);
 
 /* One whole search -- tcr_build_structure, tcr_count and tcr_emit -- that allocates nothing.
  * No counterpart in the reference: it exists for callers that cannot allocate device memory at

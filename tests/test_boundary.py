@@ -33,7 +33,7 @@ def test_library_exports_every_declared_symbol():
 def test_descriptor_layout_matches_library():
     from torchcompactradius_b200 import _lib
     assert ctypes.sizeof(_lib.SearchDesc) == _lib.load().tcr_desc_bytes()
-    assert _lib.load().tcr_version() == 1
+    assert _lib.load().tcr_version() == 4
 
 
 def test_sizes_and_layout_are_consistent():
@@ -59,7 +59,7 @@ def test_invalid_descriptor_is_rejected_without_device_work():
     d.hash_map_length = 4096
     d.n_query = 10
     d.n_ref = 10
-    rc = lib.tcr_count(ctypes.byref(d), None, None, 0, None, None, None, None, None)
+    rc = lib.tcr_count(ctypes.byref(d), None, None, 0, None, 0, None, None, None, None, None)
     assert rc == -1
 
 

@@ -52,14 +52,15 @@ def _regular(d, fmt):
     off = torch.empty(d.n_query + 1, dtype=torch.int64, device="cuda")
     ip = torch.empty(d.n_query + 1, dtype=torch.int32, device="cuda")
     re = torch.empty(d.n_query, dtype=torch.int64, device="cuda")
-    info = torch.zeros(4, dtype=torch.int64, pin_memory=True)
-    _lib.check(lib.tcr_count(ctypes.byref(d), _vp(st), _vp(sc), w, _vp(off), _vp(ip), _vp(re),
+    info = torch.zeros(8, dtype=torch.int64, pin_memory=True)
+    _lib.check(lib.tcr_count(ctypes.byref(d), _vp(st), _vp(sc), w, None, 0, _vp(off), _vp(ip), _vp(re),
                              ctypes.c_void_p(info.data_ptr()), stream), "count")
     torch.cuda.current_stream().synchronize()
     n = int(info[0])
     col = torch.empty(n, dtype=torch.int64, device="cuda")
     row = torch.empty(n, dtype=torch.int64, device="cuda") if fmt == "coo" else None
-    _lib.check(lib.tcr_emit(ctypes.byref(d), _vp(st), _vp(sc), w, _vp(off), _vp(row), _vp(col), stream), "emit")
+    _lib.check(lib.tcr_emit(ctypes.byref(d), _vp(st), _vp(sc), w, None, _vp(off), _vp(row), _vp(col), n, stream),
+               "emit")
     torch.cuda.synchronize()
     return off, ip, re, row, col
 

@@ -47,8 +47,8 @@ SIGNATURES = {
     "tcr_search_sizes": (ctypes.c_int, [_i64, _i64, _i32, ctypes.POINTER(_i64), ctypes.POINTER(_i64)]),
     "tcr_structure_offsets": (ctypes.c_int, [_i64, ctypes.POINTER(_i64), _i32]),
     "tcr_build_structure": (ctypes.c_int, [_desc_p, _vp, _i64, _vp, _i64, _vp]),
-    "tcr_count": (ctypes.c_int, [_desc_p, _vp, _vp, _i64, _vp, _vp, _vp, _vp, _vp]),
-    "tcr_emit": (ctypes.c_int, [_desc_p, _vp, _vp, _i64, _vp, _vp, _vp, _vp]),
+    "tcr_count": (ctypes.c_int, [_desc_p, _vp, _vp, _i64, _vp, _i64, _vp, _vp, _vp, _vp, _vp]),
+    "tcr_emit": (ctypes.c_int, [_desc_p, _vp, _vp, _i64, _vp, _vp, _vp, _vp, _i64, _vp]),
     "tcr_search_noalloc": (ctypes.c_int, [_desc_p, _vp, _vp, _vp, _vp, _vp, _i64, ctypes.POINTER(_i64), _vp]),
 }
 

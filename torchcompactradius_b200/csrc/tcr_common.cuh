@@ -42,17 +42,29 @@ struct SearchParams {
     int64_t n_ref;
 };
 
+// Reduction record over one set of supports.
+struct SupportStats {
+    uint32_t max_key;        // float_key of the largest support (NaN propagates)
+    int32_t bad;             // some support is not in [1e-18, 1e18] (negative, zero, tiny, huge, NaN)
+};
+
 // Device-computed grid description (one record in device memory).
 struct GridParams {
     float hmax;              // computeGridSupport result
     float hcell;             // compute_h result
     int32_t count[3];        // ceil(ext / hcell) as int32
-    int32_t always_exact;    // 1: supports outside [1e-18, 1e18] or non-finite: exact test always
+    int32_t always_exact;    // 1: some support outside [1e-18, 1e18] or non-finite: exact test always
     int32_t error;           // nonzero: invalid grid (e.g. zero cells on a periodic dim)
-    uint32_t hmax_key;       // ordered-int encoding used by the max reduction
-    uint32_t hmin_abs_key;   // min |h| (ordered key) for the exact-mode decision
-    int32_t nonfinite;       // any support is NaN/inf
-    int32_t pad;
+    int32_t out_of_grid;     // some reference point's cell lies outside [0, count) (linear indices may alias)
+    SupportStats ref_stats;  // over the reference supports (the candidates' thresholds)
+    SupportStats build_query_stats;  // over the query supports seen at build time
+};
+
+// Per-search query-side parameters of the lean test (scratch).
+struct QueryParams {
+    SupportStats stats;      // over this search's query supports
+    float qmax;              // largest query support (band of the fast test)
+    int32_t exact_all;       // decide every pair with the exact reference test
 };
 
 // Ordered uint32 encoding of floats: a < b  <=>  key(a) < key(b); NaN maps above +inf.

@@ -112,7 +112,14 @@ struct Scratch {
     int32_t* num_stray;     // [1]
     int32_t* work;          // [4] work counters
     int64_t* total;         // [1]
-    int64_t* info;          // [4] total pairs, grid error, stray queries, exact-only mode
+    int64_t* info;          // [8] total pairs, grid error, stray queries, exact-only mode, staging words
+                            //     requested, units re-walked by tcr_emit, 0, 0
+    QueryParams* qparams;   // [1]
+    int32_t* rec;           // [nq] per unit: offset of its record in the staging list (-1: not staged)
+    int32_t* query_unit;    // [nq] unit of each sorted query
+    int32_t* flagged;       // [nq] units re-walked by the emit pass
+    int32_t* num_flagged;   // [1]
+    unsigned long long* cursor;  // [1] staging fill
 };
 
 static Scratch carve_scratch(void* buf, int64_t nq, int64_t nr, int64_t* bytes) {
@@ -125,7 +132,10 @@ static Scratch carve_scratch(void* buf, int64_t nq, int64_t nr, int64_t* bytes) 
     s.num_stray = c.take<int32_t>(1);
     s.work = c.take<int32_t>(4);
     s.total = c.take<int64_t>(1);
-    s.info = c.take<int64_t>(4);
+    s.info = c.take<int64_t>(8);
+    s.qparams = c.take<QueryParams>(1);
+    s.num_flagged = c.take<int32_t>(1);
+    s.cursor = c.take<unsigned long long>(1);
     s.pack = c.take<float4>(nmax);
     s.sort.keys[0] = c.take<uint32_t>(nmax);
     s.sort.keys[1] = c.take<uint32_t>(nmax);
@@ -144,6 +154,9 @@ static Scratch carve_scratch(void* buf, int64_t nq, int64_t nr, int64_t* bytes) 
     s.unit_t0 = c.take<int32_t>(q);
     s.counts = c.take<int32_t>(q);
     s.stray = c.take<int32_t>(q);
+    s.rec = c.take<int32_t>(q);
+    s.query_unit = c.take<int32_t>(q);
+    s.flagged = c.take<int32_t>(q);
     if (bytes) *bytes = c.off;
     return s;
 }
@@ -152,29 +165,59 @@ static Scratch carve_scratch(void* buf, int64_t nq, int64_t nr, int64_t* bytes) 
 // build kernels
 
 
-// computeGridSupport (cellTable.py:40-81): max over the supports the mode uses; also tracks
-// min |h| and non-finite values for the exact-mode decision.
-__global__ void support_reduce_kernel(const float* a, int64_t na, const float* b, int64_t nb, GridParams* g) {
-    uint32_t kmax = 0, kmin = 0xffffffffu;
-    int nonfinite = 0;
-    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
-    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < na + nb; i += stride) {
-        float h = i < na ? a[i] : b[i - na];
-        kmax = max(kmax, float_key(h));
-        kmin = min(kmin, float_key(fabsf(h)));
-        nonfinite |= !isfinite(h);
-    }
+// Block reduction of max / or over a strided array; one atomic per block and field.
+__device__ __forceinline__ void block_reduce_stats(uint32_t kmax, int bad, SupportStats* out) {
+    __shared__ uint32_t s_max[32];
+    __shared__ int s_bad[32];
 #pragma unroll
     for (int o = 16; o; o >>= 1) {
         kmax = max(kmax, __shfl_xor_sync(0xffffffffu, kmax, o));
-        kmin = min(kmin, __shfl_xor_sync(0xffffffffu, kmin, o));
-        nonfinite |= __shfl_xor_sync(0xffffffffu, nonfinite, o);
+        bad |= __shfl_xor_sync(0xffffffffu, bad, o);
     }
-    if ((threadIdx.x & 31) == 0) {
-        atomicMax(&g->hmax_key, kmax);
-        atomicMin(&g->hmin_abs_key, kmin);
-        if (nonfinite) atomicOr(&g->nonfinite, 1);
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    if (lane == 0) { s_max[w] = kmax; s_bad[w] = bad; }
+    __syncthreads();
+    if (w == 0) {
+        kmax = lane < nw ? s_max[lane] : 0u;
+        bad = lane < nw ? s_bad[lane] : 0;
+#pragma unroll
+        for (int o = 16; o; o >>= 1) {
+            kmax = max(kmax, __shfl_xor_sync(0xffffffffu, kmax, o));
+            bad |= __shfl_xor_sync(0xffffffffu, bad, o);
+        }
+        if (lane == 0) {
+            atomicMax(&out->max_key, kmax);
+            if (bad) atomicOr(&out->bad, 1);
+        }
     }
+}
+
+// computeGridSupport (cellTable.py:40-81) needs the largest support; the lean test needs to know
+// whether every support lies in [1e-18, 1e18] (else the exact test decides every pair).
+__global__ void support_stats_kernel(const float* __restrict__ h, int64_t n, SupportStats* out) {
+    uint32_t kmax = 0;
+    int bad = 0;
+    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
+        const float v = h[i];
+        kmax = max(kmax, float_key(v));
+        bad |= !(v >= 1e-18f && v <= 1e18f);
+    }
+    block_reduce_stats(kmax, bad, out);
+}
+
+__global__ void stats_init_kernel(SupportStats* a, SupportStats* b) {
+    a->max_key = 0; a->bad = 0;
+    if (b) { b->max_key = 0; b->bad = 0; }
+}
+
+// Query-side parameters of one search.
+__global__ void query_params_kernel(const GridParams* g, int mode, int has_query_sup, QueryParams* qp) {
+    const float qmax = has_query_sup ? key_float(qp->stats.max_key) : 0.0f;
+    qp->qmax = (mode == kScatter) ? 0.0f : qmax;
+    const bool qbad = (mode != kScatter) && has_query_sup && qp->stats.bad;
+    const bool rbad = (mode != kGather) && g->ref_stats.bad;
+    qp->exact_all = (qbad || rbad || !(fabsf(qp->qmax) <= 1e18f)) ? 1 : 0;
 }
 
 __global__ void sort_state_init_kernel(SortState* st) {
@@ -184,10 +227,12 @@ __global__ void sort_state_init_kernel(SortState* st) {
 }
 
 __global__ void grid_init_kernel(GridParams* g, SortState* st) {
-    g->hmax_key = 0;
-    g->hmin_abs_key = 0xffffffffu;
-    g->nonfinite = 0;
+    g->ref_stats.max_key = 0;
+    g->ref_stats.bad = 0;
+    g->build_query_stats.max_key = 0;
+    g->build_query_stats.bad = 0;
     g->error = 0;
+    g->out_of_grid = 0;
     st->key_min = 0xffffffffu;
     st->key_max = 0;
     st->sel[0] = 0;
@@ -196,7 +241,12 @@ __global__ void grid_init_kernel(GridParams* g, SortState* st) {
 // util.py:28-79 compute_h and cellTable.py:27-29, float32 throughout.
 __global__ void grid_params_kernel(SearchParams sp, GridParams* g, SortState* st) {
     const float grow = 1.00010001659393310546875f;  // fl32(1e-4 + 1)
-    float hmax = key_float(g->hmax_key);
+    // computeGridSupport: scatter reads the reference supports, gather the query supports,
+    // (super)symmetric both (torch.max propagates NaN, as the key maximum does).
+    uint32_t key = 0;
+    if (sp.mode != kGather) key = max(key, g->ref_stats.max_key);
+    if (sp.mode != kScatter) key = max(key, g->build_query_stats.max_key);
+    float hmax = key_float(key);
     float ext[3], nc[3], h[3];
     bool any = false;
     for (int d = 0; d < sp.dim; ++d) {
@@ -226,8 +276,8 @@ __global__ void grid_params_kernel(SearchParams sp, GridParams* g, SortState* st
     g->hmax = hmax;
     g->hcell = hc;
     for (int d = 0; d < 3; ++d) g->count[d] = d < sp.dim ? (int32_t)ceilf(__fdiv_rn(ext[d], hc)) : 1;
-    float hmin_abs = key_float(g->hmin_abs_key);
-    g->always_exact = (g->nonfinite || !(hmin_abs >= 1e-18f) || !(fabsf(hmax) <= 1e18f)) ? 1 : 0;
+    g->always_exact = ((sp.mode != kGather && g->ref_stats.bad) || (sp.mode != kScatter && g->build_query_stats.bad))
+                          ? 1 : 0;
     int err = 0;
     if (!(hc > 0.0f) || !isfinite(hc)) err = 1;  // no valid grid (support larger than the domain, NaN, ...)
     for (int d = 0; d < sp.dim; ++d)
@@ -264,15 +314,20 @@ __device__ __forceinline__ void point_cell(const SearchParams& sp, const GridPar
 
 // Wrap (twice for the reference cloud, cppSearch.py:221 after neighborhood.py:203; once for a
 // query cloud), pack to float4 and emit the signed-order linear key.
-__global__ void pack_points_kernel(SearchParams sp, const GridParams* g, const float* x, const float* h, int64_t n,
-                                   int wraps, float4* pack, uint32_t* keys, int32_t* vals, SortState* st) {
-    if (g->error) return;
+__global__ void pack_points_kernel(SearchParams sp, GridParams* g, const float* x, const float* h, int64_t n,
+                                   int wraps, float4* pack, uint32_t* keys, int32_t* vals, SortState* st,
+                                   int track_grid) {
     uint32_t kmin = 0xffffffffu, kmax = 0;
     const int64_t stride = (int64_t)gridDim.x * blockDim.x;
-    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n && !g->error; i += stride) {
         float4 v = wrap_point(sp, load_point(x, h, i, sp.dim), wraps);
         int32_t c[3];
         point_cell(sp, g, v, c);
+        if (track_grid) {
+            bool out = false;
+            for (int d = 0; d < sp.dim; ++d) out |= c[d] < 0 || c[d] >= g->count[d];
+            if (out && !g->out_of_grid) atomicOr(&g->out_of_grid, 1);
+        }
         uint32_t key = (uint32_t)linear_index(sp.dim, c, g->count) ^ 0x80000000u;
         pack[i] = v;
         keys[i] = key;
@@ -280,14 +335,27 @@ __global__ void pack_points_kernel(SearchParams sp, const GridParams* g, const f
         kmin = min(kmin, key);
         kmax = max(kmax, key);
     }
+    __shared__ uint32_t s_min[32], s_max[32];
 #pragma unroll
     for (int o = 16; o; o >>= 1) {
         kmin = min(kmin, __shfl_xor_sync(0xffffffffu, kmin, o));
         kmax = max(kmax, __shfl_xor_sync(0xffffffffu, kmax, o));
     }
-    if ((threadIdx.x & 31) == 0) {
-        atomicMin(&st->key_min, kmin);
-        atomicMax(&st->key_max, kmax);
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    if (lane == 0) { s_min[w] = kmin; s_max[w] = kmax; }
+    __syncthreads();
+    if (w == 0) {
+        kmin = lane < nw ? s_min[lane] : 0xffffffffu;
+        kmax = lane < nw ? s_max[lane] : 0u;
+#pragma unroll
+        for (int o = 16; o; o >>= 1) {
+            kmin = min(kmin, __shfl_xor_sync(0xffffffffu, kmin, o));
+            kmax = max(kmax, __shfl_xor_sync(0xffffffffu, kmax, o));
+        }
+        if (lane == 0) {
+            atomicMin(&st->key_min, kmin);
+            atomicMax(&st->key_max, kmax);
+        }
     }
 }
 
@@ -433,22 +501,34 @@ struct BoundedUnitOut {
     const int32_t* num_groups;
     int32_t* unit_group;
     int32_t* unit_t0;
+    int32_t* query_unit;
     __device__ void operator()(int64_t g, int32_t ex, int32_t nunits) const {
         if (g >= *num_groups) return;
-        int32_t s = group_start[g];
+        const int32_t s = group_start[g], e = group_start[g + 1];
         for (int32_t u = 0; u < nunits; ++u) {
             unit_group[ex + u] = (int32_t)g;
             unit_t0[ex + u] = s + u * kUnit;
         }
+        for (int32_t t = s; t < e; ++t) query_unit[t] = ex + (t - s) / kUnit;
     }
 };
 
 // ------------------------------------------------------------------------------------------
 // the candidate walk
+//
+// Work unit: <= 32 queries of one query group (cell).  One warp walks the unit's stencil
+// candidates in chunks of 32 (lane = candidate) and tests every query of the unit against the
+// chunk (query positions broadcast from shared memory); __ballot_sync gives, per query and chunk,
+// the 32-bit hit mask.  Pass 1 keeps the masks of a unit with <= kSegChunks chunks in shared
+// memory, reserves room for the unit's hits in a staging list with one atomic and writes them
+// there query by query; pass 2 moves each query's staged hits to its CSR/COO slot (a memory-bound
+// copy).  A unit with more chunks, or one that finds the staging list full, is only counted in
+// pass 1 and is walked again (with the test) in pass 2 to write its pairs directly.
 
 struct WalkArgs {
     SearchParams sp;
     const GridParams* g;
+    const QueryParams* qp;
     const float4* __restrict__ rsorted;
     const int32_t* __restrict__ rsidx;
     const int32_t* __restrict__ cell_start;
@@ -463,13 +543,25 @@ struct WalkArgs {
     const int32_t* __restrict__ unit_group;
     const int32_t* __restrict__ unit_t0;
     const int32_t* __restrict__ num_units;
+    const int32_t* __restrict__ unit_list;  // emit re-walk: the units to walk (null: all units)
+    const int32_t* __restrict__ num_list;
     int32_t* work;
     int32_t* stray;
     int32_t* num_stray;
-    int32_t* counts;             // count pass output [nq] (original query order)
-    const int64_t* offsets;      // emit pass input [nq+1]
-    int64_t* row_out;            // emit: COO rows or null
-    int64_t* col_out;            // emit: columns
+    int32_t* counts;              // [nq] pass-1 output, original query order
+    int32_t* rec;                 // [units] offset of each unit's record in the staging list, -1 if not staged
+    int32_t no_stray_check;       // self search, no periodic dims, every point in the grid: a query's cell is
+                                  // its group's (the device flag out_of_grid withdraws this)
+    int32_t* query_unit;          // [nq] unit of each sorted query
+    int32_t* flagged;             // [units] units to re-walk in pass 2
+    int32_t* num_flagged;
+    unsigned long long* cursor;   // staging list fill
+    int32_t* stage;               // staging list (original reference indices)
+    int64_t stage_cap;
+    const int64_t* offsets;       // pass-2 input [nq+1]
+    int64_t* row_out;             // pass 2: COO rows or null
+    int64_t* col_out;             // pass 2: columns
+    int64_t out_cap;              // pass 2: entries of row_out/col_out; writes beyond are dropped
 };
 
 // Looks up stencil cell `o` (getOffsets order, last coordinate fastest) around cell gc with the
@@ -505,104 +597,499 @@ __device__ __forceinline__ bool same_cell(const int32_t* a, const int32_t* b) {
     return s;
 }
 
-constexpr int kWalkWarps = 8;
+// Per-candidate pieces of the lean test: the candidate's share of the threshold and the half
+// width of the band (conservative over every query: qmax is the largest query support).
+template <int MODE>
+__device__ __forceinline__ float cand_share(float hc) {
+    return MODE == kSymmetric ? 0.5f * hc : hc;
+}
+template <int MODE>
+__device__ __forceinline__ float cand_band(float cw, float qmax) {
+    float t;
+    if (MODE == kGather) t = qmax;
+    else if (MODE == kScatter) t = cw;
+    else if (MODE == kSymmetric) t = fmaf(qmax, 0.5f, cw);
+    else t = fmaxf(qmax, cw);
+    return kBandEps * t * t;
+}
+// thr for (query support hq, candidate share cw), float-exact as the reference evaluates it.
+template <int MODE>
+__device__ __forceinline__ float pair_thr(float hq, float cw) {
+    if (MODE == kGather) return hq;
+    if (MODE == kScatter) return cw;
+    if (MODE == kSymmetric) return fmaf(hq, 0.5f, cw);  // fl(hq/2 + hc/2) == fl(hq + hc) / 2
+    return fmaxf(hq, cw);
+}
 
-template <int DIM, bool PERIODIC, bool EMIT>
-__global__ void __launch_bounds__(kWalkWarps * 32) walk_kernel(WalkArgs a) {
+// One (query, candidate) test.  in: decided; unc: needs the exact reference test.
+template <int DIM, bool PERIODIC, int MODE>
+__device__ __forceinline__ void lean_test(const SearchParams& sp, const float4& q, const float4& c, float cw,
+                                          float band, bool& in, bool& unc) {
+    float d2;
+    bool wrap_unc = false;
+    {
+        float dd[3];
+#pragma unroll
+        for (int d = 0; d < DIM; ++d) {
+            float diff = comp(q, d) - comp(c, d);
+            if (PERIODIC && ((sp.periodic_mask >> d) & 1)) {
+                const float h = sp.ext[d];
+                const float half = 0.5f * h;
+                wrap_unc |= fabsf(fabsf(diff) - half) <= kBandEps * h;
+                if (diff >= half) diff -= h;
+                else if (diff < -half) diff += h;
+            }
+            dd[d] = diff;
+        }
+        d2 = dd[0] * dd[0];
+        if (DIM > 1) d2 = fmaf(dd[1], dd[1], d2);
+        if (DIM > 2) d2 = fmaf(dd[2], dd[2], d2);
+    }
+    const float thr = pair_thr<MODE>(q.w, cw);
+    const float r = fmaf(-thr, thr, d2);  // d2 - thr^2, one rounding; sign exact
+    in = r < 0.0f;
+    unc = (fabsf(r) <= band) || wrap_unc;
+}
+
+constexpr int kWalkWarps = 4;
+constexpr int kSegChunks = 24;  // staged units: at most 24 chunks (768 candidates)
+constexpr int kMaskStride = kSegChunks + 1;  // padded rows: conflict-free per-lane reads
+
+struct WalkSmem {
+    int32_t pre[kWalkWarps][33];
+    int32_t beg[kWalkWarps][32];
+    float4 q[kWalkWarps][32];
+    float4 cand[kWalkWarps][36];                  // the chunk's candidates, stream-major, rows padded
+    uint32_t mask[kWalkWarps][32 * kMaskStride];  // [query][chunk] hit masks
+    int32_t sj[kWalkWarps][kSegChunks][32];       // original index of candidate (chunk, lane)
+};
+
+// Candidate k of the unit (prefix pre[0..S]): returns its sorted index.
+__device__ __forceinline__ int32_t cand_index(const int32_t* pre, const int32_t* beg, int S, int32_t k) {
+    int lo = 0, hi = S;  // pre[lo] <= k < pre[hi]
+    while (hi - lo > 1) {
+        int mid = (lo + hi) >> 1;
+        if (pre[mid] <= k) lo = mid; else hi = mid;
+    }
+    return beg[lo] + (k - pre[lo]);
+}
+
+// Lane-side constants of the lean test for query q (support hq): the query's share of the
+// threshold and the half width of the band, conservative over every candidate (rmax is the
+// largest reference support).
+template <int MODE>
+__device__ __forceinline__ float query_share(float hq) {
+    return MODE == kSymmetric ? 0.5f * hq : (MODE == kGather ? hq * hq : hq);
+}
+template <int MODE>
+__device__ __forceinline__ float query_band(float hq, float rmax) {
+    float t;
+    if (MODE == kGather) t = hq;
+    else if (MODE == kScatter) t = rmax;
+    else if (MODE == kSymmetric) t = fmaf(hq, 0.5f, 0.5f * rmax);
+    else t = fmaxf(hq, rmax);
+    return kBandEps * t * t;
+}
+
+// Float test of query q (lane) against candidate c; r < 0 means inside.
+template <int DIM, bool PERIODIC, int MODE>
+__device__ __forceinline__ float lane_residual(const ExactCtx& sp, const float4& q, float qs, const float4& c,
+                                               bool& wrap_unc) {
+    float dd[3];
+#pragma unroll
+    for (int d = 0; d < DIM; ++d) {
+        float diff = comp(q, d) - comp(c, d);
+        if (PERIODIC && ((sp.periodic_mask >> d) & 1)) {
+            const float h = sp.ext[d];
+            const float half = 0.5f * h;
+            wrap_unc |= fabsf(fabsf(diff) - half) <= kBandEps * h;
+            if (diff >= half) diff -= h;
+            else if (diff < -half) diff += h;
+        }
+        dd[d] = diff;
+    }
+    float d2 = dd[0] * dd[0];
+    if (DIM > 1) d2 = fmaf(dd[1], dd[1], d2);
+    if (DIM > 2) d2 = fmaf(dd[2], dd[2], d2);
+    if (MODE == kGather) return d2 - qs;                 // qs = hq^2 (same sign as d2 - hq*hq)
+    if (MODE == kScatter) return fmaf(-c.w, c.w, d2);
+    const float thr = (MODE == kSymmetric) ? fmaf(c.w, 0.5f, qs) : fmaxf(q.w, c.w);
+    return fmaf(-thr, thr, d2);
+}
+
+// Tests the lane's query against the Q candidates of its stream; returns the Q-bit hit mask and
+// ORs into `unc` whether any pair lies in the band (those units are redone with exact decisions).
+template <int DIM, bool PERIODIC, int MODE, int Q>
+__device__ __forceinline__ uint32_t stream_mask(const ExactCtx& sp, const float4* cand, const float4& q, float qs,
+                                                float band, bool& unc) {
+    uint32_t m = 0;
+#pragma unroll
+    for (int k = 0; k < Q; ++k) {
+        const float4 c = cand[k];
+        bool wrap_unc = false;
+        const float r = lane_residual<DIM, PERIODIC, MODE>(sp, q, qs, c, wrap_unc);
+        if (r < 0.0f) m |= 1u << k;
+        unc |= (fabsf(r) <= band) || wrap_unc;
+    }
+    return m;
+}
+
+// The same with every in-band pair decided by the exact reference test (rare units only).
+template <int DIM, bool PERIODIC, int MODE>
+__device__ __noinline__ uint32_t stream_mask_exact(ExactCtx xc, const float4* cand, int n, float4 q, float qs,
+                                                   float band) {
+    const ExactCtx& sp = xc;
+    uint32_t m = 0;
+    for (int k = 0; k < n; ++k) {
+        const float4 c = cand[k];
+        bool wrap_unc = false;
+        const float r = lane_residual<DIM, PERIODIC, MODE>(sp, q, qs, c, wrap_unc);
+        bool in = r < 0.0f;
+        if ((fabsf(r) <= band) || wrap_unc) in = exact_pair_test(xc, q, q.w, c, c.w);
+        if (in) m |= 1u << k;
+    }
+    return m;
+}
+
+// Pass 1: test every (query, candidate) once; count, stage the hits of small units.
+//
+// Each chunk's 32 candidates are staged in shared memory; lane (q, s) holds query q and tests it
+// against the Q candidates of stream s (Q = 8, 16 or 32 as the unit has <= 8, <= 16 or <= 32
+// queries, so 32/Q streams keep every lane busy).  Hits become bits of a per-lane mask, merged
+// across streams with shuffles into the 32-bit (query, chunk) mask.
+template <int DIM, bool PERIODIC, int MODE>
+__global__ void __launch_bounds__(kWalkWarps * 32) walk_count_kernel(WalkArgs a) {
+    if (a.g->error) return;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    WalkSmem& sm = *reinterpret_cast<WalkSmem*>(smem_raw);
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    constexpr int S = DIM == 1 ? 3 : (DIM == 2 ? 9 : 27);
+    const ExactCtx xc = exact_ctx(a.sp);
+    const float rmax = key_float(a.g->ref_stats.max_key);
+    const bool exact_all = a.qp->exact_all != 0;
+    const int32_t nunits = *a.num_units;
+    const float4 nan4 = make_float4(__int_as_float(0x7fc00000), 0.f, 0.f, 0.f);
+    for (;;) {
+        int32_t unit = 0;
+        if (lane == 0) unit = atomicAdd(&a.work[0], 1);
+        unit = __shfl_sync(0xffffffffu, unit, 0);
+        if (unit >= nunits) break;
+        const int32_t grp = a.unit_group[unit];
+        const int32_t t0 = a.unit_t0[unit];
+        const int32_t nb = min(32, a.group_start[grp + 1] - t0);
+        const int32_t gc[3] = {a.group_coords[3 * grp], a.group_coords[3 * grp + 1], a.group_coords[3 * grp + 2]};
+        int32_t beg = 0, cnt = 0;
+        if (lane < S) stencil_lookup(a, gc, lane, beg, cnt);
+        const int32_t inc = warp_inclusive_scan(cnt);
+        sm.pre[w][lane + 1] = inc;
+        if (lane == 0) sm.pre[w][0] = 0;
+        sm.beg[w][lane] = beg;
+        const int32_t M = __shfl_sync(0xffffffffu, inc, 31);
+        bool active = false;
+        int32_t qorig = 0;
+        float4 qv = nan4;
+        if (lane < nb) {
+            const int32_t t = t0 + lane;
+            qv = a.qsorted[t];
+            qorig = a.qsidx[t];
+            active = true;
+            if (!a.no_stray_check || a.g->out_of_grid) {
+                int32_t qc[3];
+                point_cell(a.sp, a.g, qv, qc);
+                active = same_cell<DIM>(qc, gc);
+            }
+            if (!active) {  // own cell differs from the group's (aliasing or wrap rounding): serial path
+                int32_t k = atomicAdd(a.num_stray, 1);
+                a.stray[k] = t;
+                qv = nan4;
+            }
+        }
+        sm.q[w][lane] = qv;  // rows >= nb hold NaN queries and never hit
+        const int32_t nchunks = (M + 31) >> 5;
+        const bool stage = a.stage_cap > 0 && nchunks <= kSegChunks;
+        const int Q = nb <= 8 ? 8 : (nb <= 16 ? 16 : 32);
+        const int lq = lane & (Q - 1);      // this lane's query
+        const int ls = lane / Q;            // this lane's stream
+        __syncwarp();
+        const float4 myq = sm.q[w][lq];
+        const float qs = query_share<MODE>(myq.w);
+        const float band = exact_all ? __int_as_float(0x7f800000) : query_band<MODE>(myq.w, rmax);
+        const float4* my_cand = &sm.cand[w][ls * (Q + 1)];
+        // Lane k of chunk c holds candidate 32c + k.  Its stencil cell r only moves forward from
+        // chunk to chunk, so it is tracked incrementally instead of searched.
+        int32_t cr = 0;
+        const int32_t* pre = sm.pre[w];
+        const int32_t* begs = sm.beg[w];
+        const float4* __restrict__ rs = a.rsorted;
+        const int32_t* __restrict__ ri = a.rsidx;
+        auto fetch = [&cr, pre, begs, rs, ri, M, nan4](int32_t k, float4& v, int32_t& jo) {
+            v = nan4;
+            jo = 0;
+            if (k < M) {
+                while (pre[cr + 1] <= k) ++cr;
+                const int32_t j = begs[cr] + (k - pre[cr]);
+                v = __ldg(&rs[j]);
+                jo = __ldg(&ri[j]);
+            }
+        };
+        // the unit's chunk loop; `exact` redoes it deciding in-band pairs with the reference test
+        int32_t qcount = 0;
+        bool unc = false;
+        for (int pass = 0; pass < 2; ++pass) {
+            const bool exact = pass == 1;
+            cr = 0;
+            qcount = 0;
+            float4 nxt;
+            int32_t nxt_j;
+            fetch(lane, nxt, nxt_j);
+            for (int32_t c = 0; c < nchunks; ++c) {
+                // stage candidate `lane` of this chunk: stream lane / Q, slot lane % Q
+                sm.cand[w][(lane / Q) * (Q + 1) + (lane & (Q - 1))] = nxt;
+                if (stage) sm.sj[w][c][lane] = nxt_j;
+                fetch(((c + 1) << 5) + lane, nxt, nxt_j);  // prefetch the next chunk's candidate
+                __syncwarp();
+                uint32_t m;
+                if (exact) {
+                    m = stream_mask_exact<DIM, PERIODIC, MODE>(xc, my_cand, Q, myq, qs, band) << (Q == 32 ? 0 : Q * ls);
+                } else if (Q == 32) {
+                    m = stream_mask<DIM, PERIODIC, MODE, 32>(xc, my_cand, myq, qs, band, unc);
+                } else if (Q == 16) {
+                    m = stream_mask<DIM, PERIODIC, MODE, 16>(xc, my_cand, myq, qs, band, unc) << (16 * ls);
+                } else {
+                    m = stream_mask<DIM, PERIODIC, MODE, 8>(xc, my_cand, myq, qs, band, unc) << (8 * ls);
+                }
+                if (Q <= 16) m |= __shfl_xor_sync(0xffffffffu, m, 16);
+                if (Q == 8) m |= __shfl_xor_sync(0xffffffffu, m, 8);
+                if (lane < nb) {
+                    qcount += __popc(m);
+                    if (stage) sm.mask[w][lane * kMaskStride + c] = m;
+                }
+                __syncwarp();
+            }
+            if (exact || !__any_sync(0xffffffffu, unc)) break;
+        }
+        if (active) a.counts[qorig] = qcount;
+        bool staged = false;
+        if (stage) {
+            // record: [nchunks] [masks: nb x nchunks, query-major] [candidates: nchunks x 32]
+            const int64_t words = 1 + (int64_t)nb * nchunks + 32 * (int64_t)nchunks;
+            unsigned long long base = 0;
+            if (lane == 0) base = atomicAdd(a.cursor, (unsigned long long)words);
+            base = __shfl_sync(0xffffffffu, base, 0);
+            staged = base + (unsigned long long)words <= (unsigned long long)a.stage_cap;
+            if (staged) {
+                int32_t* r = a.stage + base;
+                if (lane == 0) {
+                    r[0] = nchunks;
+                    a.rec[unit] = (int32_t)base;
+                }
+                __syncwarp();
+                for (int q = 0; q < nb; ++q)
+                    if (lane < nchunks) r[1 + q * nchunks + lane] = sm.mask[w][q * kMaskStride + lane];
+                int32_t* rj = r + 1 + nb * nchunks;
+                for (int32_t c = 0; c < nchunks; ++c) rj[c * 32 + lane] = sm.sj[w][c][lane];
+            }
+        }
+        if (!staged && lane == 0) {
+            int32_t f = atomicAdd(a.num_flagged, 1);
+            a.flagged[f] = unit;
+        }
+        __syncwarp();
+    }
+}
+
+// Pass 2 for flagged units: walk again and write the pairs straight to their slots.
+template <int DIM, bool PERIODIC, int MODE>
+__global__ void __launch_bounds__(kWalkWarps * 32) walk_emit_kernel(WalkArgs a) {
     if (a.g->error) return;
     __shared__ int32_t s_pre[kWalkWarps][33];
     __shared__ int32_t s_beg[kWalkWarps][32];
     __shared__ float4 s_q[kWalkWarps][32];
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
     const unsigned lt = (1u << lane) - 1u;
-    const int S = DIM == 1 ? 3 : (DIM == 2 ? 9 : 27);
-    const bool exact_all = a.g->always_exact != 0;
-    const int mode = a.sp.mode;
+    constexpr int S = DIM == 1 ? 3 : (DIM == 2 ? 9 : 27);
     const ExactCtx xc = exact_ctx(a.sp);
-    const int32_t nunits = *a.num_units;
+    const float qmax = a.qp->qmax;
+    const bool exact_all = a.qp->exact_all != 0;
+    const int32_t nlist = *a.num_list;
+    const float4 nan4 = make_float4(__int_as_float(0x7fc00000), 0.f, 0.f, 0.f);
     for (;;) {
-        int32_t unit = 0;
-        if (lane == 0) unit = atomicAdd(&a.work[EMIT ? 1 : 0], 1);
-        unit = __shfl_sync(0xffffffffu, unit, 0);
-        if (unit >= nunits) break;
+        int32_t li = 0;
+        if (lane == 0) li = atomicAdd(&a.work[1], 1);
+        li = __shfl_sync(0xffffffffu, li, 0);
+        if (li >= nlist) break;
+        const int32_t unit = a.unit_list[li];
         const int32_t grp = a.unit_group[unit];
         const int32_t t0 = a.unit_t0[unit];
-        const int32_t nb = min(kUnit, a.group_start[grp + 1] - t0);
-        int32_t gc[3] = {a.group_coords[3 * grp], a.group_coords[3 * grp + 1], a.group_coords[3 * grp + 2]};
-        // stencil lookups, one lane per stencil cell
+        const int32_t nb = min(32, a.group_start[grp + 1] - t0);
+        const int32_t gc[3] = {a.group_coords[3 * grp], a.group_coords[3 * grp + 1], a.group_coords[3 * grp + 2]};
         int32_t beg = 0, cnt = 0;
         if (lane < S) stencil_lookup(a, gc, lane, beg, cnt);
-        int32_t inc = warp_inclusive_scan(cnt);
+        const int32_t inc = warp_inclusive_scan(cnt);
         s_pre[w][lane + 1] = inc;
         if (lane == 0) s_pre[w][0] = 0;
         s_beg[w][lane] = beg;
         const int32_t M = __shfl_sync(0xffffffffu, inc, 31);
-        // queries of this unit
-        bool active = false;
         int32_t qorig = 0;
-        float4 qv = make_float4(__int_as_float(0x7fc00000), 0.f, 0.f, 0.f);
+        float4 qv = nan4;
+        int64_t obase = 0;
         if (lane < nb) {
             const int32_t t = t0 + lane;
             qv = a.qsorted[t];
             qorig = a.qsidx[t];
             int32_t qc[3];
             point_cell(a.sp, a.g, qv, qc);
-            active = same_cell<DIM>(qc, gc);
-            if (!active && !EMIT) {  // own cell differs from the group's (aliasing or wrap rounding): serial path
-                int32_t k = atomicAdd(a.num_stray, 1);
-                a.stray[k] = t;
-            }
+            if (same_cell<DIM>(qc, gc)) obase = a.offsets[qorig];
+            else qv = nan4;  // stray: written by the serial kernel
         }
         s_q[w][lane] = qv;
-        const unsigned amask = __ballot_sync(0xffffffffu, active);
-        int64_t obase = 0;
-        if (EMIT && active) obase = a.offsets[qorig];
-        int32_t qcount = 0;
         __syncwarp();
         for (int32_t base = 0; base < M; base += 32) {
             const int32_t k = base + lane;
-            const bool valid = k < M;
-            float4 cv = make_float4(__int_as_float(0x7fc00000), 0.f, 0.f, 0.f);
+            float4 cv = nan4;
             int32_t j = 0;
-            if (valid) {
-                // stencil cell holding candidate k: last r with pre[r] <= k
-                int lo = 0, hi = S;  // pre[lo] <= k < pre[hi]
-                while (hi - lo > 1) {
-                    int mid = (lo + hi) >> 1;
-                    if (s_pre[w][mid] <= k) lo = mid; else hi = mid;
-                }
-                j = s_beg[w][lo] + (k - s_pre[w][lo]);
+            if (k < M) {
+                j = cand_index(s_pre[w], s_beg[w], S, k);
                 cv = __ldg(&a.rsorted[j]);
             }
-            unsigned todo = amask;
-            while (todo) {
-                const int qi = __ffs(todo) - 1;
-                todo &= todo - 1;
+            const int64_t jorig = (int64_t)__ldg(&a.rsidx[j]);
+            const float cw = cand_share<MODE>(cv.w);
+            const float band = exact_all ? __int_as_float(0x7f800000) : cand_band<MODE>(cw, qmax);
+            for (int qi = 0; qi < nb; ++qi) {
                 const float4 q = s_q[w][qi];
-                const float thr = mode_threshold(mode, q.w, cv.w);
                 bool in, unc;
-                fast_pair_test<DIM, PERIODIC>(a.sp, q, thr, cv, in, unc);
-                unc = (unc || exact_all) && valid;
-                if (__any_sync(0xffffffffu, unc)) {
-                    if (unc) in = exact_pair_test(xc, q, q.w, cv, cv.w);
-                }
-                in = in && valid;
-                const unsigned b = __ballot_sync(0xffffffffu, in);
-                if (EMIT) {
-                    const int64_t qb = __shfl_sync(0xffffffffu, obase, qi);
-                    const int32_t qrow = __shfl_sync(0xffffffffu, qorig, qi);
-                    if (in) {
-                        const int64_t pos = qb + __popc(b & lt);
-                        a.col_out[pos] = (int64_t)__ldg(&a.rsidx[j]);
+                lean_test<DIM, PERIODIC, MODE>(a.sp, q, cv, cw, band, in, unc);
+                const uint32_t ub = __ballot_sync(0xffffffffu, unc);
+                if (ub) in = unc ? exact_pair_test(xc, q, q.w, cv, cv.w) : in;
+                const uint32_t b = __ballot_sync(0xffffffffu, in);
+                const int64_t qb = __shfl_sync(0xffffffffu, obase, qi);
+                const int32_t qrow = __shfl_sync(0xffffffffu, qorig, qi);
+                if (in) {
+                    const int64_t pos = qb + __popc(b & lt);
+                    if (pos < a.out_cap) {
+                        a.col_out[pos] = jorig;
                         if (a.row_out) a.row_out[pos] = (int64_t)qrow;
                     }
-                    if (lane == qi) obase += __popc(b);
-                } else {
-                    if (lane == qi) qcount += __popc(b);
+                }
+                if (lane == qi) obase += __popc(b);
+            }
+        }
+        __syncwarp();
+    }
+}
+
+// Pass 2 for staged units: expand each unit's record into its queries' CSR/COO slots, one warp
+// per unit.  The warp stages the unit's mask block in shared memory; lane q expands query q's hit
+// bits into a shared output table (source chunk and bit of each of the unit's outputs, in output
+// order); then lanes = output positions read the table and write consecutive slots.  A unit with
+// more than kExpandTab outputs locates each output by binary searches over the prefixes instead.
+constexpr int kExpandWarps = 8;
+constexpr int kExpandTab = 2048;
+struct ExpandSmem {
+    uint16_t tab[kExpandWarps][kExpandTab];        // (query << 10) | (chunk << 5) | bit, in output order
+    int32_t qpre[kExpandWarps][33];                // exclusive output prefix over queries
+    int64_t qoff[kExpandWarps][32];
+    int32_t qrow[kExpandWarps][32];
+};
+
+__global__ void __launch_bounds__(kExpandWarps * 32) expand_records_kernel(
+    const int32_t* __restrict__ stage, const int32_t* __restrict__ rec, const int32_t* __restrict__ num_units,
+    const int32_t* __restrict__ unit_t0, const int32_t* __restrict__ unit_group,
+    const int32_t* __restrict__ group_start, const int32_t* __restrict__ qsidx, const int64_t* __restrict__ offsets,
+    int64_t* __restrict__ row_out, int64_t* __restrict__ col_out, int64_t out_cap) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    ExpandSmem& sm = *reinterpret_cast<ExpandSmem*>(smem_raw);
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    const int32_t nu = *num_units;
+    const int64_t warps = (int64_t)gridDim.x * kExpandWarps;
+    uint16_t* tab = sm.tab[w];
+    int64_t u = (int64_t)blockIdx.x * kExpandWarps + w;
+    int32_t r0n = u < nu ? rec[u] : -1;
+    int32_t t0n = u < nu ? unit_t0[u] : 0;
+    int32_t gn = u < nu ? unit_group[u] : 0;
+    for (; u < nu; u += warps) {
+        const int32_t r0 = r0n, t0 = t0n, grp = gn;
+        if (u + warps < nu) {  // the next unit's header, ahead of its use
+            r0n = rec[u + warps];
+            t0n = unit_t0[u + warps];
+            gn = unit_group[u + warps];
+        }
+        if (r0 < 0) continue;  // re-tested by the emit walk
+        const int32_t* r = stage + r0;
+        const int32_t nchunks = r[0];
+        if (nchunks <= 0) continue;  // no candidates, no outputs
+        const int32_t nb = min(32, group_start[grp + 1] - t0);
+        const int32_t nm = nb * nchunks;
+        const uint32_t* mk = reinterpret_cast<const uint32_t*>(r + 1);  // [query][chunk]
+        const int32_t* cands = r + 1 + nm;                               // [chunk][32]
+        int32_t total = 0;
+        if (lane < nb) {
+            const int32_t row = qsidx[t0 + lane];
+            sm.qrow[w][lane] = row;
+            sm.qoff[w][lane] = offsets[row];
+            for (int c = 0; c < nchunks; ++c) total += __popc(mk[lane * nchunks + c]);
+        }
+        const int32_t qinc = warp_inclusive_scan(total);
+        sm.qpre[w][lane + 1] = qinc;
+        if (lane == 0) sm.qpre[w][0] = 0;
+        const int32_t n = __shfl_sync(0xffffffffu, qinc, 31);
+        if (n <= kExpandTab) {
+            // lanes over (query, chunk) pairs in output order; each expands its few hit bits
+            int32_t carry = 0;
+            int pq = 0, pc = lane;  // pair (query, chunk) of p = base + lane, advanced without division
+            while (pc >= nchunks) { pc -= nchunks; ++pq; }
+            for (int32_t base = 0; base < nm; base += 32) {
+                const int32_t p = base + lane;
+                uint32_t m = p < nm ? mk[p] : 0u;
+                const int32_t cnt = __popc(m);
+                const int32_t inc = warp_inclusive_scan(cnt);
+                int32_t k = carry + inc - cnt;
+                carry += __shfl_sync(0xffffffffu, inc, 31);
+                const int32_t tag = (pq << 10) | (pc << 5);
+                while (m) {
+                    const int bit = __ffs(m) - 1;
+                    m &= m - 1;
+                    tab[k++] = (uint16_t)(tag | bit);
+                }
+                pc += 32;
+                while (pc >= nchunks) { pc -= nchunks; ++pq; }
+            }
+            __syncwarp();
+#pragma unroll 4
+            for (int32_t o = lane; o < n; o += 32) {
+                const int32_t v = tab[o];
+                const int q = v >> 10;
+                const int64_t pos = sm.qoff[w][q] + (o - sm.qpre[w][q]);
+                if (pos < out_cap) {
+                    col_out[pos] = (int64_t)cands[v & 0x3ff];
+                    if (row_out) row_out[pos] = (int64_t)sm.qrow[w][q];
+                }
+            }
+        } else {
+            __syncwarp();
+            for (int32_t o = lane; o < n; o += 32) {
+                int lo = 0, hi = nb;  // query: qpre[lo] <= o < qpre[hi]
+                while (hi - lo > 1) {
+                    const int mid = (lo + hi) >> 1;
+                    if (sm.qpre[w][mid] <= o) lo = mid; else hi = mid;
+                }
+                const int q = lo;
+                int32_t tq = o - sm.qpre[w][q];
+                int c = 0;  // chunk holding the query's tq-th hit (tq < hits of q, so c < nchunks)
+                for (; c < nchunks; ++c) {
+                    const int32_t pcnt = __popc(mk[q * nchunks + c]);
+                    if (tq < pcnt) break;
+                    tq -= pcnt;
+                }
+                if (c >= nchunks) continue;
+                const int bit = __fns(mk[q * nchunks + c], 0, tq + 1);
+                const int64_t pos = sm.qoff[w][q] + (o - sm.qpre[w][q]);
+                if (pos < out_cap) {
+                    col_out[pos] = (int64_t)cands[c * 32 + bit];
+                    if (row_out) row_out[pos] = (int64_t)sm.qrow[w][q];
                 }
             }
         }
-        if (!EMIT && active) a.counts[qorig] = qcount;
         __syncwarp();
     }
 }
@@ -629,8 +1116,10 @@ __global__ void stray_kernel(WalkArgs a) {
                 const float4 cv = a.rsorted[j];
                 if (exact_pair_test(xc, q, q.w, cv, cv.w)) {
                     if (EMIT) {
-                        a.col_out[pos] = (int64_t)a.rsidx[j];
-                        if (a.row_out) a.row_out[pos] = qorig;
+                        if (pos < a.out_cap) {
+                            a.col_out[pos] = (int64_t)a.rsidx[j];
+                            if (a.row_out) a.row_out[pos] = qorig;
+                        }
                         ++pos;
                     } else {
                         ++n;
@@ -660,11 +1149,17 @@ struct OffsetOut {
     }
 };
 
-__global__ void info_kernel(const GridParams* g, const int64_t* total, const int32_t* num_stray, int64_t* info) {
+__global__ void info_kernel(const GridParams* g, const int64_t* total, const int32_t* num_stray,
+                            const QueryParams* qp, const unsigned long long* cursor, const int32_t* num_flagged,
+                            int64_t* info) {
     info[0] = *total;
     info[1] = g->error;
     info[2] = *num_stray;
-    info[3] = g->always_exact;
+    info[3] = qp->exact_all;
+    info[4] = (int64_t)*cursor;
+    info[5] = *num_flagged;
+    info[6] = 0;
+    info[7] = 0;
 }
 
 // ------------------------------------------------------------------------------------------
@@ -719,6 +1214,7 @@ static WalkArgs make_walk(const SearchParams& sp, const Structure& S, const Scra
     memset(&a, 0, sizeof(a));
     a.sp = sp;
     a.g = S.grid;
+    a.qp = W.qparams;
     a.rsorted = S.rsorted;
     a.rsidx = S.rsidx;
     a.cell_start = S.cell_start;
@@ -733,30 +1229,65 @@ static WalkArgs make_walk(const SearchParams& sp, const Structure& S, const Scra
     a.unit_group = W.unit_group;
     a.unit_t0 = W.unit_t0;
     a.num_units = W.num_units;
+    a.unit_list = W.flagged;
+    a.num_list = W.num_flagged;
     a.work = W.work;
     a.stray = W.stray;
     a.num_stray = W.num_stray;
     a.counts = W.counts;
+    a.rec = W.rec;
+    a.flagged = W.flagged;
+    a.num_flagged = W.num_flagged;
+    a.cursor = W.cursor;
     return a;
 }
 
-template <bool EMIT>
-static cudaError_t launch_walk(const WalkArgs& a, int dim, bool periodic, int64_t nq, cudaStream_t st) {
+static int num_sms() {
     int dev = 0, nsm = 148;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+    return nsm;
+}
+
+// Dispatches a walk kernel template on (dim, any periodic dim, mode).
+template <template <int, bool, int> class K>
+static cudaError_t dispatch_walk(const WalkArgs& a, int dim, bool periodic, int mode, dim3 grid, dim3 block,
+                                 size_t smem, cudaStream_t st) {
+#define TCR_M(D, P)                                                                 \
+    switch (mode) {                                                                 \
+        case kGather: return K<D, P, kGather>::launch(a, grid, block, smem, st);    \
+        case kScatter: return K<D, P, kScatter>::launch(a, grid, block, smem, st);  \
+        case kSymmetric: return K<D, P, kSymmetric>::launch(a, grid, block, smem, st); \
+        default: return K<D, P, kSuperSymmetric>::launch(a, grid, block, smem, st); \
+    }
+    if (dim == 1) { if (periodic) { TCR_M(1, true) } else { TCR_M(1, false) } }
+    if (dim == 2) { if (periodic) { TCR_M(2, true) } else { TCR_M(2, false) } }
+    if (periodic) { TCR_M(3, true) } else { TCR_M(3, false) }
+#undef TCR_M
+}
+
+template <int D, bool P, int M>
+struct CountLaunch {
+    static cudaError_t launch(const WalkArgs& a, dim3 g, dim3 b, size_t smem, cudaStream_t st) {
+        cudaError_t e = cudaFuncSetAttribute(walk_count_kernel<D, P, M>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                             (int)smem);
+        if (e != cudaSuccess) return e;
+        walk_count_kernel<D, P, M><<<g, b, smem, st>>>(a);
+        return cudaGetLastError();
+    }
+};
+template <int D, bool P, int M>
+struct EmitLaunch {
+    static cudaError_t launch(const WalkArgs& a, dim3 g, dim3 b, size_t, cudaStream_t st) {
+        walk_emit_kernel<D, P, M><<<g, b, 0, st>>>(a);
+        return cudaGetLastError();
+    }
+};
+
+static unsigned walk_blocks(int64_t nq) {
     const int64_t max_units = (nq + kUnit - 1) / kUnit + 1;
-    unsigned blocks = (unsigned)std::max<int64_t>(1, std::min<int64_t>((int64_t)nsm * 8, (max_units + kWalkWarps - 1) / kWalkWarps));
-    dim3 grid(blocks), block(kWalkWarps * 32);
-#define TCR_WALK(D, P) walk_kernel<D, P, EMIT><<<grid, block, 0, st>>>(a)
-    if (dim == 1) { if (periodic) TCR_WALK(1, true); else TCR_WALK(1, false); }
-    else if (dim == 2) { if (periodic) TCR_WALK(2, true); else TCR_WALK(2, false); }
-    else { if (periodic) TCR_WALK(3, true); else TCR_WALK(3, false); }
-#undef TCR_WALK
-    note_launches(1);
-    stray_kernel<EMIT><<<grid_for(nq, 128, nsm * 4), 128, 0, st>>>(a);
-    note_launches(1);
-    return cudaGetLastError();
+    return (unsigned)std::max<int64_t>(1, std::min<int64_t>((int64_t)num_sms() * 12, (max_units + kWalkWarps - 1) /
+                                                                                             kWalkWarps));
 }
 
 }  // namespace tcr
@@ -816,20 +1347,22 @@ int tcr_build_structure(const tcr_search_desc* d, void* structure, int64_t struc
     grid_init_kernel<<<1, 1, 0, st>>>(S.grid, W.sort.state);
     note_launches(1);
     // computeGridSupport: which supports set hMax depends on the mode
-    const float* sa = nullptr; int64_t na = 0;
-    const float* sb = nullptr; int64_t nb = 0;
-    if (d->mode == kScatter) { sa = d->ref_sup; na = nr; }
-    else if (d->mode == kGather) { sa = d->query_sup; na = nq; }
-    else { sa = d->ref_sup; na = nr; sb = d->query_sup; nb = nq; }
-    if (na + nb > 0) support_reduce_kernel<<<grid_for(na + nb, 256), 256, 0, st>>>(sa, na, sb, nb, S.grid);
-    note_launches(1);
+    if (d->ref_sup && nr > 0) {
+        support_stats_kernel<<<grid_for(nr, 256, num_sms() * 8), 256, 0, st>>>(d->ref_sup, nr, &S.grid->ref_stats);
+        note_launches(1);
+    }
+    if (d->query_sup && nq > 0) {
+        support_stats_kernel<<<grid_for(nq, 256, num_sms() * 8), 256, 0, st>>>(d->query_sup, nq,
+                                                                                &S.grid->build_query_stats);
+        note_launches(1);
+    }
     grid_params_kernel<<<1, 1, 0, st>>>(sp, S.grid, W.sort.state);
     note_launches(1);
     TCR_CUDA(cudaMemsetAsync(S.map, 0xff, sizeof(unsigned long long) * S.map_cap, st));
     TCR_CUDA(cudaMemsetAsync(S.num_cells, 0, sizeof(int32_t), st));
     if (nr > 0) {
         pack_points_kernel<<<grid_for(nr, 256), 256, 0, st>>>(sp, S.grid, d->ref_pos, d->ref_sup, nr, 2, W.pack,
-                                                              W.sort.keys[0], W.sort.vals[0], W.sort.state);
+                                                              W.sort.keys[0], W.sort.vals[0], W.sort.state, 1);
         note_launches(1);
         TCR_CUDA(radix_sort_pairs(W.sort, nr, st));
         gather_sorted_kernel<<<grid_for(nr, 256), 256, 0, st>>>(S.grid, W.pack, W.sort.vals[0], W.sort.vals[1], W.sort.state,
@@ -846,14 +1379,17 @@ int tcr_build_structure(const tcr_search_desc* d, void* structure, int64_t struc
     return TCR_OK;
 }
 
-int tcr_count(const tcr_search_desc* d, const void* structure, void* scratch, int64_t scratch_bytes,
-              int64_t* offsets, int32_t* indptr_out, int64_t* row_entries_out, int64_t* info_out, void* stream) {
+int tcr_count(const tcr_search_desc* d, const void* structure, void* scratch, int64_t scratch_bytes, int32_t* stage,
+              int64_t stage_capacity, int64_t* offsets, int32_t* indptr_out, int64_t* row_entries_out, int64_t* info_out,
+              void* stream) {
     int rc = validate(d, false);
     if (rc) return rc;
     int64_t need_w = 0;
     carve_scratch(nullptr, d->n_query, d->n_ref, &need_w);
     if (!structure || !scratch || scratch_bytes < need_w || !offsets)
         return set_error(TCR_ERR_INVALID, "workspace too small or offsets missing");
+    if (stage_capacity < 0 || stage_capacity > 0x7fffffffLL || (stage_capacity > 0 && !stage))
+        return set_error(TCR_ERR_INVALID, "stage capacity must be in [0, 2^31) with a buffer");
     cudaStream_t st = (cudaStream_t)stream;
     const SearchParams sp = make_params(d);
     Structure S = carve_structure(const_cast<void*>(structure), d->n_ref, nullptr);
@@ -863,8 +1399,18 @@ int tcr_count(const tcr_search_desc* d, const void* structure, void* scratch, in
     TCR_CUDA(cudaMemsetAsync(W.work, 0, sizeof(int32_t) * 4, st));
     TCR_CUDA(cudaMemsetAsync(W.num_stray, 0, sizeof(int32_t), st));
     TCR_CUDA(cudaMemsetAsync(W.num_units, 0, sizeof(int32_t), st));
+    TCR_CUDA(cudaMemsetAsync(W.num_flagged, 0, sizeof(int32_t), st));
+    TCR_CUDA(cudaMemsetAsync(W.cursor, 0, sizeof(unsigned long long), st));
+    TCR_CUDA(cudaMemsetAsync(&W.qparams->stats, 0, sizeof(SupportStats), st));
+    if (d->query_sup && nq > 0) {
+        support_stats_kernel<<<grid_for(nq, 256, num_sms() * 8), 256, 0, st>>>(d->query_sup, nq, &W.qparams->stats);
+        note_launches(1);
+    }
+    query_params_kernel<<<1, 1, 0, st>>>(S.grid, d->mode, d->query_sup != nullptr, W.qparams);
+    note_launches(1);
     if (nq > 0) {
         TCR_CUDA(cudaMemsetAsync(W.counts, 0, sizeof(int32_t) * nq, st));
+        TCR_CUDA(cudaMemsetAsync(W.rec, 0xff, sizeof(int32_t) * nq, st));
         const int32_t* gstart;
         const int32_t* ngroups;
         if (self) {
@@ -879,7 +1425,7 @@ int tcr_count(const tcr_search_desc* d, const void* structure, void* scratch, in
             note_launches(1);
             pack_points_kernel<<<grid_for(nq, 256), 256, 0, st>>>(sp, S.grid, d->query_pos, d->query_sup, nq, 1,
                                                                   W.pack, W.sort.keys[0], W.sort.vals[0],
-                                                                  W.sort.state);
+                                                                  W.sort.state, 0);
             note_launches(1);
             TCR_CUDA(radix_sort_pairs(W.sort, nq, st));
             gather_sorted_kernel<<<grid_for(nq, 256), 256, 0, st>>>(S.grid, W.pack, W.sort.vals[0], W.sort.vals[1],
@@ -894,22 +1440,31 @@ int tcr_count(const tcr_search_desc* d, const void* structure, void* scratch, in
             ngroups = W.num_qgroups;
         }
         BoundedUnitCountIn ui{gstart, ngroups};
-        BoundedUnitOut uo{gstart, ngroups, W.unit_group, W.unit_t0};
+        BoundedUnitOut uo{gstart, ngroups, W.unit_group, W.unit_t0, W.query_unit};
         TCR_CUDA(device_exclusive_scan<int32_t>(ui, uo, nq, W.scan_tiles32, W.num_units, st));
         WalkArgs a = make_walk(sp, S, W, self);
-        TCR_CUDA(launch_walk<false>(a, d->dim, d->periodic_mask != 0, nq, st));
+        a.stage = stage;
+        a.stage_cap = stage_capacity;
+        // identical positions: every query sits in its group's cell
+        a.no_stray_check = self && d->periodic_mask == 0 && d->query_pos == d->ref_pos;
+        TCR_CUDA(dispatch_walk<CountLaunch>(a, d->dim, d->periodic_mask != 0, d->mode, dim3(walk_blocks(nq)),
+                                            dim3(kWalkWarps * 32), sizeof(WalkSmem), st));
+        note_launches(1);
+        stray_kernel<false><<<grid_for(nq, 128, num_sms() * 4), 128, 0, st>>>(a);
+        note_launches(1);
     }
     CountIn ci{W.counts, nq};
     OffsetOut oo{nq, offsets, indptr_out, row_entries_out};
     TCR_CUDA(device_exclusive_scan<int64_t>(ci, oo, nq + 1, W.scan_tiles64, W.total, st));
-    info_kernel<<<1, 1, 0, st>>>(S.grid, W.total, W.num_stray, W.info);
+    info_kernel<<<1, 1, 0, st>>>(S.grid, W.total, W.num_stray, W.qparams, W.cursor, W.num_flagged, W.info);
     note_launches(1);
-    if (info_out) TCR_CUDA(cudaMemcpyAsync(info_out, W.info, 4 * sizeof(int64_t), cudaMemcpyDeviceToHost, st));
+    if (info_out) TCR_CUDA(cudaMemcpyAsync(info_out, W.info, 8 * sizeof(int64_t), cudaMemcpyDeviceToHost, st));
     return TCR_OK;
 }
 
 int tcr_emit(const tcr_search_desc* d, const void* structure, void* scratch, int64_t scratch_bytes,
-             const int64_t* offsets, int64_t* row_out, int64_t* col_out, void* stream) {
+             const int32_t* stage, const int64_t* offsets, int64_t* row_out, int64_t* col_out, int64_t out_capacity,
+             void* stream) {
     int rc = validate(d, false);
     if (rc) return rc;
     int64_t need_w = 0;
@@ -926,9 +1481,25 @@ int tcr_emit(const tcr_search_desc* d, const void* structure, void* scratch, int
     a.offsets = offsets;
     a.row_out = row_out;
     a.col_out = col_out;
-    // the count pass already collected the stray queries; the emit walk must not re-append them
+    a.out_cap = out_capacity;
+    if (out_capacity < 0 || (out_capacity > 0 && !col_out)) return set_error(TCR_ERR_INVALID, "bad output buffer");
+    if (stage) {
+        const int nsm = num_sms();
+        const unsigned blocks = (unsigned)std::max<int64_t>(1, std::min<int64_t>((int64_t)nsm * 16, (nq / 16 + kExpandWarps) / kExpandWarps));
+        const int32_t* group_start = d->self_search ? S.cell_start : W.qgroup_start;
+        TCR_CUDA(cudaFuncSetAttribute(expand_records_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      (int)sizeof(ExpandSmem)));
+        expand_records_kernel<<<blocks, kExpandWarps * 32, sizeof(ExpandSmem), st>>>(
+            stage, W.rec, W.num_units, W.unit_t0, W.unit_group, group_start, W.qsidx, offsets, row_out, col_out,
+            out_capacity);
+        note_launches(1);
+    }
     TCR_CUDA(cudaMemsetAsync(W.work + 1, 0, sizeof(int32_t), st));
-    TCR_CUDA(launch_walk<true>(a, d->dim, d->periodic_mask != 0, nq, st));
+    TCR_CUDA(dispatch_walk<EmitLaunch>(a, d->dim, d->periodic_mask != 0, d->mode, dim3(walk_blocks(nq)),
+                                       dim3(kWalkWarps * 32), 0, st));
+    note_launches(1);
+    stray_kernel<true><<<grid_for(nq, 128, num_sms() * 4), 128, 0, st>>>(a);
+    note_launches(1);
     return TCR_OK;
 }
 
@@ -1002,8 +1573,8 @@ extern "C" int tcr_search_noalloc(const tcr_search_desc* d, int64_t* offsets, in
     // previous call left in the array do not matter.
     rc = tcr_build_structure(d, structure, s_bytes, scratch, w_bytes, stream);
     if (rc) return rc;
-    int64_t info[4] = {0, 0, 0, 0};
-    rc = tcr_count(d, structure, scratch, w_bytes, offsets, indptr_out, row_entries_out, info, stream);
+    int64_t info[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+    rc = tcr_count(d, structure, scratch, w_bytes, nullptr, 0, offsets, indptr_out, row_entries_out, info, stream);
     if (rc) return rc;
     TCR_CUDA(cudaStreamSynchronize((cudaStream_t)stream));
     if (total_out) *total_out = info[0];
@@ -1012,5 +1583,5 @@ extern "C" int tcr_search_noalloc(const tcr_search_desc* d, int64_t* offsets, in
         return set_error(TCR_ERR_INVALID, "tcr_search_noalloc: %lld pairs do not fit the %lld-entry output",
                          (long long)info[0], (long long)pair_capacity);
     if (info[0] == 0) return TCR_OK;
-    return tcr_emit(d, structure, scratch, w_bytes, offsets, row_out, col_out, stream);
+    return tcr_emit(d, structure, scratch, w_bytes, nullptr, offsets, row_out, col_out, pair_capacity, stream);
 }

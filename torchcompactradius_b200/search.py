@@ -1,9 +1,10 @@
 """Host orchestration of the CUDA search through the C ABI, and the reusable structure.
 
 One search is three C-ABI calls on torch's current stream -- ``tcr_build_structure``,
-``tcr_count`` and ``tcr_emit`` -- with one host synchronisation between the last two, to
-learn the pair count and allocate the output (the reference synchronises at the same point,
-compactHashing/cppSearch.py:89).  Device memory comes from torch's caching allocator.
+``tcr_count`` and ``tcr_emit`` -- enqueued back to back into buffers sized from the previous
+search's pairs per query; the host synchronises once at the end to learn the pair count (the
+reference synchronises between count and build, compactHashing/cppSearch.py:89) and re-runs
+only the emit when the estimate was short.  Device memory comes from torch's caching allocator.
 """
 import ctypes
 import threading
@@ -15,11 +16,16 @@ from . import _lib
 
 _tls = threading.local()
 
+# Pairs and staging words per query of the previous search: they size the output and the staging
+# list of the next one.
+_pairs_per_query = [64.0]
+_stage_per_query = [64.0]
+
 
 def _info_buffer():
     buf = getattr(_tls, "info", None)
     if buf is None:
-        buf = torch.zeros(4, dtype=torch.int64, pin_memory=torch.cuda.is_available())
+        buf = torch.zeros(8, dtype=torch.int64, pin_memory=torch.cuda.is_available())
         _tls.info = buf
     return buf
 
@@ -253,21 +259,36 @@ def compact_search(xq, hq, xr, hr, domain_lo, domain_hi, mask, mode, L, fmt, sel
         indptr = torch.empty(nq + 1, dtype=torch.int32, device=device)
         rowEntries = torch.empty(nq, dtype=torch.int64, device=device)
     info = _info_buffer()
+    # One estimate sizes both the staging list and the output, so count and emit are enqueued
+    # back to back and the host waits only once, at the end.
+    cap = int(min(0x7fffffff, _pairs_per_query[0] * 1.25 * nq + 4096))
+    stage_cap = int(min(0x7fffffff, _stage_per_query[0] * 1.1 * nq + 65536))
+    stage = torch.empty(stage_cap, dtype=torch.int32, device=device)
+    col = torch.empty(cap, dtype=torch.int64, device=device)
+    row = torch.empty(cap, dtype=torch.int64, device=device) if fmt == "coo" else None
     mark("count")
-    _lib.check(lib.tcr_count(ctypes.byref(desc), _ptr(sbuf), _ptr(scratch), w_bytes, _ptr(offsets), _ptr(indptr),
-                             _ptr(rowEntries), ctypes.c_void_p(info.data_ptr()), sptr), "tcr_count")
+    _lib.check(lib.tcr_count(ctypes.byref(desc), _ptr(sbuf), _ptr(scratch), w_bytes, _ptr(stage), stage_cap,
+                             _ptr(offsets), _ptr(indptr), _ptr(rowEntries), ctypes.c_void_p(info.data_ptr()), sptr),
+               "tcr_count")
     mark("count", True)
+    mark("emit")
+    _lib.check(lib.tcr_emit(ctypes.byref(desc), _ptr(sbuf), _ptr(scratch), w_bytes, _ptr(stage), _ptr(offsets),
+                            _ptr(row), _ptr(col), cap, sptr), "tcr_emit")
+    mark("emit", True)
     stream.synchronize()
     _check_info(info)
     total = int(info[0])
+    if nq:
+        _pairs_per_query[0] = max(total / nq, 1.0)
+        _stage_per_query[0] = max(int(info[4]) / nq, 1.0)
     if fmt == "csr" and total > 0x7fffffff:
         raise ValueError(f"{total} pairs do not fit the int32 indptr of SparseCSR")
-    col = torch.empty(total, dtype=torch.int64, device=device)
-    row = torch.empty(total, dtype=torch.int64, device=device) if fmt == "coo" else None
-    if total:
-        mark("emit")
-        _lib.check(lib.tcr_emit(ctypes.byref(desc), _ptr(sbuf), _ptr(scratch), w_bytes, _ptr(offsets), _ptr(row),
-                                _ptr(col), sptr), "tcr_emit")
-        mark("emit", True)
+    if total > cap:  # the estimate was short: emit again into an exact buffer (the count is kept)
+        col = torch.empty(total, dtype=torch.int64, device=device)
+        row = torch.empty(total, dtype=torch.int64, device=device) if fmt == "coo" else None
+        _lib.check(lib.tcr_emit(ctypes.byref(desc), _ptr(sbuf), _ptr(scratch), w_bytes, _ptr(stage), _ptr(offsets),
+                                _ptr(row), _ptr(col), total, sptr), "tcr_emit")
+    col = col[:total]
+    row = row[:total] if row is not None else None
     out = (row, col) if fmt == "coo" else (col, indptr, rowEntries)
     return out, structure
