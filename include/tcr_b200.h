@@ -20,7 +20,7 @@
 extern "C" {
 #endif
 
-#define TCR_ABI_VERSION 4
+#define TCR_ABI_VERSION 5
 
 #define TCR_OK 0
 #define TCR_ERR_INVALID (-1) /* bad argument or workspace too small */
@@ -51,6 +51,15 @@ typedef struct tcr_search_desc {
     const float* query_sup;  /* device [n_query]; may be NULL for TCR_SCATTER */
     const float* ref_pos;    /* device [n_ref*dim] */
     const float* ref_sup;    /* device [n_ref]; may be NULL for TCR_GATHER */
+    /* Optional extensions (all zero / NULL: the reference's compact search). */
+    const int32_t* query_ids; /* device [n_query]: row index written for local query q (subset searches) */
+    const int32_t* ref_ids;   /* device [n_ref]: column index written for local reference j */
+    float hcell[3];           /* > 0: per-dimension cell sizes to use instead of the reference's compute_h */
+    int32_t clamped_grid;     /* 1: exact grid semantics for caller-chosen cells (multi-level search):
+                                 cell coordinates clamped into [0, count), stencil cells outside the grid
+                                 skipped, wrapped stencil cells on periodic dims with < 3 cells visited
+                                 once (the reference visits them twice and reports those pairs twice) */
+    int32_t reserved;
 } tcr_search_desc;
 
 /* Message of the last failing call on this thread. */
@@ -76,7 +85,7 @@ int tcr_search_sizes(int64_t n_query, int64_t n_ref, int32_t dim, int64_t* struc
  * CompactHashMap, datastructure.py:8-31, are derived from them).  Host-only.  offsets[k] is the
  * byte offset of field k (TCR_STRUCT_*), except offsets[TCR_STRUCT_MAP_CAPACITY], which is the
  * number of 64-bit slots of the linear-index map.  Field contents:
- *   GRID          float hmax, float hCell, int32 cellCount[3], int32 exact_only, int32 error, ...
+ *   GRID          float hmax, float hCell, float hcell_d[3], int32 cellCount[3], int32 exact_only, ...
  *   NUM_CELLS     int32 number of occupied cells C
  *   SORTED_POINTS float4 [n_ref] wrapped reference positions in cell order, .w = support
  *   SORT_INDEX    int32 [n_ref] original index of each sorted point

@@ -33,7 +33,7 @@ def test_library_exports_every_declared_symbol():
 def test_descriptor_layout_matches_library():
     from torchcompactradius_b200 import _lib
     assert ctypes.sizeof(_lib.SearchDesc) == _lib.load().tcr_desc_bytes()
-    assert _lib.load().tcr_version() == 4
+    assert _lib.load().tcr_version() == 5
 
 
 def test_sizes_and_layout_are_consistent():

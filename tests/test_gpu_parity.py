@@ -166,3 +166,70 @@ def test_full_size_3d_1m_symmetric_csr_matches_oracle():
     P = _check_vs_oracle(pos, sup, None, None, np.array([-1] * 3, np.float32), np.array([1] * 3, np.float32),
                          np.array([False] * 3), "symmetric")
     assert P == 51798992  # the reference's own count for this input (measured with its CPU operators)
+
+
+# ---------------------------------------------------------------- multi-level cells ----------
+def _mlm_vs_brute_force(x, hx, y, hy, dmin, dmax, per, mode, fmt="csr"):
+    import torchcompactradius_b200 as tcr
+    bf = compact.brute_force(x, hx, y, hy, dmin, dmax, per, mode)
+    adj = gpu_search(x, hx, y, hy, dmin, dmax, per, mode, 4096, fmt)  # compact, for the record
+    t = lambda a: None if a is None else torch.as_tensor(np.asarray(a)).cuda()
+    dom = tcr.DomainDescription(torch.tensor(np.asarray(dmin, np.float32)), torch.tensor(np.asarray(dmax, np.float32)),
+                                torch.tensor(np.asarray(per, bool)), len(dmin))
+    m = tcr.radiusSearch(tcr.PointCloud(t(x), t(hx)), None if y is None else tcr.PointCloud(t(y), t(hy)), mode=mode,
+                         domain=dom, algorithm="mlm", format=fmt)
+    if fmt == "csr":
+        r, c = csr_rows(m)
+        np.testing.assert_array_equal(m.rowEntries.cpu().numpy(), bf.counts)
+        np.testing.assert_array_equal(m.indptr.cpu().numpy().astype(np.int64), bf.offsets)
+    else:
+        r, c = coo_arrays(m)
+    assert cases.pair_sha(r, c) == cases.pair_sha(bf.row, bf.col)
+    return len(c)
+
+
+def _adaptive_cloud(seed, n, dim=3, blobs=3, ratio=4.0):
+    """Blob cores (small supports) in a uniform background (supports up to `ratio` x larger)."""
+    rng = np.random.default_rng(seed)
+    nb = int(0.7 * n)
+    centres = rng.uniform(-0.6, 0.6, (blobs, dim))
+    x = np.concatenate([centres[rng.integers(0, blobs, nb)] + 0.1 * rng.standard_normal((nb, dim)),
+                        rng.uniform(-1, 1, (n - nb, dim))]).astype(np.float32)
+    x = np.clip(x, -0.999, 0.999).astype(np.float32)
+    d2 = np.min(((x[:, None, :] - centres[None]) ** 2).sum(-1), 1)
+    hmax = 0.12 if dim == 3 else 0.05
+    h = (hmax * np.clip(np.sqrt(d2) / 0.3, 1 / ratio, 1.0)).astype(np.float32)
+    return x, h
+
+
+@pytest.mark.parametrize("mode", cases.MODES)
+@pytest.mark.parametrize("per", [[False, False, False], [True, False, False], [True, True, True]])
+def test_multilevel_exact_on_adaptive_cloud(mode, per):
+    x, h = _adaptive_cloud(41, 12000)
+    assert _mlm_vs_brute_force(x, h, None, None, np.full(3, -1, np.float32), np.full(3, 1, np.float32),
+                               np.array(per), mode) > 0
+
+
+@pytest.mark.parametrize("mode", cases.MODES)
+def test_multilevel_distinct_clouds_2d_coo(mode):
+    x, h = _adaptive_cloud(42, 6000, dim=2)
+    y, hy = _adaptive_cloud(43, 8000, dim=2)
+    assert _mlm_vs_brute_force(x, h, y, hy, np.full(2, -1, np.float32), np.full(2, 1, np.float32),
+                               np.array([True, False]), mode, "coo") > 0
+
+
+def test_multilevel_matches_compact_where_compact_is_exact():
+    # 3D 1M-style uniform cloud with +-10% supports: one or two levels, no periodic seam
+    x, hx, _, _, dmin, dmax, per = cases.random_case(seed=12, dim=3, n=60000, nref=None, hscale=0.05,
+                                                     extent=[2.0] * 3, periodic=[False] * 3)
+    assert _mlm_vs_brute_force(x, hx, None, None, dmin, dmax, per, "symmetric") > 0
+
+
+def test_multilevel_wide_support_and_tiny_periodic_box():
+    # fewer than 3 cells along periodic dims: the clamped grid visits each wrapped cell once
+    rng = np.random.default_rng(9)
+    x = rng.uniform(0, 1, (3000, 2)).astype(np.float32)
+    h = rng.uniform(0.05, 0.45, 3000).astype(np.float32)
+    for mode in cases.MODES:
+        _mlm_vs_brute_force(x, h, None, None, np.zeros(2, np.float32), np.ones(2, np.float32),
+                            np.array([True, True]), mode)

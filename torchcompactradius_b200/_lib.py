@@ -33,6 +33,11 @@ class SearchDesc(ctypes.Structure):
         ("query_sup", ctypes.c_void_p),
         ("ref_pos", ctypes.c_void_p),
         ("ref_sup", ctypes.c_void_p),
+        ("query_ids", ctypes.c_void_p),
+        ("ref_ids", ctypes.c_void_p),
+        ("hcell", ctypes.c_float * 3),
+        ("clamped_grid", ctypes.c_int32),
+        ("reserved", ctypes.c_int32),
     ]
 
 

@@ -40,6 +40,9 @@ struct SearchParams {
     float ext[3];            // fl(dmax - dmin), as the reference computes it
     int64_t n_query;
     int64_t n_ref;
+    float hcell_override[3];  // > 0: use these per-dimension cell sizes instead of compute_h
+    int32_t dedupe;           // clamped grid (multi-level): clamp cells, skip outside cells, no repeats
+    int32_t pad;
 };
 
 // Reduction record over one set of supports.
@@ -51,8 +54,9 @@ struct SupportStats {
 // Device-computed grid description (one record in device memory).
 struct GridParams {
     float hmax;              // computeGridSupport result
-    float hcell;             // compute_h result
-    int32_t count[3];        // ceil(ext / hcell) as int32
+    float hcell;             // compute_h result (the reference's single cell size)
+    float hcell_d[3];        // per-dimension cell size actually used (all hcell unless overridden)
+    int32_t count[3];        // ceil(ext / hcell_d) as int32
     int32_t always_exact;    // 1: some support outside [1e-18, 1e18] or non-finite: exact test always
     int32_t error;           // nonzero: invalid grid (e.g. zero cells on a periodic dim)
     int32_t out_of_grid;     // some reference point's cell lies outside [0, count) (linear indices may alias)

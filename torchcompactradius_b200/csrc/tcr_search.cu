@@ -275,11 +275,35 @@ __global__ void grid_params_kernel(SearchParams sp, GridParams* g, SortState* st
     }
     g->hmax = hmax;
     g->hcell = hc;
-    for (int d = 0; d < 3; ++d) g->count[d] = d < sp.dim ? (int32_t)ceilf(__fdiv_rn(ext[d], hc)) : 1;
+    if (sp.hcell_override[0] > 0.0f) {  // caller-chosen grid (multi-level search)
+        hc = sp.hcell_override[0];
+        for (int d = 0; d < 3; ++d) {
+            g->hcell_d[d] = d < sp.dim ? sp.hcell_override[d] : 1.0f;
+            hc = fminf(hc, g->hcell_d[d]);
+        }
+        for (int d = 0; d < 3; ++d) {
+            if (d >= sp.dim) { g->count[d] = 1; continue; }
+            const float r = __fdiv_rn(ext[d], g->hcell_d[d]);
+            // periodic dims of a clamped grid hold a whole number of cells (ext / n each); rounding
+            // must not add a sliver cell at the seam
+            g->count[d] = (sp.dedupe && ((sp.periodic_mask >> d) & 1)) ? max(1, (int32_t)rintf(r))
+                                                                         : (int32_t)ceilf(r);
+        }
+    } else {
+        for (int d = 0; d < 3; ++d) {
+            g->hcell_d[d] = hc;
+            g->count[d] = d < sp.dim ? (int32_t)ceilf(__fdiv_rn(ext[d], hc)) : 1;
+        }
+    }
     g->always_exact = ((sp.mode != kGather && g->ref_stats.bad) || (sp.mode != kScatter && g->build_query_stats.bad))
                           ? 1 : 0;
     int err = 0;
     if (!(hc > 0.0f) || !isfinite(hc)) err = 1;  // no valid grid (support larger than the domain, NaN, ...)
+    if (sp.dedupe) {  // clamped grid: linear indices must not wrap
+        double cells = 1.0;
+        for (int d = 0; d < sp.dim; ++d) cells *= (double)max(g->count[d], 1);
+        if (cells >= 2147483647.0) err = 1;
+    }
     for (int d = 0; d < sp.dim; ++d)
         if (((sp.periodic_mask >> d) & 1) && g->count[d] <= 0) err = 1;
     g->error = err;
@@ -306,10 +330,11 @@ __device__ __forceinline__ float4 wrap_point(const SearchParams& sp, float4 v, i
 }
 
 __device__ __forceinline__ void point_cell(const SearchParams& sp, const GridParams* g, const float4& v, int32_t* c) {
-    const float hc = g->hcell;
-    c[0] = cell_coord(v.x, sp.dmin[0], hc);
-    c[1] = sp.dim > 1 ? cell_coord(v.y, sp.dmin[1], hc) : 0;
-    c[2] = sp.dim > 2 ? cell_coord(v.z, sp.dmin[2], hc) : 0;
+    c[0] = cell_coord(v.x, sp.dmin[0], g->hcell_d[0]);
+    c[1] = sp.dim > 1 ? cell_coord(v.y, sp.dmin[1], g->hcell_d[1]) : 0;
+    c[2] = sp.dim > 2 ? cell_coord(v.z, sp.dmin[2], g->hcell_d[2]) : 0;
+    if (sp.dedupe)  // clamped grid: every point in a cell of [0, count) -- no aliasing, no short seam cell
+        for (int d = 0; d < sp.dim; ++d) c[d] = min(max(c[d], 0), g->count[d] - 1);
 }
 
 // Wrap (twice for the reference cloud, cppSearch.py:221 after neighborhood.py:203; once for a
@@ -558,6 +583,8 @@ struct WalkArgs {
     unsigned long long* cursor;   // staging list fill
     int32_t* stage;               // staging list (original reference indices)
     int64_t stage_cap;
+    const int32_t* __restrict__ query_ids;  // optional: row written for local query q is query_ids[q]
+    const int32_t* __restrict__ ref_ids;    // optional: column written for local reference j is ref_ids[j]
     const int64_t* offsets;       // pass-2 input [nq+1]
     int64_t* row_out;             // pass 2: COO rows or null
     int64_t* col_out;             // pass 2: columns
@@ -571,15 +598,24 @@ __device__ __forceinline__ void stencil_lookup(const WalkArgs& a, const int32_t*
     const SearchParams& sp = a.sp;
     int32_t c[3] = {0, 0, 0};
     int rem = o;
+    bool dup = false;
     for (int d = sp.dim - 1; d >= 0; --d) {
         int32_t off = rem % 3 - 1;
         rem /= 3;
         int32_t v = gc[d] + off;
-        if ((sp.periodic_mask >> d) & 1) v = pymod(v, a.g->count[d]);
+        if ((sp.periodic_mask >> d) & 1) {
+            const int32_t n = a.g->count[d];
+            v = pymod(v, n);
+            // with fewer than 3 cells the wrapped offsets repeat a cell; the clamped grid visits it once
+            if (sp.dedupe && ((n == 1 && off != 0) || (n == 2 && off == 1))) dup = true;
+        } else if (sp.dedupe && (v < 0 || v >= a.g->count[d])) {
+            dup = true;  // clamped grid: nothing lies outside it
+        }
         c[d] = v;
     }
     beg = 0;
     cnt = 0;
+    if (dup) return;
     int32_t lin = linear_index(sp.dim, c, a.g->count);
     int32_t cell = map_find(a.map, a.map_cap, lin);
     if (cell < 0) return;
@@ -822,7 +858,8 @@ __global__ void __launch_bounds__(kWalkWarps * 32) walk_count_kernel(WalkArgs a)
         const int32_t* begs = sm.beg[w];
         const float4* __restrict__ rs = a.rsorted;
         const int32_t* __restrict__ ri = a.rsidx;
-        auto fetch = [&cr, pre, begs, rs, ri, M, nan4](int32_t k, float4& v, int32_t& jo) {
+        const int32_t* __restrict__ rid = a.ref_ids;
+        auto fetch = [&cr, pre, begs, rs, ri, rid, M, nan4](int32_t k, float4& v, int32_t& jo) {
             v = nan4;
             jo = 0;
             if (k < M) {
@@ -830,6 +867,7 @@ __global__ void __launch_bounds__(kWalkWarps * 32) walk_count_kernel(WalkArgs a)
                 const int32_t j = begs[cr] + (k - pre[cr]);
                 v = __ldg(&rs[j]);
                 jo = __ldg(&ri[j]);
+                if (rid) jo = __ldg(&rid[jo]);
             }
         };
         // the unit's chunk loop; `exact` redoes it deciding in-band pairs with the reference test
@@ -952,7 +990,9 @@ __global__ void __launch_bounds__(kWalkWarps * 32) walk_emit_kernel(WalkArgs a) 
                 j = cand_index(s_pre[w], s_beg[w], S, k);
                 cv = __ldg(&a.rsorted[j]);
             }
-            const int64_t jorig = (int64_t)__ldg(&a.rsidx[j]);
+            int32_t jl = __ldg(&a.rsidx[j]);
+            if (a.ref_ids) jl = __ldg(&a.ref_ids[jl]);
+            const int64_t jorig = (int64_t)jl;
             const float cw = cand_share<MODE>(cv.w);
             const float band = exact_all ? __int_as_float(0x7f800000) : cand_band<MODE>(cw, qmax);
             for (int qi = 0; qi < nb; ++qi) {
@@ -963,7 +1003,8 @@ __global__ void __launch_bounds__(kWalkWarps * 32) walk_emit_kernel(WalkArgs a) 
                 if (ub) in = unc ? exact_pair_test(xc, q, q.w, cv, cv.w) : in;
                 const uint32_t b = __ballot_sync(0xffffffffu, in);
                 const int64_t qb = __shfl_sync(0xffffffffu, obase, qi);
-                const int32_t qrow = __shfl_sync(0xffffffffu, qorig, qi);
+                int32_t qrow = __shfl_sync(0xffffffffu, qorig, qi);
+                if (a.query_ids) qrow = __ldg(&a.query_ids[qrow]);
                 if (in) {
                     const int64_t pos = qb + __popc(b & lt);
                     if (pos < a.out_cap) {
@@ -996,7 +1037,8 @@ __global__ void __launch_bounds__(kExpandWarps * 32) expand_records_kernel(
     const int32_t* __restrict__ stage, const int32_t* __restrict__ rec, const int32_t* __restrict__ num_units,
     const int32_t* __restrict__ unit_t0, const int32_t* __restrict__ unit_group,
     const int32_t* __restrict__ group_start, const int32_t* __restrict__ qsidx, const int64_t* __restrict__ offsets,
-    int64_t* __restrict__ row_out, int64_t* __restrict__ col_out, int64_t out_cap) {
+    const int32_t* __restrict__ query_ids, int64_t* __restrict__ row_out, int64_t* __restrict__ col_out,
+    int64_t out_cap) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     ExpandSmem& sm = *reinterpret_cast<ExpandSmem*>(smem_raw);
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
@@ -1025,7 +1067,7 @@ __global__ void __launch_bounds__(kExpandWarps * 32) expand_records_kernel(
         int32_t total = 0;
         if (lane < nb) {
             const int32_t row = qsidx[t0 + lane];
-            sm.qrow[w][lane] = row;
+            sm.qrow[w][lane] = query_ids ? query_ids[row] : row;
             sm.qoff[w][lane] = offsets[row];
             for (int c = 0; c < nchunks; ++c) total += __popc(mk[lane * nchunks + c]);
         }
@@ -1117,8 +1159,9 @@ __global__ void stray_kernel(WalkArgs a) {
                 if (exact_pair_test(xc, q, q.w, cv, cv.w)) {
                     if (EMIT) {
                         if (pos < a.out_cap) {
-                            a.col_out[pos] = (int64_t)a.rsidx[j];
-                            if (a.row_out) a.row_out[pos] = qorig;
+                            const int32_t jl = a.rsidx[j];
+                            a.col_out[pos] = (int64_t)(a.ref_ids ? a.ref_ids[jl] : jl);
+                            if (a.row_out) a.row_out[pos] = a.query_ids ? a.query_ids[qorig] : qorig;
                         }
                         ++pos;
                     } else {
@@ -1179,6 +1222,8 @@ static SearchParams make_params(const tcr_search_desc* d) {
     }
     sp.n_query = d->n_query;
     sp.n_ref = d->n_ref;
+    for (int k = 0; k < 3; ++k) sp.hcell_override[k] = d->hcell[0] > 0.0f ? (k < d->dim ? d->hcell[k] : 1.0f) : 0.0f;
+    sp.dedupe = d->clamped_grid ? 1 : 0;
     return sp;
 }
 
@@ -1201,7 +1246,17 @@ static int validate(const tcr_search_desc* d, bool need_ref_sup = true) {
         return set_error(TCR_ERR_INVALID, "this mode needs reference supports");
     if (d->self_search && d->n_query != d->n_ref)
         return set_error(TCR_ERR_INVALID, "self search needs one cloud");
+    if (d->hcell[0] > 0.0f)
+        for (int k = 0; k < d->dim; ++k)
+            if (!(d->hcell[k] > 0.0f) || !(d->hcell[k] < 3.0e38f))
+                return set_error(TCR_ERR_INVALID, "cell size override must be positive and finite in every dimension");
     return TCR_OK;
+}
+
+// Self search on one cloud with no periodic dimension: the queries, wrapped once, are the
+// references, wrapped twice, so the sorted query array is the sorted reference array.
+static inline bool same_sorted_points(const tcr_search_desc* d) {
+    return d->self_search && d->periodic_mask == 0 && d->query_pos == d->ref_pos && d->query_sup == d->ref_sup;
 }
 
 static inline unsigned grid_for(int64_t n, int threads, int max_blocks = 148 * 16) {
@@ -1414,9 +1469,11 @@ int tcr_count(const tcr_search_desc* d, const void* structure, void* scratch, in
         const int32_t* gstart;
         const int32_t* ngroups;
         if (self) {
-            pack_self_queries_kernel<<<grid_for(nq, 256), 256, 0, st>>>(sp, S.grid, d->query_pos, d->query_sup,
-                                                                        S.rsidx, nq, W.qsorted, W.qsidx);
-            note_launches(1);
+            if (!same_sorted_points(d)) {
+                pack_self_queries_kernel<<<grid_for(nq, 256), 256, 0, st>>>(sp, S.grid, d->query_pos, d->query_sup,
+                                                                            S.rsidx, nq, W.qsorted, W.qsidx);
+                note_launches(1);
+            }
             gstart = S.cell_start;
             ngroups = S.num_cells;
         } else {
@@ -1443,6 +1500,12 @@ int tcr_count(const tcr_search_desc* d, const void* structure, void* scratch, in
         BoundedUnitOut uo{gstart, ngroups, W.unit_group, W.unit_t0, W.query_unit};
         TCR_CUDA(device_exclusive_scan<int32_t>(ui, uo, nq, W.scan_tiles32, W.num_units, st));
         WalkArgs a = make_walk(sp, S, W, self);
+        if (same_sorted_points(d)) {  // the sorted queries are the sorted references
+            a.qsorted = S.rsorted;
+            a.qsidx = S.rsidx;
+        }
+        a.query_ids = d->query_ids;
+        a.ref_ids = d->ref_ids;
         a.stage = stage;
         a.stage_cap = stage_capacity;
         // identical positions: every query sits in its group's cell
@@ -1478,6 +1541,12 @@ int tcr_emit(const tcr_search_desc* d, const void* structure, void* scratch, int
     const int64_t nq = d->n_query;
     if (nq <= 0) return TCR_OK;
     WalkArgs a = make_walk(sp, S, W, d->self_search != 0);
+    if (same_sorted_points(d)) {
+        a.qsorted = S.rsorted;
+        a.qsidx = S.rsidx;
+    }
+    a.query_ids = d->query_ids;
+    a.ref_ids = d->ref_ids;
     a.offsets = offsets;
     a.row_out = row_out;
     a.col_out = col_out;
@@ -1490,8 +1559,8 @@ int tcr_emit(const tcr_search_desc* d, const void* structure, void* scratch, int
         TCR_CUDA(cudaFuncSetAttribute(expand_records_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                       (int)sizeof(ExpandSmem)));
         expand_records_kernel<<<blocks, kExpandWarps * 32, sizeof(ExpandSmem), st>>>(
-            stage, W.rec, W.num_units, W.unit_t0, W.unit_group, group_start, W.qsidx, offsets, row_out, col_out,
-            out_capacity);
+            stage, W.rec, W.num_units, W.unit_t0, W.unit_group, group_start, a.qsidx, offsets, d->query_ids, row_out,
+            col_out, out_capacity);
         note_launches(1);
     }
     TCR_CUDA(cudaMemsetAsync(W.work + 1, 0, sizeof(int32_t), st));

@@ -34,9 +34,11 @@ def radiusSearch(queryPointCloud: PointCloud, referencePointCloud: Optional[Poin
     to query i is strictly below the mode's support: gather h_i, scatter h_j, symmetric
     (h_i + h_j)/2, superSymmetric max(h_i, h_j), periodic dimensions measured across the wrap.
 
-    The result is the reference's ``algorithm='compact'`` result, bit for bit, whatever the
-    ``algorithm`` argument ('naive', 'small', 'mlm' name the same CUDA search; 'cluster'
-    needs the absent torch_cluster package, as in the reference).  ``supportOverride`` gives
+    ``algorithm='compact'`` (and 'naive' / 'small', which name the same CUDA search here) returns
+    the reference's compact result bit for bit.  ``algorithm='mlm'`` runs the multi-level search
+    (torchcompactradius_b200.multilevel): the exact pair set of the same float test on per-level
+    grids, which is the compact result wherever the compact grid itself misses nothing; 'cluster'
+    needs the absent torch_cluster package, as in the reference.  ``supportOverride`` gives
     every point that support (the reference's compact path rejects it).  Outputs live on the
     queries' CUDA device (CPU inputs are searched on the current CUDA device and the result is
     returned to the CPU).
@@ -88,9 +90,14 @@ def radiusSearch(queryPointCloud: PointCloud, referencePointCloud: Optional[Poin
             assert hq is not None, f"queryParticleSupports must be provided for {mode} mode"
         if mode in ("scatter", "symmetric", "superSymmetric"):
             assert hr is not None, f"referenceSupports must be provided for {mode} mode"
-        out, ds = compact_search(xq, hq, xr, hr, lo, hi, mask, mode, hashMapLength, format, same,
-                                 return_structure=returnStructure, ref_pos_user=rpos,
-                                 ref_sup_user=referencePointCloud.supports, fixed_support=supportOverride)
+        if algorithm == "mlm":
+            from .multilevel import multilevel_search
+            out = multilevel_search(xq, hq, xr, hr, lo, hi, mask, mode, format)
+            ds = None  # neighborhood.py:260-263: the multi-level path returns no reusable structure
+        else:
+            out, ds = compact_search(xq, hq, xr, hr, lo, hi, mask, mode, hashMapLength, format, same,
+                                     return_structure=returnStructure, ref_pos_user=rpos,
+                                     ref_sup_user=referencePointCloud.supports, fixed_support=supportOverride)
         if in_device.type != "cuda":
             out = tuple(None if t is None else t.to(in_device) for t in out)
         if format == "coo":

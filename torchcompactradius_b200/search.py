@@ -116,10 +116,12 @@ class CompactHashMap:
         return self._buf[off:off + nbytes].view(dtype)
 
     def _grid(self):
+        # GridParams (include/tcr_b200.h, TCR_STRUCT_GRID): float hmax, float hCell, float hcell_d[3],
+        # int32 cellCount[3], ...
         if "grid" not in self._cache:
-            g = self._view("grid", torch.int32, 5).cpu()
-            f = g[:2].view(torch.float32)
-            self._cache["grid"] = (float(f[0]), float(f[1]), g[2:5].tolist())
+            g = self._view("grid", torch.int32, 8).cpu()
+            f = g[:5].view(torch.float32)
+            self._cache["grid"] = (float(f[0]), float(f[1]), g[5:8].tolist())
         return self._cache["grid"]
 
     @property
