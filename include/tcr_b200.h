@@ -20,7 +20,7 @@
 extern "C" {
 #endif
 
-#define TCR_ABI_VERSION 5
+#define TCR_ABI_VERSION 6
 
 #define TCR_OK 0
 #define TCR_ERR_INVALID (-1) /* bad argument or workspace too small */
@@ -62,14 +62,51 @@ typedef struct tcr_search_desc {
     int32_t reserved;
 } tcr_search_desc;
 
+/* One cloud of a batch: an independent search with its own domain, periodicity, supports and
+ * hashMapLength (the fields mean what they mean in tcr_search_desc). */
+typedef struct tcr_cloud_desc {
+    int32_t dim;             /* 1, 2 or 3 */
+    int32_t periodic_mask;   /* bit d set: dimension d is periodic */
+    float domain_min[3];
+    float domain_max[3];
+    int64_t hash_map_length;
+    int64_t n_query;
+    int64_t n_ref;
+    const float* query_pos;  /* device [n_query*dim] */
+    const float* query_sup;  /* device [n_query] or NULL (TCR_SCATTER) */
+    const float* ref_pos;    /* device [n_ref*dim] */
+    const float* ref_sup;    /* device [n_ref] or NULL (TCR_GATHER) */
+} tcr_cloud_desc;
+
+/* A batch of independent searches run by one set of launches (the many scenes or timesteps of a
+ * simulation sweep; the reference runs them one call at a time, or through its batched
+ * radius(), neighborhood.py:313-363, which searches each batch id on its own).  Clouds never see
+ * each other.  Points are numbered globally in table order: query q of cloud k has the global
+ * index (n_query of clouds 0..k-1) + q, and likewise for reference points.  Offsets, counts and
+ * indptr span all clouds' queries in global order; with local_index = 0 the written rows and
+ * columns are global indices, with local_index = 1 they are indices within the cloud (query_ids /
+ * ref_ids, when given, map global indices and take precedence). */
+typedef struct tcr_batch_desc {
+    int32_t n_clouds;        /* >= 1 */
+    int32_t mode;            /* TCR_GATHER .. TCR_SUPERSYMMETRIC, for every cloud */
+    int32_t self_search;     /* 1: every cloud's query set is its reference set */
+    int32_t local_index;     /* 1: rows and columns numbered within each cloud */
+    const tcr_cloud_desc* clouds;  /* HOST array [n_clouds] */
+    const int32_t* query_ids;      /* device [total queries] or NULL */
+    const int32_t* ref_ids;        /* device [total references] or NULL */
+} tcr_batch_desc;
+
 /* Message of the last failing call on this thread. */
 const char* tcr_last_error(void);
 
 /* TCR_ABI_VERSION of the loaded library. */
 int tcr_version(void);
 
-/* sizeof(tcr_search_desc) as compiled into the library, for FFI layout checks. */
+/* sizeof(tcr_search_desc), sizeof(tcr_cloud_desc) and sizeof(tcr_batch_desc) as compiled into
+ * the library, for FFI layout checks. */
 int64_t tcr_desc_bytes(void);
+int64_t tcr_cloud_desc_bytes(void);
+int64_t tcr_batch_desc_bytes(void);
 
 /* Total number of CUDA kernels this library has launched in this process (launch accounting
  * for benchmarks; no reference counterpart). */
@@ -142,6 +179,23 @@ int tcr_count(const tcr_search_desc* d, const void* structure, void* scratch, in
 int tcr_emit(const tcr_search_desc* d, const void* structure, void* scratch, int64_t scratch_bytes,
              const int32_t* stage, const int64_t* offsets, int64_t* row_out, int64_t* col_out, int64_t out_capacity,
              void* stream);
+
+/* The batched counterparts of tcr_search_sizes / tcr_build_structure / tcr_count / tcr_emit:
+ * the same phases over every cloud of `b` at once, with the same buffer contracts (offsets,
+ * indptr and row entries over all clouds' queries, pairs of all clouds in one output).  All four
+ * calls of one search take descriptors with the same clouds in the same order.  A cloud with
+ * points on both sides and no valid cell grid finds no pairs; info entry 1 counts such clouds and
+ * entry 3 the clouds decided by the exact test alone.  No reference counterpart beyond the
+ * per-cloud operators named above. */
+int tcr_batch_sizes(const tcr_batch_desc* b, int64_t* structure_bytes, int64_t* scratch_bytes);
+int tcr_batch_build_structure(const tcr_batch_desc* b, void* structure, int64_t structure_bytes, void* scratch,
+                              int64_t scratch_bytes, void* stream);
+int tcr_batch_count(const tcr_batch_desc* b, const void* structure, void* scratch, int64_t scratch_bytes,
+                    int32_t* stage, int64_t stage_capacity, int64_t* offsets, int32_t* indptr_out,
+                    int64_t* row_entries_out, int64_t* info_out, void* stream);
+int tcr_batch_emit(const tcr_batch_desc* b, const void* structure, void* scratch, int64_t scratch_bytes,
+                   const int32_t* stage, const int64_t* offsets, int64_t* row_out, int64_t* col_out,
+                   int64_t out_capacity, void* stream);
 
 /* One whole search -- tcr_build_structure, tcr_count and tcr_emit -- that allocates nothing.
  * No counterpart in the reference: it exists for callers that cannot allocate device memory at

@@ -33,7 +33,55 @@ def test_library_exports_every_declared_symbol():
 def test_descriptor_layout_matches_library():
     from torchcompactradius_b200 import _lib
     assert ctypes.sizeof(_lib.SearchDesc) == _lib.load().tcr_desc_bytes()
-    assert _lib.load().tcr_version() == 5
+    assert ctypes.sizeof(_lib.CloudDesc) == _lib.load().tcr_cloud_desc_bytes()
+    assert ctypes.sizeof(_lib.BatchDesc) == _lib.load().tcr_batch_desc_bytes()
+    assert _lib.load().tcr_version() == 6
+
+
+def _batch(clouds, mode=0, self_search=1):
+    from torchcompactradius_b200 import _lib
+    arr = (_lib.CloudDesc * len(clouds))()
+    for k, (dim, nq, nr) in enumerate(clouds):
+        arr[k].dim = dim
+        arr[k].hash_map_length = 4096
+        arr[k].n_query = nq
+        arr[k].n_ref = nr
+        for d in range(3):
+            arr[k].domain_min[d] = -1.0
+            arr[k].domain_max[d] = 1.0
+    b = _lib.BatchDesc()
+    b.n_clouds = len(clouds)
+    b.mode = mode
+    b.self_search = self_search
+    b.clouds = arr
+    return b, arr
+
+
+def test_batch_sizes_grow_with_the_clouds_and_cover_one_search():
+    from torchcompactradius_b200 import _lib
+    b1, keep1 = _batch([(3, 1000, 1000)])
+    s1, w1 = _lib.batch_sizes(b1)
+    b2, keep2 = _batch([(3, 1000, 1000), (2, 5000, 5000), (3, 0, 0)])
+    s2, w2 = _lib.batch_sizes(b2)
+    assert s2 > s1 and w2 > w1
+    s, w = _lib.search_sizes(6000, 6000, 3)
+    assert w2 <= w + 3 * 4096  # one scratch over all points, plus the per-cloud tables
+
+
+def test_invalid_batch_is_rejected_without_device_work():
+    from torchcompactradius_b200 import _lib
+    lib = _lib.load()
+    b, keep = _batch([(3, 10, 10), (4, 10, 10)])
+    rc = lib.tcr_batch_sizes(ctypes.byref(b), None, None)
+    assert rc == -1 and b"cloud 1" in lib.tcr_last_error()
+    b, keep = _batch([(3, 10, 12)])  # a self search needs the same cloud on both sides
+    assert lib.tcr_batch_sizes(ctypes.byref(b), None, None) == -1
+    b, keep = _batch([(3, 10, 10)])
+    b.n_clouds = 0
+    assert lib.tcr_batch_sizes(ctypes.byref(b), None, None) == -1
+    b, keep = _batch([(2, 10, 10)])  # positions missing
+    rc = lib.tcr_batch_build_structure(ctypes.byref(b), None, 0, None, 0, None)
+    assert rc == -1 and b"positions" in lib.tcr_last_error()
 
 
 def test_sizes_and_layout_are_consistent():

@@ -4,12 +4,13 @@ A drop-in for torchCompactRadius's ``radiusSearch`` / ``radius`` / ``neighborSea
 API (same types, arguments and outputs), computed by hand-written CUDA kernels behind a C ABI
 (include/tcr_b200.h).  There is no CPU fallback.
 """
+from .batched import BatchedAdjacency, radiusSearchBatch
 from .neighborhood import neighborSearchExisting, radius, radiusSearch
 from .search import CompactHashMap
 from .util import (DomainDescription, PointCloud, SparseCOO, SparseCSR, coo_to_csr, csr_to_coo,
                    getPeriodicPointCloud, volumeToSupport)
 
 __version__ = "0.1.0"
-__all__ = ["radiusSearch", "radius", "neighborSearchExisting", "volumeToSupport", "PointCloud",
+__all__ = ["radiusSearch", "radiusSearchBatch", "BatchedAdjacency", "radius", "neighborSearchExisting", "volumeToSupport", "PointCloud",
            "DomainDescription", "SparseCOO", "SparseCSR", "CompactHashMap", "coo_to_csr", "csr_to_coo",
            "getPeriodicPointCloud"]

@@ -41,19 +41,56 @@ class SearchDesc(ctypes.Structure):
     ]
 
 
+class CloudDesc(ctypes.Structure):
+    """tcr_cloud_desc (include/tcr_b200.h): one cloud of a batch."""
+    _fields_ = [
+        ("dim", ctypes.c_int32),
+        ("periodic_mask", ctypes.c_int32),
+        ("domain_min", ctypes.c_float * 3),
+        ("domain_max", ctypes.c_float * 3),
+        ("hash_map_length", ctypes.c_int64),
+        ("n_query", ctypes.c_int64),
+        ("n_ref", ctypes.c_int64),
+        ("query_pos", ctypes.c_void_p),
+        ("query_sup", ctypes.c_void_p),
+        ("ref_pos", ctypes.c_void_p),
+        ("ref_sup", ctypes.c_void_p),
+    ]
+
+
+class BatchDesc(ctypes.Structure):
+    """tcr_batch_desc (include/tcr_b200.h): a batch of independent clouds."""
+    _fields_ = [
+        ("n_clouds", ctypes.c_int32),
+        ("mode", ctypes.c_int32),
+        ("self_search", ctypes.c_int32),
+        ("local_index", ctypes.c_int32),
+        ("clouds", ctypes.POINTER(CloudDesc)),
+        ("query_ids", ctypes.c_void_p),
+        ("ref_ids", ctypes.c_void_p),
+    ]
+
+
 # name -> (restype, argtypes); every function declared in include/tcr_b200.h
 _vp, _i64, _i32 = ctypes.c_void_p, ctypes.c_int64, ctypes.c_int32
 _desc_p = ctypes.POINTER(SearchDesc)
+_batch_p = ctypes.POINTER(BatchDesc)
 SIGNATURES = {
     "tcr_last_error": (ctypes.c_char_p, []),
     "tcr_version": (ctypes.c_int, []),
     "tcr_desc_bytes": (_i64, []),
+    "tcr_cloud_desc_bytes": (_i64, []),
+    "tcr_batch_desc_bytes": (_i64, []),
     "tcr_kernel_launches": (_i64, []),
     "tcr_search_sizes": (ctypes.c_int, [_i64, _i64, _i32, ctypes.POINTER(_i64), ctypes.POINTER(_i64)]),
     "tcr_structure_offsets": (ctypes.c_int, [_i64, ctypes.POINTER(_i64), _i32]),
     "tcr_build_structure": (ctypes.c_int, [_desc_p, _vp, _i64, _vp, _i64, _vp]),
     "tcr_count": (ctypes.c_int, [_desc_p, _vp, _vp, _i64, _vp, _i64, _vp, _vp, _vp, _vp, _vp]),
     "tcr_emit": (ctypes.c_int, [_desc_p, _vp, _vp, _i64, _vp, _vp, _vp, _vp, _i64, _vp]),
+    "tcr_batch_sizes": (ctypes.c_int, [_batch_p, ctypes.POINTER(_i64), ctypes.POINTER(_i64)]),
+    "tcr_batch_build_structure": (ctypes.c_int, [_batch_p, _vp, _i64, _vp, _i64, _vp]),
+    "tcr_batch_count": (ctypes.c_int, [_batch_p, _vp, _vp, _i64, _vp, _i64, _vp, _vp, _vp, _vp, _vp]),
+    "tcr_batch_emit": (ctypes.c_int, [_batch_p, _vp, _vp, _i64, _vp, _vp, _vp, _vp, _i64, _vp]),
     "tcr_search_noalloc": (ctypes.c_int, [_desc_p, _vp, _vp, _vp, _vp, _vp, _i64, ctypes.POINTER(_i64), _vp]),
 }
 
@@ -98,4 +135,10 @@ def structure_offsets(n_ref):
 def search_sizes(n_query, n_ref, dim):
     s, w = _i64(0), _i64(0)
     check(load().tcr_search_sizes(n_query, n_ref, dim, ctypes.byref(s), ctypes.byref(w)), "tcr_search_sizes")
+    return s.value, w.value
+
+
+def batch_sizes(bdesc):
+    s, w = _i64(0), _i64(0)
+    check(load().tcr_batch_sizes(ctypes.byref(bdesc), ctypes.byref(s), ctypes.byref(w)), "tcr_batch_sizes")
     return s.value, w.value

@@ -29,8 +29,9 @@ constexpr int kWarp = 32;
 // 4e-6 (~67 ulps) is a safe margin.
 constexpr float kBandEps = 4e-6f;
 
-// Host-filled description of the domain and search (passed by value to kernels).
-struct SearchParams {
+// Host-filled description of one cloud's search: one entry per cloud in a device table (a single
+// search is a table of one).  Global point indices count the clouds' points in table order.
+struct CloudParams {
     int32_t dim;
     int32_t mode;
     int32_t periodic_mask;   // bit d: dimension d is periodic
@@ -38,11 +39,16 @@ struct SearchParams {
     float dmin[3];
     float dmax[3];
     float ext[3];            // fl(dmax - dmin), as the reference computes it
-    int64_t n_query;
-    int64_t n_ref;
-    float hcell_override[3];  // > 0: use these per-dimension cell sizes instead of compute_h
-    int32_t dedupe;           // clamped grid (multi-level): clamp cells, skip outside cells, no repeats
+    float hcell_override[3]; // > 0: use these per-dimension cell sizes instead of compute_h
+    int32_t dedupe;          // clamped grid (multi-level): clamp cells, skip outside cells, no repeats
+    int32_t n_query, n_ref;  // the cloud's points
+    int32_t query_base, ref_base;  // global index of the cloud's first query / reference point
     int32_t pad;
+    int64_t map_base, map_cap;     // the cloud's region of the lin -> cell map (capacity a power of two)
+    const float* query_pos;  // [n_query * dim]
+    const float* query_sup;  // [n_query] or null
+    const float* ref_pos;    // [n_ref * dim]
+    const float* ref_sup;    // [n_ref] or null
 };
 
 // Reduction record over one set of supports.
@@ -134,17 +140,6 @@ struct ExactCtx {
     int32_t dim, mode, periodic_mask;
     float ext[3];
 };
-__device__ __forceinline__ ExactCtx exact_ctx(const SearchParams& sp) {
-    ExactCtx c;
-    c.dim = sp.dim;
-    c.mode = sp.mode;
-    c.periodic_mask = sp.periodic_mask;
-    c.ext[0] = sp.ext[0];
-    c.ext[1] = sp.ext[1];
-    c.ext[2] = sp.ext[2];
-    return c;
-}
-
 // The reference's exact distance test (common.h:106-129 at scalar_t=float).
 __device__ __noinline__ bool exact_pair_test(ExactCtx sp, float4 xi, float hi, float4 xj, float hj) {
     float sum = 0.0f;
@@ -165,32 +160,6 @@ __device__ __noinline__ bool exact_pair_test(ExactCtx sp, float4 xi, float hi, f
     }
     float dist = __fsqrt_rn(sum);
     return dist < mode_threshold(sp.mode, hi, hj);
-}
-
-// Float fast test.  Returns the decision in *in and whether it is uncertain (inside the band or
-// a periodic difference near +-ext/2), in which case exact_pair_test decides.
-template <int DIM, bool PERIODIC>
-__device__ __forceinline__ void fast_pair_test(const SearchParams& sp, const float4& xi, float thr, const float4& xj,
-                                               bool& in, bool& unc) {
-    float d2 = 0.0f;
-    bool wrap_unc = false;
-#pragma unroll
-    for (int d = 0; d < DIM; ++d) {
-        float diff = __fsub_rn(comp(xi, d), comp(xj, d));
-        if (PERIODIC && ((sp.periodic_mask >> d) & 1)) {
-            float h = sp.ext[d];
-            float half = 0.5f * h;
-            float ad = fabsf(diff);
-            wrap_unc |= fabsf(ad - half) <= kBandEps * h;
-            if (diff >= half) diff = __fsub_rn(diff, h);
-            else if (diff < -half) diff = __fadd_rn(diff, h);
-        }
-        d2 = (d == 0) ? __fmul_rn(diff, diff) : __fmaf_rn(diff, diff, d2);
-    }
-    float t2 = thr * fabsf(thr);
-    float r = d2 - t2;
-    in = r < 0.0f;
-    unc = wrap_unc || (fabsf(r) <= kBandEps * fabsf(t2));
 }
 
 }  // namespace tcr

@@ -1,21 +1,29 @@
 // tcr_search.cu -- compact-hashing fixed-radius neighbour search for sm_100a, with a C ABI.
 //
-// Pipeline (one CUDA stream, no host synchronisation inside a phase):
-//   build:  support max-reduction -> grid parameters (compute_h) -> wrap + pack reference points
-//           into float4 (x, y, z, h) and int32 linear cell keys -> stable radix sort ->
-//           run-length cell table (begin, coords, bucket) + open-addressing lin -> cell map.
-//   count:  query packing (self search reuses the reference order) -> query groups (cells) ->
-//           work units of <= 32 queries -> warp-per-unit candidate walk over the 3^d stencil with
-//           broadcast query positions and ballot counting -> device scan -> offsets.
-//   emit:   the same walk writing int64 (row, col) pairs at the scanned offsets.
+// One engine serves a single search and a batch of independent clouds (the scenes or timesteps
+// of a simulation sweep, of uneven sizes, each with its own domain, periodicity, supports and
+// hashMapLength); a single search is a batch of one cloud.  Every phase is one set of launches
+// over all clouds, on one CUDA stream, with no host synchronisation inside a phase:
+//   build:  per-cloud support max-reductions -> per-cloud grid parameters (compute_h) -> wrap and
+//           pack reference points into float4 (x, y, z, h) with (cloud, linear cell) sort keys ->
+//           stable radix sort -> run-length cell table (begin, coords, bucket, cloud) and one
+//           open-addressing lin -> cell map region per cloud.
+//   count:  query packing (a self search reuses the reference order) -> query groups (cells) ->
+//           work units of <= 32 queries of one group -> warp-per-unit candidate walk that tests
+//           every (query, candidate) pair once, counts, and stages per-unit hit records -> scan.
+//   emit:   expansion of the staged records into CSR/COO slots; units that were not staged are
+//           walked again.
 // The candidate set of every query is the reference's (cppSrc/neighborhood.h:73-132): the
 // stencil cells of its own cell, found by linear index inside the bucket of the stencil cell's
-// hash; the pair test is the reference's float test (tcr_common.cuh).
+// hash; the pair test is the reference's float test (tcr_common.cuh).  Clouds never see each
+// other: keys, cells, map regions and work units all carry the cloud.
 #include <cstdio>
 #include <cstring>
 #include <cstdarg>
+#include <cstddef>
 #include <algorithm>
 #include <mutex>
+#include <vector>
 
 #include "tcr_common.cuh"
 #include "tcr_scan.cuh"
@@ -49,7 +57,13 @@ static inline int64_t next_pow2(int64_t x) {
     while (p < x) p <<= 1;
     return p;
 }
-static inline int64_t hash_capacity(int64_t n_ref) { return std::max<int64_t>(1024, next_pow2(2 * std::max<int64_t>(n_ref, 1))); }
+// Map slots of a cloud with n reference points: a power of two >= 2n (load factor <= 1/2).
+static inline int64_t hash_capacity(int64_t n_ref, int64_t min_cap) {
+    return std::max<int64_t>(min_cap, next_pow2(2 * std::max<int64_t>(n_ref, 1)));
+}
+constexpr int64_t kSingleMapMin = 1024;  // one search
+constexpr int64_t kBatchMapMin = 64;     // per cloud of a batch
+constexpr int kWorkCounters = 4;
 
 struct Carve {
     char* base;
@@ -64,108 +78,172 @@ struct Carve {
 
 // Persistent structure (reference side); kept alive for reuse.
 struct Structure {
-    GridParams* grid;       // [1]
-    float4* rsorted;        // [nr] wrapped reference points in cell order, .w = support
-    int32_t* rsidx;         // [nr] original index of each sorted point
-    int32_t* cell_start;    // [nr+1]
-    int32_t* cell_lin;      // [nr]
-    int32_t* cell_coords;   // [3*nr]
-    int32_t* cell_bucket;   // [nr] ref hash of the cell's coordinates mod hashMapLength
-    int32_t* num_cells;     // [1]
-    unsigned long long* map;  // [H] (lin << 32 | cell), empty = ~0
-    int64_t map_cap;
+    GridParams* grid;         // [C] per cloud
+    int32_t* num_cells;       // [1]
+    int32_t* bad_grids;       // [1] clouds with points on both sides and no valid grid
+    float4* rsorted;          // [nr] wrapped reference points in (cloud, cell) order, .w = support
+    int32_t* rsidx;           // [nr] global index of each sorted point
+    int32_t* cell_start;      // [nr+1]
+    int32_t* cell_lin;        // [nr]
+    int32_t* cell_coords;     // [3*nr]
+    int32_t* cell_bucket;     // [nr] reference hash of the cell's coordinates mod hashMapLength
+    int32_t* cell_cloud;      // [nr]
+    unsigned long long* map;  // [map_total] per-cloud regions of (lin << 32 | cell), empty = ~0
+    int64_t map_total;
 };
 
-static Structure carve_structure(void* buf, int64_t nr, int64_t* bytes) {
+static Structure carve_structure(void* buf, int64_t nr, int64_t C, int64_t map_total, int64_t* bytes) {
     Carve c{(char*)buf, 0};
     Structure s;
-    s.grid = c.take<GridParams>(1);
+    s.grid = c.take<GridParams>(C);
     s.num_cells = c.take<int32_t>(1);
+    s.bad_grids = c.take<int32_t>(1);
     s.rsorted = c.take<float4>(nr);
     s.rsidx = c.take<int32_t>(nr);
     s.cell_start = c.take<int32_t>(nr + 1);
     s.cell_lin = c.take<int32_t>(nr);
     s.cell_coords = c.take<int32_t>(3 * nr);
     s.cell_bucket = c.take<int32_t>(nr);
-    s.map_cap = hash_capacity(nr);
-    s.map = c.take<unsigned long long>(s.map_cap);
+    s.cell_cloud = c.take<int32_t>(nr);
+    s.map_total = map_total;
+    s.map = c.take<unsigned long long>(map_total);
     if (bytes) *bytes = c.off;
     return s;
 }
 
 // Per-search scratch.
 struct Scratch {
+    CloudParams* table;     // [C] this search's cloud table
+    int32_t* query_prefix;  // [C+1] global index of each cloud's first query (last: total)
+    int32_t* ref_prefix;    // [C+1] the same for reference points
+    QueryParams* qparams;   // [C]
+    void* sort_state;       // SortState32 or SortState64
+    int32_t* num_qgroups;   // [1]
+    int32_t* num_units;     // [1]
+    int32_t* num_stray;     // [1]
+    int32_t* work;          // [kWorkCounters] work distribution counters
+    int64_t* total;         // [1]
+    int64_t* info;          // [8] see tcr_count
+    int32_t* num_flagged;   // [1]
+    int32_t* exact_clouds;  // [1] clouds whose every pair takes the exact test
+    unsigned long long* cursor;  // [1] staging fill
     float4* pack;           // [max(nq,nr)] packed input points before sorting
-    SortWorkspace sort;
+    void* keys[2];          // [max(nq,nr)] 64-bit slots (32-bit keys use the first half)
+    int32_t* vals[2];
+    int32_t* hist;
+    int32_t* tile_sums;
     int64_t* scan_tiles64;  // [scan_tiles(max)]
     int32_t* scan_tiles32;  // [scan_tiles(max)]
     float4* qsorted;        // [nq]
-    int32_t* qsidx;         // [nq]
+    int32_t* qsidx;         // [nq] global query index of each sorted query
     int32_t* qgroup_start;  // [nq+1]
     int32_t* qgroup_coords; // [3*nq]
-    int32_t* num_qgroups;   // [1]
+    int32_t* qgroup_cloud;  // [nq]
     int32_t* unit_group;    // [nq]
     int32_t* unit_t0;       // [nq]
-    int32_t* num_units;     // [1]
-    int32_t* counts;        // [nq]
+    int32_t* counts;        // [nq] global query order
     int32_t* stray;         // [nq]
-    int32_t* num_stray;     // [1]
-    int32_t* work;          // [4] work counters
-    int64_t* total;         // [1]
-    int64_t* info;          // [8] total pairs, grid error, stray queries, exact-only mode, staging words
-                            //     requested, units re-walked by tcr_emit, 0, 0
-    QueryParams* qparams;   // [1]
     int32_t* rec;           // [nq] per unit: offset of its record in the staging list (-1: not staged)
-    int32_t* query_unit;    // [nq] unit of each sorted query
     int32_t* flagged;       // [nq] units re-walked by the emit pass
-    int32_t* num_flagged;   // [1]
-    unsigned long long* cursor;  // [1] staging fill
 };
 
-static Scratch carve_scratch(void* buf, int64_t nq, int64_t nr, int64_t* bytes) {
+static Scratch carve_scratch(void* buf, int64_t nq, int64_t nr, int64_t C, int64_t* bytes) {
     Carve c{(char*)buf, 0};
     Scratch s;
-    int64_t nmax = std::max<int64_t>(std::max<int64_t>(nq, nr), 1);
-    s.sort.state = c.take<SortState>(1);
+    const int64_t nmax = std::max<int64_t>(std::max<int64_t>(nq, nr), 1);
+    s.table = c.take<CloudParams>(C);
+    s.query_prefix = c.take<int32_t>(C + 1);
+    s.ref_prefix = c.take<int32_t>(C + 1);
+    s.qparams = c.take<QueryParams>(C);
+    s.sort_state = c.take<SortState64>(1);
     s.num_qgroups = c.take<int32_t>(1);
     s.num_units = c.take<int32_t>(1);
     s.num_stray = c.take<int32_t>(1);
-    s.work = c.take<int32_t>(4);
+    s.work = c.take<int32_t>(kWorkCounters);
     s.total = c.take<int64_t>(1);
     s.info = c.take<int64_t>(8);
-    s.qparams = c.take<QueryParams>(1);
     s.num_flagged = c.take<int32_t>(1);
+    s.exact_clouds = c.take<int32_t>(1);
     s.cursor = c.take<unsigned long long>(1);
     s.pack = c.take<float4>(nmax);
-    s.sort.keys[0] = c.take<uint32_t>(nmax);
-    s.sort.keys[1] = c.take<uint32_t>(nmax);
-    s.sort.vals[0] = c.take<int32_t>(nmax);
-    s.sort.vals[1] = c.take<int32_t>(nmax);
-    s.sort.hist = c.take<int32_t>(sort_hist_elems(nmax));
-    s.sort.tile_sums = c.take<int32_t>(scan_tiles(sort_hist_elems(nmax)));
+    s.keys[0] = c.take<unsigned long long>(nmax);
+    s.keys[1] = c.take<unsigned long long>(nmax);
+    s.vals[0] = c.take<int32_t>(nmax);
+    s.vals[1] = c.take<int32_t>(nmax);
+    s.hist = c.take<int32_t>(sort_hist_elems(nmax));
+    s.tile_sums = c.take<int32_t>(scan_tiles(sort_hist_elems(nmax)));
     s.scan_tiles64 = c.take<int64_t>(scan_tiles(nmax + 1));
     s.scan_tiles32 = c.take<int32_t>(scan_tiles(nmax + 1));
-    int64_t q = std::max<int64_t>(nq, 1);
+    const int64_t q = std::max<int64_t>(nq, 1);
     s.qsorted = c.take<float4>(q);
     s.qsidx = c.take<int32_t>(q);
     s.qgroup_start = c.take<int32_t>(q + 1);
     s.qgroup_coords = c.take<int32_t>(3 * q);
+    s.qgroup_cloud = c.take<int32_t>(q);
     s.unit_group = c.take<int32_t>(q);
     s.unit_t0 = c.take<int32_t>(q);
     s.counts = c.take<int32_t>(q);
     s.stray = c.take<int32_t>(q);
     s.rec = c.take<int32_t>(q);
-    s.query_unit = c.take<int32_t>(q);
     s.flagged = c.take<int32_t>(q);
     if (bytes) *bytes = c.off;
     return s;
 }
 
+template <typename K>
+static SortWorkspaceT<K> sort_workspace(const Scratch& W) {
+    SortWorkspaceT<K> s;
+    s.keys[0] = reinterpret_cast<K*>(W.keys[0]);
+    s.keys[1] = reinterpret_cast<K*>(W.keys[1]);
+    s.vals[0] = W.vals[0];
+    s.vals[1] = W.vals[1];
+    s.hist = W.hist;
+    s.tile_sums = W.tile_sums;
+    s.state = reinterpret_cast<SortStateT<K>*>(W.sort_state);
+    return s;
+}
+
+// ------------------------------------------------------------------------------------------
+// the cloud table
+
+// Host -> device copy of the table as kernel parameters (no pageable copy, so it also records
+// into a CUDA graph): chunks of kUploadChunk clouds per launch.
+constexpr int kUploadChunk = 24;
+struct CloudChunk {
+    int32_t first, count, n_clouds, query_total, ref_total, pad;
+    CloudParams p[kUploadChunk];
+};
+static_assert(sizeof(CloudChunk) <= 4000, "kernel parameter block too large");
+
+__global__ void upload_clouds_kernel(CloudChunk ch, CloudParams* table, int32_t* query_prefix, int32_t* ref_prefix) {
+    const int i = threadIdx.x;
+    if (i < ch.count) {
+        const int c = ch.first + i;
+        table[c] = ch.p[i];
+        query_prefix[c] = ch.p[i].query_base;
+        ref_prefix[c] = ch.p[i].ref_base;
+    }
+    if (i == 0 && ch.first + ch.count == ch.n_clouds) {
+        query_prefix[ch.n_clouds] = ch.query_total;
+        ref_prefix[ch.n_clouds] = ch.ref_total;
+    }
+}
+
+// Cloud of global point index i: the last c with prefix[c] <= i (empty clouds are skipped).
+__device__ __forceinline__ int cloud_of(const int32_t* __restrict__ prefix, int C, int64_t i) {
+    if (C == 1) return 0;
+    int lo = 0, hi = C;
+    while (hi - lo > 1) {
+        const int mid = (lo + hi) >> 1;
+        if (prefix[mid] <= i) lo = mid; else hi = mid;
+    }
+    return lo;
+}
+
 // ------------------------------------------------------------------------------------------
 // build kernels
 
-
-// Block reduction of max / or over a strided array; one atomic per block and field.
+// Block reduction of max / or; one atomic per block and field.
 __device__ __forceinline__ void block_reduce_stats(uint32_t kmax, int bad, SupportStats* out) {
     __shared__ uint32_t s_max[32];
     __shared__ int s_bad[32];
@@ -192,122 +270,180 @@ __device__ __forceinline__ void block_reduce_stats(uint32_t kmax, int bad, Suppo
     }
 }
 
-// computeGridSupport (cellTable.py:40-81) needs the largest support; the lean test needs to know
-// whether every support lies in [1e-18, 1e18] (else the exact test decides every pair).
-__global__ void support_stats_kernel(const float* __restrict__ h, int64_t n, SupportStats* out) {
+__device__ __forceinline__ SupportStats* stats_at(char* base, int64_t stride, int c) {
+    return reinterpret_cast<SupportStats*>(base + stride * c);
+}
+__device__ __forceinline__ void stats_atomic(SupportStats* s, uint32_t kmax, int bad) {
+    if (kmax) atomicMax(&s->max_key, kmax);
+    if (bad) atomicOr(&s->bad, 1);
+}
+
+// Per-cloud maximum support (computeGridSupport, cellTable.py:40-81, needs it) and whether every
+// support lies in [1e-18, 1e18] (else the exact test decides every pair).  Each block reduces a
+// contiguous range, so a thread changes cloud only at cloud boundaries; a block that stayed in one
+// cloud issues one atomic per field.  The record of cloud c is at out + c * stride.
+__global__ void support_stats_kernel(const CloudParams* __restrict__ table, const int32_t* __restrict__ prefix, int C,
+                                     int64_t n, int query_side, char* out, int64_t stride) {
+    const int64_t per = (n + gridDim.x - 1) / gridDim.x;
+    const int64_t lo = (int64_t)blockIdx.x * per;
+    const int64_t hi = min(n, lo + per);
+    int cur = -1;
+    int64_t cbase = 0, cend = 0;
+    const float* h = nullptr;
     uint32_t kmax = 0;
     int bad = 0;
-    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
-    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
-        const float v = h[i];
-        kmax = max(kmax, float_key(v));
-        bad |= !(v >= 1e-18f && v <= 1e18f);
+    for (int64_t i = lo + threadIdx.x; i < hi; i += blockDim.x) {
+        if (cur < 0 || i >= cend) {
+            if (cur >= 0) stats_atomic(stats_at(out, stride, cur), kmax, bad);
+            cur = cloud_of(prefix, C, i);
+            cbase = prefix[cur];
+            cend = prefix[cur + 1];
+            h = query_side ? table[cur].query_sup : table[cur].ref_sup;
+            kmax = 0;
+            bad = 0;
+        }
+        if (h) {
+            const float v = h[i - cbase];
+            kmax = max(kmax, float_key(v));
+            bad |= !(v >= 1e-18f && v <= 1e18f);
+        }
     }
-    block_reduce_stats(kmax, bad, out);
+    __shared__ int s_cloud;
+    if (threadIdx.x == 0) s_cloud = cur;  // thread 0 holds the block's first point, if it has any
+    __syncthreads();
+    if (__syncthreads_and(cur < 0 || cur == s_cloud)) {
+        if (s_cloud >= 0) block_reduce_stats(kmax, bad, stats_at(out, stride, s_cloud));
+    } else if (cur >= 0) {
+        stats_atomic(stats_at(out, stride, cur), kmax, bad);
+    }
 }
 
-__global__ void stats_init_kernel(SupportStats* a, SupportStats* b) {
-    a->max_key = 0; a->bad = 0;
-    if (b) { b->max_key = 0; b->bad = 0; }
+template <typename K>
+__global__ void grid_init_kernel(GridParams* g, int C, int32_t* bad_grids, SortStateT<K>* st) {
+    for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < C; c += gridDim.x * blockDim.x) {
+        g[c].ref_stats.max_key = 0;
+        g[c].ref_stats.bad = 0;
+        g[c].build_query_stats.max_key = 0;
+        g[c].build_query_stats.bad = 0;
+        g[c].error = 0;
+        g[c].out_of_grid = 0;
+    }
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        *bad_grids = 0;
+        sort_state_reset(st);
+    }
 }
 
-// Query-side parameters of one search.
-__global__ void query_params_kernel(const GridParams* g, int mode, int has_query_sup, QueryParams* qp) {
-    const float qmax = has_query_sup ? key_float(qp->stats.max_key) : 0.0f;
-    qp->qmax = (mode == kScatter) ? 0.0f : qmax;
-    const bool qbad = (mode != kScatter) && has_query_sup && qp->stats.bad;
-    const bool rbad = (mode != kGather) && g->ref_stats.bad;
-    qp->exact_all = (qbad || rbad || !(fabsf(qp->qmax) <= 1e18f)) ? 1 : 0;
-}
+template <typename K>
+__global__ void sort_state_init_kernel(SortStateT<K>* st) { sort_state_reset(st); }
 
-__global__ void sort_state_init_kernel(SortState* st) {
-    st->key_min = 0xffffffffu;
-    st->key_max = 0;
-    st->sel[0] = 0;
-}
-
-__global__ void grid_init_kernel(GridParams* g, SortState* st) {
-    g->ref_stats.max_key = 0;
-    g->ref_stats.bad = 0;
-    g->build_query_stats.max_key = 0;
-    g->build_query_stats.bad = 0;
-    g->error = 0;
-    g->out_of_grid = 0;
-    st->key_min = 0xffffffffu;
-    st->key_max = 0;
-    st->sel[0] = 0;
-}
-
-// util.py:28-79 compute_h and cellTable.py:27-29, float32 throughout.
-__global__ void grid_params_kernel(SearchParams sp, GridParams* g, SortState* st) {
+// Per cloud: util.py:28-79 compute_h and cellTable.py:27-29, float32 throughout.
+__global__ void grid_params_kernel(const CloudParams* __restrict__ table, GridParams* grid, int C,
+                                   int32_t* bad_grids) {
     const float grow = 1.00010001659393310546875f;  // fl32(1e-4 + 1)
-    // computeGridSupport: scatter reads the reference supports, gather the query supports,
-    // (super)symmetric both (torch.max propagates NaN, as the key maximum does).
-    uint32_t key = 0;
-    if (sp.mode != kGather) key = max(key, g->ref_stats.max_key);
-    if (sp.mode != kScatter) key = max(key, g->build_query_stats.max_key);
-    float hmax = key_float(key);
-    float ext[3], nc[3], h[3];
-    bool any = false;
-    for (int d = 0; d < sp.dim; ++d) {
-        ext[d] = __fsub_rn(sp.dmax[d], sp.dmin[d]);
-        nc[d] = floorf(__fdiv_rn(ext[d], hmax));
-        h[d] = __fdiv_rn(ext[d], nc[d]);
-    }
-    for (int d = 0; d < sp.dim; ++d) any |= __fsub_rn(__fdiv_rn(ext[d], h[d]), nc[d]) > 0.0f;
-    if (any)
+    for (int cl = blockIdx.x * blockDim.x + threadIdx.x; cl < C; cl += gridDim.x * blockDim.x) {
+        const CloudParams& sp = table[cl];
+        GridParams* g = &grid[cl];
+        // computeGridSupport: scatter reads the reference supports, gather the query supports,
+        // (super)symmetric both (torch.max propagates NaN, as the key maximum does).
+        uint32_t key = 0;
+        if (sp.mode != kGather) key = max(key, g->ref_stats.max_key);
+        if (sp.mode != kScatter) key = max(key, g->build_query_stats.max_key);
+        const float hmax = key_float(key);
+        float ext[3], nc[3], h[3];
+        bool any = false;
         for (int d = 0; d < sp.dim; ++d) {
-            nc[d] = __fsub_rn(nc[d], 1.0f);
+            ext[d] = __fsub_rn(sp.dmax[d], sp.dmin[d]);
+            nc[d] = floorf(__fdiv_rn(ext[d], hmax));
             h[d] = __fdiv_rn(ext[d], nc[d]);
         }
-    any = false;
-    for (int d = 0; d < sp.dim; ++d) {
-        float r = __fdiv_rn(ext[d], h[d]);
-        any |= ceilf(r) > r;
-    }
-    if (any)
-        for (int d = 0; d < sp.dim; ++d) h[d] = __fmul_rn(h[d], grow);
-    float hc = h[0];
-    for (int d = 1; d < sp.dim; ++d) {
-        float v = h[d];
-        if (hc != hc) break;
-        if (v != v || v > hc) hc = v;  // torch.max propagates NaN
-    }
-    g->hmax = hmax;
-    g->hcell = hc;
-    if (sp.hcell_override[0] > 0.0f) {  // caller-chosen grid (multi-level search)
-        hc = sp.hcell_override[0];
-        for (int d = 0; d < 3; ++d) {
-            g->hcell_d[d] = d < sp.dim ? sp.hcell_override[d] : 1.0f;
-            hc = fminf(hc, g->hcell_d[d]);
+        for (int d = 0; d < sp.dim; ++d) any |= __fsub_rn(__fdiv_rn(ext[d], h[d]), nc[d]) > 0.0f;
+        if (any)
+            for (int d = 0; d < sp.dim; ++d) {
+                nc[d] = __fsub_rn(nc[d], 1.0f);
+                h[d] = __fdiv_rn(ext[d], nc[d]);
+            }
+        any = false;
+        for (int d = 0; d < sp.dim; ++d) {
+            const float r = __fdiv_rn(ext[d], h[d]);
+            any |= ceilf(r) > r;
         }
-        for (int d = 0; d < 3; ++d) {
-            if (d >= sp.dim) { g->count[d] = 1; continue; }
-            const float r = __fdiv_rn(ext[d], g->hcell_d[d]);
-            // periodic dims of a clamped grid hold a whole number of cells (ext / n each); rounding
-            // must not add a sliver cell at the seam
-            g->count[d] = (sp.dedupe && ((sp.periodic_mask >> d) & 1)) ? max(1, (int32_t)rintf(r))
-                                                                         : (int32_t)ceilf(r);
+        if (any)
+            for (int d = 0; d < sp.dim; ++d) h[d] = __fmul_rn(h[d], grow);
+        float hc = h[0];
+        for (int d = 1; d < sp.dim; ++d) {
+            const float v = h[d];
+            if (hc != hc) break;
+            if (v != v || v > hc) hc = v;  // torch.max propagates NaN
         }
-    } else {
-        for (int d = 0; d < 3; ++d) {
-            g->hcell_d[d] = hc;
-            g->count[d] = d < sp.dim ? (int32_t)ceilf(__fdiv_rn(ext[d], hc)) : 1;
+        g->hmax = hmax;
+        g->hcell = hc;
+        if (sp.hcell_override[0] > 0.0f) {  // caller-chosen grid (multi-level search)
+            hc = sp.hcell_override[0];
+            for (int d = 0; d < 3; ++d) {
+                g->hcell_d[d] = d < sp.dim ? sp.hcell_override[d] : 1.0f;
+                hc = fminf(hc, g->hcell_d[d]);
+            }
+            for (int d = 0; d < 3; ++d) {
+                if (d >= sp.dim) { g->count[d] = 1; continue; }
+                const float r = __fdiv_rn(ext[d], g->hcell_d[d]);
+                // periodic dims of a clamped grid hold a whole number of cells (ext / n each);
+                // rounding must not add a sliver cell at the seam
+                g->count[d] = (sp.dedupe && ((sp.periodic_mask >> d) & 1)) ? max(1, (int32_t)rintf(r))
+                                                                             : (int32_t)ceilf(r);
+            }
+        } else {
+            for (int d = 0; d < 3; ++d) {
+                g->hcell_d[d] = hc;
+                g->count[d] = d < sp.dim ? (int32_t)ceilf(__fdiv_rn(ext[d], hc)) : 1;
+            }
         }
+        g->always_exact = ((sp.mode != kGather && g->ref_stats.bad) || (sp.mode != kScatter && g->build_query_stats.bad))
+                              ? 1 : 0;
+        int err = 0;
+        if (!(hc > 0.0f) || !isfinite(hc)) err = 1;  // no valid grid (support larger than the domain, NaN, ...)
+        if (sp.dedupe) {  // clamped grid: linear indices must not wrap
+            double cells = 1.0;
+            for (int d = 0; d < sp.dim; ++d) cells *= (double)max(g->count[d], 1);
+            if (cells >= 2147483647.0) err = 1;
+        }
+        for (int d = 0; d < sp.dim; ++d)
+            if (((sp.periodic_mask >> d) & 1) && g->count[d] <= 0) err = 1;
+        g->error = err;
+        if (err && sp.n_query > 0 && sp.n_ref > 0) atomicAdd(bad_grids, 1);
     }
-    g->always_exact = ((sp.mode != kGather && g->ref_stats.bad) || (sp.mode != kScatter && g->build_query_stats.bad))
-                          ? 1 : 0;
-    int err = 0;
-    if (!(hc > 0.0f) || !isfinite(hc)) err = 1;  // no valid grid (support larger than the domain, NaN, ...)
-    if (sp.dedupe) {  // clamped grid: linear indices must not wrap
-        double cells = 1.0;
-        for (int d = 0; d < sp.dim; ++d) cells *= (double)max(g->count[d], 1);
-        if (cells >= 2147483647.0) err = 1;
+}
+
+// Per cloud: the query-side parameters of the lean test.
+__global__ void query_params_kernel(const CloudParams* __restrict__ table, const GridParams* __restrict__ grid, int C,
+                                    QueryParams* qp, int32_t* exact_clouds) {
+    for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < C; c += gridDim.x * blockDim.x) {
+        const CloudParams& cp = table[c];
+        QueryParams& q = qp[c];
+        const bool has_q = cp.query_sup != nullptr;
+        const float qmax = has_q ? key_float(q.stats.max_key) : 0.0f;
+        q.qmax = (cp.mode == kScatter) ? 0.0f : qmax;
+        const bool qbad = (cp.mode != kScatter) && has_q && q.stats.bad;
+        const bool rbad = (cp.mode != kGather) && grid[c].ref_stats.bad;
+        q.exact_all = (qbad || rbad || !(fabsf(q.qmax) <= 1e18f)) ? 1 : 0;
+        if (q.exact_all && cp.n_query > 0) atomicAdd(exact_clouds, 1);
     }
-    for (int d = 0; d < sp.dim; ++d)
-        if (((sp.periodic_mask >> d) & 1) && g->count[d] <= 0) err = 1;
-    g->error = err;
-    if (err) st->key_min = st->key_max = 0;  // no radix pass runs on keys that were never written
+}
+
+// Zeroes the per-search counters and the per-cloud query statistics.
+__global__ void count_init_kernel(Scratch W, int C) {
+    for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < C; c += gridDim.x * blockDim.x) {
+        W.qparams[c].stats.max_key = 0;
+        W.qparams[c].stats.bad = 0;
+    }
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        for (int k = 0; k < kWorkCounters; ++k) W.work[k] = 0;
+        *W.num_stray = 0;
+        *W.num_units = 0;
+        *W.num_flagged = 0;
+        *W.exact_clouds = 0;
+        *W.cursor = 0ull;
+    }
 }
 
 __device__ __forceinline__ float4 load_point(const float* x, const float* h, int64_t i, int dim) {
@@ -319,63 +455,128 @@ __device__ __forceinline__ float4 load_point(const float* x, const float* h, int
     return v;
 }
 
-__device__ __forceinline__ float4 wrap_point(const SearchParams& sp, float4 v, int times) {
-    for (int d = 0; d < sp.dim; ++d)
-        if ((sp.periodic_mask >> d) & 1) {
+__device__ __forceinline__ float4 wrap_point(int dim, int mask, const float* dmin, const float* ext, float4 v,
+                                             int times) {
+    for (int d = 0; d < dim; ++d)
+        if ((mask >> d) & 1) {
             float c = comp(v, d);
-            for (int t = 0; t < times; ++t) c = wrap_coord(c, sp.dmin[d], sp.ext[d]);
+            for (int t = 0; t < times; ++t) c = wrap_coord(c, dmin[d], ext[d]);
             if (d == 0) v.x = c; else if (d == 1) v.y = c; else v.z = c;
         }
     return v;
 }
 
-__device__ __forceinline__ void point_cell(const SearchParams& sp, const GridParams* g, const float4& v, int32_t* c) {
-    c[0] = cell_coord(v.x, sp.dmin[0], g->hcell_d[0]);
-    c[1] = sp.dim > 1 ? cell_coord(v.y, sp.dmin[1], g->hcell_d[1]) : 0;
-    c[2] = sp.dim > 2 ? cell_coord(v.z, sp.dmin[2], g->hcell_d[2]) : 0;
-    if (sp.dedupe)  // clamped grid: every point in a cell of [0, count) -- no aliasing, no short seam cell
-        for (int d = 0; d < sp.dim; ++d) c[d] = min(max(c[d], 0), g->count[d] - 1);
+// Integer cell of a point; a clamped grid (dedupe) puts every point in a cell of [0, count):
+// no aliasing, no short seam cell.
+__device__ __forceinline__ void cell_of(int dim, int dedupe, const float* dmin, const float* hcell,
+                                        const int32_t* count, const float4& v, int32_t* c) {
+    c[0] = cell_coord(v.x, dmin[0], hcell[0]);
+    c[1] = dim > 1 ? cell_coord(v.y, dmin[1], hcell[1]) : 0;
+    c[2] = dim > 2 ? cell_coord(v.z, dmin[2], hcell[2]) : 0;
+    if (dedupe)
+        for (int d = 0; d < dim; ++d) c[d] = min(max(c[d], 0), count[d] - 1);
+}
+
+// (cloud, signed-order linear index) sort keys; one cloud needs no cloud bits.
+__device__ __forceinline__ void make_key(uint32_t& k, int, uint32_t lin_key) { k = lin_key; }
+__device__ __forceinline__ void make_key(unsigned long long& k, int cloud, uint32_t lin_key) {
+    k = ((unsigned long long)(uint32_t)cloud << 32) | lin_key;
+}
+__device__ __forceinline__ int key_cloud(uint32_t) { return 0; }
+__device__ __forceinline__ int key_cloud(unsigned long long k) { return (int)(k >> 32); }
+__device__ __forceinline__ uint32_t key_low(uint32_t k) { return k; }
+__device__ __forceinline__ uint32_t key_low(unsigned long long k) { return (uint32_t)k; }
+template <typename K>
+__device__ __forceinline__ K kmin2(K a, K b) { return a < b ? a : b; }
+template <typename K>
+__device__ __forceinline__ K kmax2(K a, K b) { return a < b ? b : a; }
+
+// What a point-parallel kernel needs of the point's cloud, reloaded when a thread crosses into
+// another cloud.
+struct PointCtx {
+    int32_t cloud, dim, periodic_mask, dedupe, error;
+    int64_t base, end;
+    float dmin[3], ext[3], hcell[3];
+    int32_t count[3];
+    const float* pos;
+    const float* sup;
+};
+__device__ __forceinline__ void load_point_ctx(PointCtx& p, const CloudParams* __restrict__ table,
+                                               const GridParams* grid, const int32_t* __restrict__ prefix, int c,
+                                               bool query_side) {
+    const CloudParams& cp = table[c];
+    const GridParams& g = grid[c];
+    p.cloud = c;
+    p.dim = cp.dim;
+    p.periodic_mask = cp.periodic_mask;
+    p.dedupe = cp.dedupe;
+    p.error = g.error;
+    p.base = prefix[c];
+    p.end = prefix[c + 1];
+    for (int d = 0; d < 3; ++d) {
+        p.dmin[d] = cp.dmin[d];
+        p.ext[d] = cp.ext[d];
+        p.hcell[d] = g.hcell_d[d];
+        p.count[d] = g.count[d];
+    }
+    p.pos = query_side ? cp.query_pos : cp.ref_pos;
+    p.sup = query_side ? cp.query_sup : cp.ref_sup;
 }
 
 // Wrap (twice for the reference cloud, cppSearch.py:221 after neighborhood.py:203; once for a
-// query cloud), pack to float4 and emit the signed-order linear key.
-__global__ void pack_points_kernel(SearchParams sp, GridParams* g, const float* x, const float* h, int64_t n,
-                                   int wraps, float4* pack, uint32_t* keys, int32_t* vals, SortState* st,
-                                   int track_grid) {
-    uint32_t kmin = 0xffffffffu, kmax = 0;
-    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
-    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n && !g->error; i += stride) {
-        float4 v = wrap_point(sp, load_point(x, h, i, sp.dim), wraps);
-        int32_t c[3];
-        point_cell(sp, g, v, c);
-        if (track_grid) {
-            bool out = false;
-            for (int d = 0; d < sp.dim; ++d) out |= c[d] < 0 || c[d] >= g->count[d];
-            if (out && !g->out_of_grid) atomicOr(&g->out_of_grid, 1);
+// query cloud), pack to float4 and emit the (cloud, linear cell) key.  A cloud without a valid
+// grid gets one constant key (its points form one cell that no walk visits).
+template <typename K>
+__global__ void pack_points_kernel(const CloudParams* __restrict__ table, GridParams* grid,
+                                   const int32_t* __restrict__ prefix, int C, int64_t n, int query_side, int wraps,
+                                   int track_grid, float4* __restrict__ pack, K* __restrict__ keys,
+                                   int32_t* __restrict__ vals, SortStateT<K>* st) {
+    K kmin = ~(K)0, kmax = 0;
+    const int64_t per = (n + gridDim.x - 1) / gridDim.x;
+    const int64_t lo = (int64_t)blockIdx.x * per;
+    const int64_t hi = min(n, lo + per);
+    PointCtx p;
+    p.cloud = -1;
+    p.end = 0;
+    for (int64_t i = lo + threadIdx.x; i < hi; i += blockDim.x) {
+        if (p.cloud < 0 || i >= p.end) load_point_ctx(p, table, grid, prefix, cloud_of(prefix, C, i), query_side != 0);
+        float4 v = load_point(p.pos, p.sup, i - p.base, p.dim);
+        uint32_t lin = 0;
+        if (!p.error) {
+            v = wrap_point(p.dim, p.periodic_mask, p.dmin, p.ext, v, wraps);
+            int32_t c[3];
+            cell_of(p.dim, p.dedupe, p.dmin, p.hcell, p.count, v, c);
+            if (track_grid) {
+                bool out = false;
+                for (int d = 0; d < p.dim; ++d) out |= c[d] < 0 || c[d] >= p.count[d];
+                if (out && !*(volatile int32_t*)&grid[p.cloud].out_of_grid) atomicOr(&grid[p.cloud].out_of_grid, 1);
+            }
+            lin = (uint32_t)linear_index(p.dim, c, p.count);
         }
-        uint32_t key = (uint32_t)linear_index(sp.dim, c, g->count) ^ 0x80000000u;
+        K key;
+        make_key(key, p.cloud, lin ^ 0x80000000u);
         pack[i] = v;
         keys[i] = key;
         vals[i] = (int32_t)i;
-        kmin = min(kmin, key);
-        kmax = max(kmax, key);
+        kmin = kmin2(kmin, key);
+        kmax = kmax2(kmax, key);
     }
-    __shared__ uint32_t s_min[32], s_max[32];
+    __shared__ K s_min[32], s_max[32];
 #pragma unroll
     for (int o = 16; o; o >>= 1) {
-        kmin = min(kmin, __shfl_xor_sync(0xffffffffu, kmin, o));
-        kmax = max(kmax, __shfl_xor_sync(0xffffffffu, kmax, o));
+        kmin = kmin2(kmin, (K)__shfl_xor_sync(0xffffffffu, kmin, o));
+        kmax = kmax2(kmax, (K)__shfl_xor_sync(0xffffffffu, kmax, o));
     }
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, nw = blockDim.x >> 5;
     if (lane == 0) { s_min[w] = kmin; s_max[w] = kmax; }
     __syncthreads();
     if (w == 0) {
-        kmin = lane < nw ? s_min[lane] : 0xffffffffu;
-        kmax = lane < nw ? s_max[lane] : 0u;
+        kmin = lane < nw ? s_min[lane] : ~(K)0;
+        kmax = lane < nw ? s_max[lane] : (K)0;
 #pragma unroll
         for (int o = 16; o; o >>= 1) {
-            kmin = min(kmin, __shfl_xor_sync(0xffffffffu, kmin, o));
-            kmax = max(kmax, __shfl_xor_sync(0xffffffffu, kmax, o));
+            kmin = kmin2(kmin, (K)__shfl_xor_sync(0xffffffffu, kmin, o));
+            kmax = kmax2(kmax, (K)__shfl_xor_sync(0xffffffffu, kmax, o));
         }
         if (lane == 0) {
             atomicMin(&st->key_min, kmin);
@@ -414,58 +615,67 @@ __device__ __forceinline__ int32_t map_find(const unsigned long long* __restrict
     return -1;
 }
 
-// Gathers sorted points and flags run starts (unique_consecutive, hashTable.py:193).
+// Run starts of the sorted keys (unique_consecutive, hashTable.py:193).
+template <typename K>
 struct RunFlagIn {
-    const GridParams* g;
-    const uint32_t* keys0;
-    const uint32_t* keys1;
-    const SortState* st;
+    const K* keys0;
+    const K* keys1;
+    const SortStateT<K>* st;
     __device__ int32_t operator()(int64_t i) const {
-        if (g->error) return 0;
-        const uint32_t* k = st->sel[4] ? keys1 : keys0;
+        const K* k = st->sel[key_passes<K>()] ? keys1 : keys0;
         return (i == 0 || k[i] != k[i - 1]) ? 1 : 0;
     }
 };
 
-// Writes one cell record per run start: begin, lin, coords of the run's first point, bucket.
+// Writes one cell record per run start: begin, lin, cloud, coords of the run's first point,
+// bucket, and the cell's entry in its cloud's map region.
+template <typename K>
 struct CellOut {
-    SearchParams sp;
-    const GridParams* g;
-    const uint32_t* keys0;
-    const uint32_t* keys1;
-    const SortState* st;
+    const CloudParams* table;
+    const GridParams* grid;
+    const K* keys0;
+    const K* keys1;
+    const SortStateT<K>* st;
     const float4* rsorted;
     int32_t* cell_start;
     int32_t* cell_lin;
     int32_t* cell_coords;
     int32_t* cell_bucket;
+    int32_t* cell_cloud;
     unsigned long long* map;
-    int64_t map_cap;
     __device__ void operator()(int64_t i, int32_t ex, int32_t flag) const {
         if (!flag) return;
-        const uint32_t* k = st->sel[4] ? keys1 : keys0;
-        const int32_t cell = ex;
-        const int32_t lin = (int32_t)(k[i] ^ 0x80000000u);
-        int32_t c[3];
-        point_cell(sp, g, rsorted[i], c);
-        cell_start[cell] = (int32_t)i;
-        cell_lin[cell] = lin;
-        cell_coords[3 * cell + 0] = c[0];
-        cell_coords[3 * cell + 1] = c[1];
-        cell_coords[3 * cell + 2] = c[2];
-        cell_bucket[cell] = (int32_t)ref_hash(sp.dim, c, sp.hash_len);
-        map_insert(map, map_cap, lin, cell);
+        const K* k = st->sel[key_passes<K>()] ? keys1 : keys0;
+        const K key = k[i];
+        const int cloud = key_cloud(key);
+        const int32_t lin = (int32_t)(key_low(key) ^ 0x80000000u);
+        const CloudParams& cp = table[cloud];
+        const GridParams& g = grid[cloud];
+        int32_t c[3] = {0, 0, 0};
+        uint32_t bucket = 0;
+        if (!g.error) {
+            cell_of(cp.dim, cp.dedupe, cp.dmin, g.hcell_d, g.count, rsorted[i], c);
+            bucket = ref_hash(cp.dim, c, cp.hash_len);
+            map_insert(map + cp.map_base, cp.map_cap, lin, ex);
+        }
+        cell_start[ex] = (int32_t)i;
+        cell_lin[ex] = lin;
+        cell_cloud[ex] = cloud;
+        cell_coords[3 * ex + 0] = c[0];
+        cell_coords[3 * ex + 1] = c[1];
+        cell_coords[3 * ex + 2] = c[2];
+        cell_bucket[ex] = (int32_t)bucket;
     }
 };
 
-__global__ void gather_sorted_kernel(const GridParams* g, const float4* pack, const int32_t* vals0,
-                                     const int32_t* vals1, const SortState* st, int64_t n, float4* sorted,
-                                     int32_t* sidx) {
-    if (g->error) return;
-    const int32_t* v = st->sel[4] ? vals1 : vals0;
+template <typename K>
+__global__ void gather_sorted_kernel(const float4* __restrict__ pack, const int32_t* vals0, const int32_t* vals1,
+                                     const SortStateT<K>* st, int64_t n, float4* __restrict__ sorted,
+                                     int32_t* __restrict__ sidx) {
+    const int32_t* v = st->sel[key_passes<K>()] ? vals1 : vals0;
     const int64_t stride = (int64_t)gridDim.x * blockDim.x;
     for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
-        int32_t p = v[i];
+        const int32_t p = v[i];
         sorted[i] = pack[p];
         sidx[i] = p;
     }
@@ -480,28 +690,44 @@ __global__ void finish_cells_kernel(int32_t* cell_start, const int32_t* num_cell
 
 // Self search: query i is reference i, so the reference order and cells group the queries.
 // Positions are the once-wrapped query coordinates (only periodic dims differ from rsorted).
-__global__ void pack_self_queries_kernel(SearchParams sp, const GridParams* g, const float* x, const float* h,
-                                         const int32_t* rsidx, int64_t n, float4* qsorted, int32_t* qsidx) {
-    if (g->error) return;
-    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
-    for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < n; t += stride) {
-        int32_t i = rsidx[t];
-        qsorted[t] = wrap_point(sp, load_point(x, h, i, sp.dim), 1);
+__global__ void pack_self_queries_kernel(const CloudParams* __restrict__ table, const GridParams* grid,
+                                         const int32_t* __restrict__ prefix, int C, const int32_t* __restrict__ rsidx,
+                                         int64_t n, float4* __restrict__ qsorted, int32_t* __restrict__ qsidx) {
+    const int64_t per = (n + gridDim.x - 1) / gridDim.x;
+    const int64_t lo = (int64_t)blockIdx.x * per;
+    const int64_t hi = min(n, lo + per);
+    PointCtx p;
+    p.cloud = -1;
+    p.base = p.end = 0;
+    for (int64_t t = lo + threadIdx.x; t < hi; t += blockDim.x) {
+        const int32_t i = rsidx[t];
+        if (p.cloud < 0 || i < p.base || i >= p.end) load_point_ctx(p, table, grid, prefix, cloud_of(prefix, C, i), true);
+        qsorted[t] = wrap_point(p.dim, p.periodic_mask, p.dmin, p.ext, load_point(p.pos, p.sup, i - p.base, p.dim), 1);
         qsidx[t] = i;
     }
 }
 
+template <typename K>
 struct QueryGroupOut {
-    SearchParams sp;
-    const GridParams* g;
+    const CloudParams* table;
+    const GridParams* grid;
+    const K* keys0;
+    const K* keys1;
+    const SortStateT<K>* st;
     const float4* qsorted;
     int32_t* group_start;
     int32_t* group_coords;
+    int32_t* group_cloud;
     __device__ void operator()(int64_t i, int32_t ex, int32_t flag) const {
         if (!flag) return;
-        int32_t c[3];
-        point_cell(sp, g, qsorted[i], c);
+        const K* k = st->sel[key_passes<K>()] ? keys1 : keys0;
+        const int cloud = key_cloud(k[i]);
+        const CloudParams& cp = table[cloud];
+        const GridParams& g = grid[cloud];
+        int32_t c[3] = {0, 0, 0};
+        if (!g.error) cell_of(cp.dim, cp.dedupe, cp.dmin, g.hcell_d, g.count, qsorted[i], c);
         group_start[ex] = (int32_t)i;
+        group_cloud[ex] = cloud;
         group_coords[3 * ex + 0] = c[0];
         group_coords[3 * ex + 1] = c[1];
         group_coords[3 * ex + 2] = c[2];
@@ -526,89 +752,137 @@ struct BoundedUnitOut {
     const int32_t* num_groups;
     int32_t* unit_group;
     int32_t* unit_t0;
-    int32_t* query_unit;
     __device__ void operator()(int64_t g, int32_t ex, int32_t nunits) const {
         if (g >= *num_groups) return;
-        const int32_t s = group_start[g], e = group_start[g + 1];
+        const int32_t s = group_start[g];
         for (int32_t u = 0; u < nunits; ++u) {
             unit_group[ex + u] = (int32_t)g;
             unit_t0[ex + u] = s + u * kUnit;
         }
-        for (int32_t t = s; t < e; ++t) query_unit[t] = ex + (t - s) / kUnit;
     }
 };
 
 // ------------------------------------------------------------------------------------------
 // the candidate walk
 //
-// Work unit: <= 32 queries of one query group (cell).  One warp walks the unit's stencil
-// candidates in chunks of 32 (lane = candidate) and tests every query of the unit against the
-// chunk (query positions broadcast from shared memory); __ballot_sync gives, per query and chunk,
-// the 32-bit hit mask.  Pass 1 keeps the masks of a unit with <= kSegChunks chunks in shared
-// memory, reserves room for the unit's hits in a staging list with one atomic and writes them
-// there query by query; pass 2 moves each query's staged hits to its CSR/COO slot (a memory-bound
-// copy).  A unit with more chunks, or one that finds the staging list full, is only counted in
-// pass 1 and is walked again (with the test) in pass 2 to write its pairs directly.
+// Work unit: <= 32 queries of one query group (cell).  One warp takes a unit, looks up its
+// cloud (one copy of the cloud's parameters in shared memory, refreshed when the warp moves to
+// another cloud), finds the unit's 3^d stencil cells and walks their candidates in chunks of 32.
+// The count walk tests every (query, candidate) pair once, keeps the 32-bit hit masks of a unit
+// with <= kSegChunks chunks in shared memory and writes them with the chunk's candidate indices
+// as one record to a staging list; the emit pass expands the records into CSR/COO slots.  A unit
+// with more chunks, or one that finds the staging list full, is only counted and is walked again
+// by the emit walk, which writes its pairs directly.
+
+// The unit's cloud, as the walk kernels read it (shared memory, warp-uniform).
+struct UnitCtx {
+    int32_t cloud, dim, periodic_mask, dedupe;
+    uint32_t hash_len;
+    int32_t error, out_of_grid, exact_all;
+    int32_t count[3];
+    int32_t qshift, rshift;  // subtracted from global query / reference indices (cloud-local numbering)
+    float dmin[3], hcell[3], ext[3];
+    float rmax, qmax;        // largest reference / query support (band of the fast test)
+    int64_t map_base, map_cap;
+};
 
 struct WalkArgs {
-    SearchParams sp;
-    const GridParams* g;
-    const QueryParams* qp;
+    const CloudParams* __restrict__ table;
+    const GridParams* grid;
+    const QueryParams* __restrict__ qparams;
+    const int32_t* __restrict__ query_prefix;
+    int32_t num_clouds;
+    int32_t local_index;          // 1: rows and columns numbered within each cloud
+    int32_t mode;
+    int32_t no_stray_check;       // self search, no periodic dims, same positions: a query's cell is its
+                                  // group's unless its cloud has points outside the grid (out_of_grid)
     const float4* __restrict__ rsorted;
     const int32_t* __restrict__ rsidx;
     const int32_t* __restrict__ cell_start;
-    const int32_t* __restrict__ cell_coords;
     const int32_t* __restrict__ cell_bucket;
     const unsigned long long* __restrict__ map;
-    int64_t map_cap;
     const float4* __restrict__ qsorted;
     const int32_t* __restrict__ qsidx;
     const int32_t* __restrict__ group_start;
     const int32_t* __restrict__ group_coords;
+    const int32_t* __restrict__ group_cloud;
     const int32_t* __restrict__ unit_group;
     const int32_t* __restrict__ unit_t0;
     const int32_t* __restrict__ num_units;
-    const int32_t* __restrict__ unit_list;  // emit re-walk: the units to walk (null: all units)
+    const int32_t* __restrict__ unit_list;  // emit re-walk: the units to walk
     const int32_t* __restrict__ num_list;
     int32_t* work;
     int32_t* stray;
     int32_t* num_stray;
-    int32_t* counts;              // [nq] pass-1 output, original query order
+    int32_t* counts;              // [nq] count output, global query order
     int32_t* rec;                 // [units] offset of each unit's record in the staging list, -1 if not staged
-    int32_t no_stray_check;       // self search, no periodic dims, every point in the grid: a query's cell is
-                                  // its group's (the device flag out_of_grid withdraws this)
-    int32_t* query_unit;          // [nq] unit of each sorted query
-    int32_t* flagged;             // [units] units to re-walk in pass 2
+    int32_t* flagged;             // [units] units to re-walk in the emit pass
     int32_t* num_flagged;
     unsigned long long* cursor;   // staging list fill
-    int32_t* stage;               // staging list (original reference indices)
+    int32_t* stage;               // staging list
     int64_t stage_cap;
-    const int32_t* __restrict__ query_ids;  // optional: row written for local query q is query_ids[q]
-    const int32_t* __restrict__ ref_ids;    // optional: column written for local reference j is ref_ids[j]
-    const int64_t* offsets;       // pass-2 input [nq+1]
-    int64_t* row_out;             // pass 2: COO rows or null
-    int64_t* col_out;             // pass 2: columns
-    int64_t out_cap;              // pass 2: entries of row_out/col_out; writes beyond are dropped
+    const int32_t* __restrict__ query_ids;  // optional: row written for global query q is query_ids[q]
+    const int32_t* __restrict__ ref_ids;    // optional: column written for global reference j is ref_ids[j]
+    const int64_t* offsets;       // emit input [nq+1]
+    int64_t* row_out;             // emit: COO rows or null
+    int64_t* col_out;             // emit: columns
+    int64_t out_cap;              // emit: entries of row_out/col_out; writes beyond are dropped
 };
+
+__device__ __forceinline__ void load_unit_ctx(UnitCtx& u, const WalkArgs& a, int cloud) {
+    const CloudParams& cp = a.table[cloud];
+    const GridParams& g = a.grid[cloud];
+    const QueryParams& q = a.qparams[cloud];
+    u.cloud = cloud;
+    u.dim = cp.dim;
+    u.periodic_mask = cp.periodic_mask;
+    u.dedupe = cp.dedupe;
+    u.hash_len = cp.hash_len;
+    u.error = g.error;
+    u.out_of_grid = g.out_of_grid;
+    u.exact_all = q.exact_all;
+    for (int d = 0; d < 3; ++d) {
+        u.count[d] = g.count[d];
+        u.dmin[d] = cp.dmin[d];
+        u.hcell[d] = g.hcell_d[d];
+        u.ext[d] = cp.ext[d];
+    }
+    u.qshift = a.local_index ? cp.query_base : 0;
+    u.rshift = a.local_index ? cp.ref_base : 0;
+    u.rmax = key_float(g.ref_stats.max_key);
+    u.qmax = q.qmax;
+    u.map_base = cp.map_base;
+    u.map_cap = cp.map_cap;
+}
+
+__device__ __forceinline__ ExactCtx unit_exact_ctx(const UnitCtx& u, int mode) {
+    ExactCtx c;
+    c.dim = u.dim;
+    c.mode = mode;
+    c.periodic_mask = u.periodic_mask;
+    c.ext[0] = u.ext[0];
+    c.ext[1] = u.ext[1];
+    c.ext[2] = u.ext[2];
+    return c;
+}
 
 // Looks up stencil cell `o` (getOffsets order, last coordinate fastest) around cell gc with the
 // reference's semantics; returns the sorted range or an empty one.
-__device__ __forceinline__ void stencil_lookup(const WalkArgs& a, const int32_t* gc, int o, int32_t& beg,
-                                               int32_t& cnt) {
-    const SearchParams& sp = a.sp;
+__device__ __forceinline__ void stencil_lookup(const WalkArgs& a, const UnitCtx& u, const int32_t* gc, int o,
+                                               int32_t& beg, int32_t& cnt) {
     int32_t c[3] = {0, 0, 0};
     int rem = o;
     bool dup = false;
-    for (int d = sp.dim - 1; d >= 0; --d) {
-        int32_t off = rem % 3 - 1;
+    for (int d = u.dim - 1; d >= 0; --d) {
+        const int32_t off = rem % 3 - 1;
         rem /= 3;
         int32_t v = gc[d] + off;
-        if ((sp.periodic_mask >> d) & 1) {
-            const int32_t n = a.g->count[d];
+        if ((u.periodic_mask >> d) & 1) {
+            const int32_t n = u.count[d];
             v = pymod(v, n);
             // with fewer than 3 cells the wrapped offsets repeat a cell; the clamped grid visits it once
-            if (sp.dedupe && ((n == 1 && off != 0) || (n == 2 && off == 1))) dup = true;
-        } else if (sp.dedupe && (v < 0 || v >= a.g->count[d])) {
+            if (u.dedupe && ((n == 1 && off != 0) || (n == 2 && off == 1))) dup = true;
+        } else if (u.dedupe && (v < 0 || v >= u.count[d])) {
             dup = true;  // clamped grid: nothing lies outside it
         }
         c[d] = v;
@@ -616,11 +890,11 @@ __device__ __forceinline__ void stencil_lookup(const WalkArgs& a, const int32_t*
     beg = 0;
     cnt = 0;
     if (dup) return;
-    int32_t lin = linear_index(sp.dim, c, a.g->count);
-    int32_t cell = map_find(a.map, a.map_cap, lin);
+    const int32_t lin = linear_index(u.dim, c, u.count);
+    const int32_t cell = map_find(a.map + u.map_base, u.map_cap, lin);
     if (cell < 0) return;
     // queryHashMap matches the linear index inside bucket hash(c) only.
-    if ((uint32_t)__ldg(&a.cell_bucket[cell]) != ref_hash(sp.dim, c, sp.hash_len)) return;
+    if ((uint32_t)__ldg(&a.cell_bucket[cell]) != ref_hash(u.dim, c, u.hash_len)) return;
     beg = __ldg(&a.cell_start[cell]);
     cnt = __ldg(&a.cell_start[cell + 1]) - beg;
 }
@@ -659,8 +933,8 @@ __device__ __forceinline__ float pair_thr(float hq, float cw) {
 
 // One (query, candidate) test.  in: decided; unc: needs the exact reference test.
 template <int DIM, bool PERIODIC, int MODE>
-__device__ __forceinline__ void lean_test(const SearchParams& sp, const float4& q, const float4& c, float cw,
-                                          float band, bool& in, bool& unc) {
+__device__ __forceinline__ void lean_test(const ExactCtx& sp, const float4& q, const float4& c, float cw, float band,
+                                          bool& in, bool& unc) {
     float d2;
     bool wrap_unc = false;
     {
@@ -697,7 +971,8 @@ struct WalkSmem {
     float4 q[kWalkWarps][32];
     float4 cand[kWalkWarps][36];                  // the chunk's candidates, stream-major, rows padded
     uint32_t mask[kWalkWarps][32 * kMaskStride];  // [query][chunk] hit masks
-    int32_t sj[kWalkWarps][kSegChunks][32];       // original index of candidate (chunk, lane)
+    int32_t sj[kWalkWarps][kSegChunks][32];       // output column of candidate (chunk, lane)
+    UnitCtx u[kWalkWarps];
 };
 
 // Candidate k of the unit (prefix pre[0..S]): returns its sorted index.
@@ -787,170 +1062,271 @@ __device__ __noinline__ uint32_t stream_mask_exact(ExactCtx xc, const float4* ca
     return m;
 }
 
-// Pass 1: test every (query, candidate) once; count, stage the hits of small units.
+// Count walk of one unit: test every (query, candidate) once; count, stage the hits of small units.
 //
 // Each chunk's 32 candidates are staged in shared memory; lane (q, s) holds query q and tests it
 // against the Q candidates of stream s (Q = 8, 16 or 32 as the unit has <= 8, <= 16 or <= 32
 // queries, so 32/Q streams keep every lane busy).  Hits become bits of a per-lane mask, merged
 // across streams with shuffles into the 32-bit (query, chunk) mask.
 template <int DIM, bool PERIODIC, int MODE>
+__device__ __forceinline__ void count_unit(const WalkArgs& a, WalkSmem& sm, int32_t unit, int32_t grp, int lane,
+                                           int w) {
+    constexpr int S = DIM == 1 ? 3 : (DIM == 2 ? 9 : 27);
+    const UnitCtx& u = sm.u[w];
+    const ExactCtx xc = unit_exact_ctx(u, MODE);
+    const float rmax = u.rmax;
+    const bool exact_all = u.exact_all != 0;
+    const int32_t rshift = u.rshift;
+    const float4 nan4 = make_float4(__int_as_float(0x7fc00000), 0.f, 0.f, 0.f);
+    const int32_t t0 = a.unit_t0[unit];
+    const int32_t nb = min(32, a.group_start[grp + 1] - t0);
+    const int32_t gc[3] = {a.group_coords[3 * grp], a.group_coords[3 * grp + 1], a.group_coords[3 * grp + 2]};
+    int32_t beg = 0, cnt = 0;
+    if (lane < S) stencil_lookup(a, u, gc, lane, beg, cnt);
+    const int32_t inc = warp_inclusive_scan(cnt);
+    sm.pre[w][lane + 1] = inc;
+    if (lane == 0) sm.pre[w][0] = 0;
+    sm.beg[w][lane] = beg;
+    const int32_t M = __shfl_sync(0xffffffffu, inc, 31);
+    bool active = false;
+    int32_t qorig = 0;
+    float4 qv = nan4;
+    if (lane < nb) {
+        const int32_t t = t0 + lane;
+        qv = a.qsorted[t];
+        qorig = a.qsidx[t];
+        active = true;
+        if (!a.no_stray_check || u.out_of_grid) {
+            int32_t qc[3];
+            cell_of(DIM, u.dedupe, u.dmin, u.hcell, u.count, qv, qc);
+            active = same_cell<DIM>(qc, gc);
+        }
+        if (!active) {  // own cell differs from the group's (aliasing or wrap rounding): serial path
+            int32_t k = atomicAdd(a.num_stray, 1);
+            a.stray[k] = t;
+            qv = nan4;
+        }
+    }
+    sm.q[w][lane] = qv;  // rows >= nb hold NaN queries and never hit
+    const int32_t nchunks = (M + 31) >> 5;
+    const bool stage = a.stage_cap > 0 && nchunks <= kSegChunks;
+    const int Q = nb <= 8 ? 8 : (nb <= 16 ? 16 : 32);
+    const int lq = lane & (Q - 1);      // this lane's query
+    const int ls = lane / Q;            // this lane's stream
+    __syncwarp();
+    const float4 myq = sm.q[w][lq];
+    const float qs = query_share<MODE>(myq.w);
+    const float band = exact_all ? __int_as_float(0x7f800000) : query_band<MODE>(myq.w, rmax);
+    const float4* my_cand = &sm.cand[w][ls * (Q + 1)];
+    // Lane k of chunk c holds candidate 32c + k.  Its stencil cell r only moves forward from
+    // chunk to chunk, so it is tracked incrementally instead of searched.
+    int32_t cr = 0;
+    const int32_t* pre = sm.pre[w];
+    const int32_t* begs = sm.beg[w];
+    const float4* __restrict__ rs = a.rsorted;
+    const int32_t* __restrict__ ri = a.rsidx;
+    const int32_t* __restrict__ rid = a.ref_ids;
+    auto fetch = [&cr, pre, begs, rs, ri, rid, rshift, M, nan4](int32_t k, float4& v, int32_t& jo) {
+        v = nan4;
+        jo = 0;
+        if (k < M) {
+            while (pre[cr + 1] <= k) ++cr;
+            const int32_t j = begs[cr] + (k - pre[cr]);
+            v = __ldg(&rs[j]);
+            jo = __ldg(&ri[j]);
+            jo = rid ? __ldg(&rid[jo]) : jo - rshift;
+        }
+    };
+    // the unit's chunk loop; `exact` redoes it deciding in-band pairs with the reference test
+    int32_t qcount = 0;
+    bool unc = false;
+    for (int pass = 0; pass < 2; ++pass) {
+        const bool exact = pass == 1;
+        cr = 0;
+        qcount = 0;
+        float4 nxt;
+        int32_t nxt_j;
+        fetch(lane, nxt, nxt_j);
+        for (int32_t c = 0; c < nchunks; ++c) {
+            // stage candidate `lane` of this chunk: stream lane / Q, slot lane % Q
+            sm.cand[w][(lane / Q) * (Q + 1) + (lane & (Q - 1))] = nxt;
+            if (stage) sm.sj[w][c][lane] = nxt_j;
+            fetch(((c + 1) << 5) + lane, nxt, nxt_j);  // prefetch the next chunk's candidate
+            __syncwarp();
+            uint32_t m;
+            if (exact) {
+                m = stream_mask_exact<DIM, PERIODIC, MODE>(xc, my_cand, Q, myq, qs, band) << (Q == 32 ? 0 : Q * ls);
+            } else if (Q == 32) {
+                m = stream_mask<DIM, PERIODIC, MODE, 32>(xc, my_cand, myq, qs, band, unc);
+            } else if (Q == 16) {
+                m = stream_mask<DIM, PERIODIC, MODE, 16>(xc, my_cand, myq, qs, band, unc) << (16 * ls);
+            } else {
+                m = stream_mask<DIM, PERIODIC, MODE, 8>(xc, my_cand, myq, qs, band, unc) << (8 * ls);
+            }
+            if (Q <= 16) m |= __shfl_xor_sync(0xffffffffu, m, 16);
+            if (Q == 8) m |= __shfl_xor_sync(0xffffffffu, m, 8);
+            if (lane < nb) {
+                qcount += __popc(m);
+                if (stage) sm.mask[w][lane * kMaskStride + c] = m;
+            }
+            __syncwarp();
+        }
+        if (exact || !__any_sync(0xffffffffu, unc)) break;
+    }
+    if (active) a.counts[qorig] = qcount;
+    bool staged = false;
+    if (stage) {
+        // record: [nchunks] [masks: nb x nchunks, query-major] [candidates: nchunks x 32]
+        const int64_t words = 1 + (int64_t)nb * nchunks + 32 * (int64_t)nchunks;
+        unsigned long long base = 0;
+        if (lane == 0) base = atomicAdd(a.cursor, (unsigned long long)words);
+        base = __shfl_sync(0xffffffffu, base, 0);
+        staged = base + (unsigned long long)words <= (unsigned long long)a.stage_cap;
+        if (staged) {
+            int32_t* r = a.stage + base;
+            if (lane == 0) {
+                r[0] = nchunks;
+                a.rec[unit] = (int32_t)base;
+            }
+            __syncwarp();
+            for (int q = 0; q < nb; ++q)
+                if (lane < nchunks) r[1 + q * nchunks + lane] = sm.mask[w][q * kMaskStride + lane];
+            int32_t* rj = r + 1 + nb * nchunks;
+            for (int32_t c = 0; c < nchunks; ++c) rj[c * 32 + lane] = sm.sj[w][c][lane];
+        }
+    }
+    if (!staged && lane == 0) {
+        a.rec[unit] = -1;
+        int32_t f = atomicAdd(a.num_flagged, 1);
+        a.flagged[f] = unit;
+    }
+    __syncwarp();
+}
+
+// Units come from one counter.  DIM == 0: the clouds differ in dimension or periodicity, and
+// each unit runs the body of its own cloud's class.
+template <int DIM, bool PERIODIC, int MODE>
 __global__ void __launch_bounds__(kWalkWarps * 32) walk_count_kernel(WalkArgs a) {
-    if (a.g->error) return;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     WalkSmem& sm = *reinterpret_cast<WalkSmem*>(smem_raw);
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-    constexpr int S = DIM == 1 ? 3 : (DIM == 2 ? 9 : 27);
-    const ExactCtx xc = exact_ctx(a.sp);
-    const float rmax = key_float(a.g->ref_stats.max_key);
-    const bool exact_all = a.qp->exact_all != 0;
     const int32_t nunits = *a.num_units;
-    const float4 nan4 = make_float4(__int_as_float(0x7fc00000), 0.f, 0.f, 0.f);
+    int cur = -1;
     for (;;) {
         int32_t unit = 0;
         if (lane == 0) unit = atomicAdd(&a.work[0], 1);
         unit = __shfl_sync(0xffffffffu, unit, 0);
         if (unit >= nunits) break;
         const int32_t grp = a.unit_group[unit];
-        const int32_t t0 = a.unit_t0[unit];
-        const int32_t nb = min(32, a.group_start[grp + 1] - t0);
-        const int32_t gc[3] = {a.group_coords[3 * grp], a.group_coords[3 * grp + 1], a.group_coords[3 * grp + 2]};
-        int32_t beg = 0, cnt = 0;
-        if (lane < S) stencil_lookup(a, gc, lane, beg, cnt);
-        const int32_t inc = warp_inclusive_scan(cnt);
-        sm.pre[w][lane + 1] = inc;
-        if (lane == 0) sm.pre[w][0] = 0;
-        sm.beg[w][lane] = beg;
-        const int32_t M = __shfl_sync(0xffffffffu, inc, 31);
-        bool active = false;
-        int32_t qorig = 0;
-        float4 qv = nan4;
-        if (lane < nb) {
-            const int32_t t = t0 + lane;
-            qv = a.qsorted[t];
-            qorig = a.qsidx[t];
-            active = true;
-            if (!a.no_stray_check || a.g->out_of_grid) {
-                int32_t qc[3];
-                point_cell(a.sp, a.g, qv, qc);
-                active = same_cell<DIM>(qc, gc);
-            }
-            if (!active) {  // own cell differs from the group's (aliasing or wrap rounding): serial path
-                int32_t k = atomicAdd(a.num_stray, 1);
-                a.stray[k] = t;
-                qv = nan4;
-            }
+        const int cloud = a.num_clouds == 1 ? 0 : a.group_cloud[grp];
+        if (cloud != cur) {
+            if (lane == 0) load_unit_ctx(sm.u[w], a, cloud);
+            cur = cloud;
+            __syncwarp();
         }
-        sm.q[w][lane] = qv;  // rows >= nb hold NaN queries and never hit
-        const int32_t nchunks = (M + 31) >> 5;
-        const bool stage = a.stage_cap > 0 && nchunks <= kSegChunks;
-        const int Q = nb <= 8 ? 8 : (nb <= 16 ? 16 : 32);
-        const int lq = lane & (Q - 1);      // this lane's query
-        const int ls = lane / Q;            // this lane's stream
-        __syncwarp();
-        const float4 myq = sm.q[w][lq];
-        const float qs = query_share<MODE>(myq.w);
-        const float band = exact_all ? __int_as_float(0x7f800000) : query_band<MODE>(myq.w, rmax);
-        const float4* my_cand = &sm.cand[w][ls * (Q + 1)];
-        // Lane k of chunk c holds candidate 32c + k.  Its stencil cell r only moves forward from
-        // chunk to chunk, so it is tracked incrementally instead of searched.
-        int32_t cr = 0;
-        const int32_t* pre = sm.pre[w];
-        const int32_t* begs = sm.beg[w];
-        const float4* __restrict__ rs = a.rsorted;
-        const int32_t* __restrict__ ri = a.rsidx;
-        const int32_t* __restrict__ rid = a.ref_ids;
-        auto fetch = [&cr, pre, begs, rs, ri, rid, M, nan4](int32_t k, float4& v, int32_t& jo) {
-            v = nan4;
-            jo = 0;
-            if (k < M) {
-                while (pre[cr + 1] <= k) ++cr;
-                const int32_t j = begs[cr] + (k - pre[cr]);
-                v = __ldg(&rs[j]);
-                jo = __ldg(&ri[j]);
-                if (rid) jo = __ldg(&rid[jo]);
-            }
-        };
-        // the unit's chunk loop; `exact` redoes it deciding in-band pairs with the reference test
-        int32_t qcount = 0;
-        bool unc = false;
-        for (int pass = 0; pass < 2; ++pass) {
-            const bool exact = pass == 1;
-            cr = 0;
-            qcount = 0;
-            float4 nxt;
-            int32_t nxt_j;
-            fetch(lane, nxt, nxt_j);
-            for (int32_t c = 0; c < nchunks; ++c) {
-                // stage candidate `lane` of this chunk: stream lane / Q, slot lane % Q
-                sm.cand[w][(lane / Q) * (Q + 1) + (lane & (Q - 1))] = nxt;
-                if (stage) sm.sj[w][c][lane] = nxt_j;
-                fetch(((c + 1) << 5) + lane, nxt, nxt_j);  // prefetch the next chunk's candidate
-                __syncwarp();
-                uint32_t m;
-                if (exact) {
-                    m = stream_mask_exact<DIM, PERIODIC, MODE>(xc, my_cand, Q, myq, qs, band) << (Q == 32 ? 0 : Q * ls);
-                } else if (Q == 32) {
-                    m = stream_mask<DIM, PERIODIC, MODE, 32>(xc, my_cand, myq, qs, band, unc);
-                } else if (Q == 16) {
-                    m = stream_mask<DIM, PERIODIC, MODE, 16>(xc, my_cand, myq, qs, band, unc) << (16 * ls);
-                } else {
-                    m = stream_mask<DIM, PERIODIC, MODE, 8>(xc, my_cand, myq, qs, band, unc) << (8 * ls);
-                }
-                if (Q <= 16) m |= __shfl_xor_sync(0xffffffffu, m, 16);
-                if (Q == 8) m |= __shfl_xor_sync(0xffffffffu, m, 8);
-                if (lane < nb) {
-                    qcount += __popc(m);
-                    if (stage) sm.mask[w][lane * kMaskStride + c] = m;
-                }
-                __syncwarp();
-            }
-            if (exact || !__any_sync(0xffffffffu, unc)) break;
+        if (sm.u[w].error) {  // no grid: nothing found, nothing staged
+            if (lane == 0) a.rec[unit] = -1;
+            continue;
         }
-        if (active) a.counts[qorig] = qcount;
-        bool staged = false;
-        if (stage) {
-            // record: [nchunks] [masks: nb x nchunks, query-major] [candidates: nchunks x 32]
-            const int64_t words = 1 + (int64_t)nb * nchunks + 32 * (int64_t)nchunks;
-            unsigned long long base = 0;
-            if (lane == 0) base = atomicAdd(a.cursor, (unsigned long long)words);
-            base = __shfl_sync(0xffffffffu, base, 0);
-            staged = base + (unsigned long long)words <= (unsigned long long)a.stage_cap;
-            if (staged) {
-                int32_t* r = a.stage + base;
-                if (lane == 0) {
-                    r[0] = nchunks;
-                    a.rec[unit] = (int32_t)base;
-                }
-                __syncwarp();
-                for (int q = 0; q < nb; ++q)
-                    if (lane < nchunks) r[1 + q * nchunks + lane] = sm.mask[w][q * kMaskStride + lane];
-                int32_t* rj = r + 1 + nb * nchunks;
-                for (int32_t c = 0; c < nchunks; ++c) rj[c * 32 + lane] = sm.sj[w][c][lane];
+        if constexpr (DIM == 0) {
+            switch (sm.u[w].dim * 2 + (sm.u[w].periodic_mask != 0 ? 1 : 0)) {
+                case 2: count_unit<1, false, MODE>(a, sm, unit, grp, lane, w); break;
+                case 3: count_unit<1, true, MODE>(a, sm, unit, grp, lane, w); break;
+                case 4: count_unit<2, false, MODE>(a, sm, unit, grp, lane, w); break;
+                case 5: count_unit<2, true, MODE>(a, sm, unit, grp, lane, w); break;
+                case 6: count_unit<3, false, MODE>(a, sm, unit, grp, lane, w); break;
+                default: count_unit<3, true, MODE>(a, sm, unit, grp, lane, w); break;
             }
+        } else {
+            count_unit<DIM, PERIODIC, MODE>(a, sm, unit, grp, lane, w);
         }
-        if (!staged && lane == 0) {
-            int32_t f = atomicAdd(a.num_flagged, 1);
-            a.flagged[f] = unit;
-        }
-        __syncwarp();
     }
 }
 
-// Pass 2 for flagged units: walk again and write the pairs straight to their slots.
+struct EmitSmem {
+    int32_t pre[kWalkWarps][33];
+    int32_t beg[kWalkWarps][32];
+    float4 q[kWalkWarps][32];
+    UnitCtx u[kWalkWarps];
+};
+
+// Emit walk of one unit that was not staged: walk again and write the pairs straight to their slots.
+template <int DIM, bool PERIODIC, int MODE>
+__device__ __forceinline__ void emit_unit(const WalkArgs& a, EmitSmem& sm, int32_t unit, int32_t grp, int lane,
+                                          int w) {
+    constexpr int S = DIM == 1 ? 3 : (DIM == 2 ? 9 : 27);
+    const UnitCtx& u = sm.u[w];
+    const ExactCtx xc = unit_exact_ctx(u, MODE);
+    const float qmax = u.qmax;
+    const bool exact_all = u.exact_all != 0;
+    const unsigned lt = (1u << lane) - 1u;
+    const float4 nan4 = make_float4(__int_as_float(0x7fc00000), 0.f, 0.f, 0.f);
+    const int32_t t0 = a.unit_t0[unit];
+    const int32_t nb = min(32, a.group_start[grp + 1] - t0);
+    const int32_t gc[3] = {a.group_coords[3 * grp], a.group_coords[3 * grp + 1], a.group_coords[3 * grp + 2]};
+    int32_t beg = 0, cnt = 0;
+    if (lane < S) stencil_lookup(a, u, gc, lane, beg, cnt);
+    const int32_t inc = warp_inclusive_scan(cnt);
+    sm.pre[w][lane + 1] = inc;
+    if (lane == 0) sm.pre[w][0] = 0;
+    sm.beg[w][lane] = beg;
+    const int32_t M = __shfl_sync(0xffffffffu, inc, 31);
+    int32_t qorig = 0;
+    float4 qv = nan4;
+    int64_t obase = 0;
+    if (lane < nb) {
+        const int32_t t = t0 + lane;
+        qv = a.qsorted[t];
+        qorig = a.qsidx[t];
+        int32_t qc[3];
+        cell_of(DIM, u.dedupe, u.dmin, u.hcell, u.count, qv, qc);
+        if (same_cell<DIM>(qc, gc)) obase = a.offsets[qorig];
+        else qv = nan4;  // stray: written by the serial kernel
+    }
+    sm.q[w][lane] = qv;
+    __syncwarp();
+    for (int32_t base = 0; base < M; base += 32) {
+        const int32_t k = base + lane;
+        float4 cv = nan4;
+        int32_t j = 0;
+        if (k < M) {
+            j = cand_index(sm.pre[w], sm.beg[w], S, k);
+            cv = __ldg(&a.rsorted[j]);
+        }
+        int32_t jl = __ldg(&a.rsidx[j]);
+        jl = a.ref_ids ? __ldg(&a.ref_ids[jl]) : jl - u.rshift;
+        const int64_t jorig = (int64_t)jl;
+        const float cw = cand_share<MODE>(cv.w);
+        const float band = exact_all ? __int_as_float(0x7f800000) : cand_band<MODE>(cw, qmax);
+        for (int qi = 0; qi < nb; ++qi) {
+            const float4 q = sm.q[w][qi];
+            bool in, unc;
+            lean_test<DIM, PERIODIC, MODE>(xc, q, cv, cw, band, in, unc);
+            const uint32_t ub = __ballot_sync(0xffffffffu, unc);
+            if (ub) in = unc ? exact_pair_test(xc, q, q.w, cv, cv.w) : in;
+            const uint32_t b = __ballot_sync(0xffffffffu, in);
+            const int64_t qb = __shfl_sync(0xffffffffu, obase, qi);
+            int32_t qrow = __shfl_sync(0xffffffffu, qorig, qi);
+            qrow = a.query_ids ? __ldg(&a.query_ids[qrow]) : qrow - u.qshift;
+            if (in) {
+                const int64_t pos = qb + __popc(b & lt);
+                if (pos < a.out_cap) {
+                    a.col_out[pos] = jorig;
+                    if (a.row_out) a.row_out[pos] = (int64_t)qrow;
+                }
+            }
+            if (lane == qi) obase += __popc(b);
+        }
+    }
+    __syncwarp();
+}
+
 template <int DIM, bool PERIODIC, int MODE>
 __global__ void __launch_bounds__(kWalkWarps * 32) walk_emit_kernel(WalkArgs a) {
-    if (a.g->error) return;
-    __shared__ int32_t s_pre[kWalkWarps][33];
-    __shared__ int32_t s_beg[kWalkWarps][32];
-    __shared__ float4 s_q[kWalkWarps][32];
+    __shared__ EmitSmem sm;
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-    const unsigned lt = (1u << lane) - 1u;
-    constexpr int S = DIM == 1 ? 3 : (DIM == 2 ? 9 : 27);
-    const ExactCtx xc = exact_ctx(a.sp);
-    const float qmax = a.qp->qmax;
-    const bool exact_all = a.qp->exact_all != 0;
     const int32_t nlist = *a.num_list;
-    const float4 nan4 = make_float4(__int_as_float(0x7fc00000), 0.f, 0.f, 0.f);
+    int cur = -1;
     for (;;) {
         int32_t li = 0;
         if (lane == 0) li = atomicAdd(&a.work[1], 1);
@@ -958,72 +1334,33 @@ __global__ void __launch_bounds__(kWalkWarps * 32) walk_emit_kernel(WalkArgs a) 
         if (li >= nlist) break;
         const int32_t unit = a.unit_list[li];
         const int32_t grp = a.unit_group[unit];
-        const int32_t t0 = a.unit_t0[unit];
-        const int32_t nb = min(32, a.group_start[grp + 1] - t0);
-        const int32_t gc[3] = {a.group_coords[3 * grp], a.group_coords[3 * grp + 1], a.group_coords[3 * grp + 2]};
-        int32_t beg = 0, cnt = 0;
-        if (lane < S) stencil_lookup(a, gc, lane, beg, cnt);
-        const int32_t inc = warp_inclusive_scan(cnt);
-        s_pre[w][lane + 1] = inc;
-        if (lane == 0) s_pre[w][0] = 0;
-        s_beg[w][lane] = beg;
-        const int32_t M = __shfl_sync(0xffffffffu, inc, 31);
-        int32_t qorig = 0;
-        float4 qv = nan4;
-        int64_t obase = 0;
-        if (lane < nb) {
-            const int32_t t = t0 + lane;
-            qv = a.qsorted[t];
-            qorig = a.qsidx[t];
-            int32_t qc[3];
-            point_cell(a.sp, a.g, qv, qc);
-            if (same_cell<DIM>(qc, gc)) obase = a.offsets[qorig];
-            else qv = nan4;  // stray: written by the serial kernel
+        const int cloud = a.num_clouds == 1 ? 0 : a.group_cloud[grp];
+        if (cloud != cur) {
+            if (lane == 0) load_unit_ctx(sm.u[w], a, cloud);
+            cur = cloud;
+            __syncwarp();
         }
-        s_q[w][lane] = qv;
-        __syncwarp();
-        for (int32_t base = 0; base < M; base += 32) {
-            const int32_t k = base + lane;
-            float4 cv = nan4;
-            int32_t j = 0;
-            if (k < M) {
-                j = cand_index(s_pre[w], s_beg[w], S, k);
-                cv = __ldg(&a.rsorted[j]);
+        if (sm.u[w].error) continue;
+        if constexpr (DIM == 0) {
+            switch (sm.u[w].dim * 2 + (sm.u[w].periodic_mask != 0 ? 1 : 0)) {
+                case 2: emit_unit<1, false, MODE>(a, sm, unit, grp, lane, w); break;
+                case 3: emit_unit<1, true, MODE>(a, sm, unit, grp, lane, w); break;
+                case 4: emit_unit<2, false, MODE>(a, sm, unit, grp, lane, w); break;
+                case 5: emit_unit<2, true, MODE>(a, sm, unit, grp, lane, w); break;
+                case 6: emit_unit<3, false, MODE>(a, sm, unit, grp, lane, w); break;
+                default: emit_unit<3, true, MODE>(a, sm, unit, grp, lane, w); break;
             }
-            int32_t jl = __ldg(&a.rsidx[j]);
-            if (a.ref_ids) jl = __ldg(&a.ref_ids[jl]);
-            const int64_t jorig = (int64_t)jl;
-            const float cw = cand_share<MODE>(cv.w);
-            const float band = exact_all ? __int_as_float(0x7f800000) : cand_band<MODE>(cw, qmax);
-            for (int qi = 0; qi < nb; ++qi) {
-                const float4 q = s_q[w][qi];
-                bool in, unc;
-                lean_test<DIM, PERIODIC, MODE>(a.sp, q, cv, cw, band, in, unc);
-                const uint32_t ub = __ballot_sync(0xffffffffu, unc);
-                if (ub) in = unc ? exact_pair_test(xc, q, q.w, cv, cv.w) : in;
-                const uint32_t b = __ballot_sync(0xffffffffu, in);
-                const int64_t qb = __shfl_sync(0xffffffffu, obase, qi);
-                int32_t qrow = __shfl_sync(0xffffffffu, qorig, qi);
-                if (a.query_ids) qrow = __ldg(&a.query_ids[qrow]);
-                if (in) {
-                    const int64_t pos = qb + __popc(b & lt);
-                    if (pos < a.out_cap) {
-                        a.col_out[pos] = jorig;
-                        if (a.row_out) a.row_out[pos] = (int64_t)qrow;
-                    }
-                }
-                if (lane == qi) obase += __popc(b);
-            }
+        } else {
+            emit_unit<DIM, PERIODIC, MODE>(a, sm, unit, grp, lane, w);
         }
-        __syncwarp();
     }
 }
 
-// Pass 2 for staged units: expand each unit's record into its queries' CSR/COO slots, one warp
-// per unit.  The warp stages the unit's mask block in shared memory; lane q expands query q's hit
-// bits into a shared output table (source chunk and bit of each of the unit's outputs, in output
-// order); then lanes = output positions read the table and write consecutive slots.  A unit with
-// more than kExpandTab outputs locates each output by binary searches over the prefixes instead.
+// Emit pass for staged units: expand each unit's record into its queries' CSR/COO slots, one warp
+// per unit.  Lane q expands query q's hit bits into a shared output table (source chunk and bit of
+// each of the unit's outputs, in output order); then lanes = output positions read the table and
+// write consecutive slots.  A unit with more than kExpandTab outputs locates each output by binary
+// searches over the prefixes instead.
 constexpr int kExpandWarps = 8;
 constexpr int kExpandTab = 2048;
 struct ExpandSmem {
@@ -1033,42 +1370,59 @@ struct ExpandSmem {
     int32_t qrow[kExpandWarps][32];
 };
 
-__global__ void __launch_bounds__(kExpandWarps * 32) expand_records_kernel(
-    const int32_t* __restrict__ stage, const int32_t* __restrict__ rec, const int32_t* __restrict__ num_units,
-    const int32_t* __restrict__ unit_t0, const int32_t* __restrict__ unit_group,
-    const int32_t* __restrict__ group_start, const int32_t* __restrict__ qsidx, const int64_t* __restrict__ offsets,
-    const int32_t* __restrict__ query_ids, int64_t* __restrict__ row_out, int64_t* __restrict__ col_out,
-    int64_t out_cap) {
+struct ExpandArgs {
+    const int32_t* __restrict__ stage;
+    const int32_t* __restrict__ rec;
+    const int32_t* __restrict__ num_units;
+    const int32_t* __restrict__ unit_t0;
+    const int32_t* __restrict__ unit_group;
+    const int32_t* __restrict__ group_start;
+    const int32_t* __restrict__ group_cloud;
+    const int32_t* __restrict__ qsidx;
+    const int64_t* __restrict__ offsets;
+    const int32_t* __restrict__ query_ids;
+    const CloudParams* __restrict__ table;
+    int32_t num_clouds;
+    int32_t local_index;
+    int64_t* __restrict__ row_out;
+    int64_t* __restrict__ col_out;
+    int64_t out_cap;
+};
+
+__global__ void __launch_bounds__(kExpandWarps * 32) expand_records_kernel(ExpandArgs a) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     ExpandSmem& sm = *reinterpret_cast<ExpandSmem*>(smem_raw);
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-    const int32_t nu = *num_units;
+    const int32_t nu = *a.num_units;
     const int64_t warps = (int64_t)gridDim.x * kExpandWarps;
     uint16_t* tab = sm.tab[w];
     int64_t u = (int64_t)blockIdx.x * kExpandWarps + w;
-    int32_t r0n = u < nu ? rec[u] : -1;
-    int32_t t0n = u < nu ? unit_t0[u] : 0;
-    int32_t gn = u < nu ? unit_group[u] : 0;
+    int32_t r0n = u < nu ? a.rec[u] : -1;
+    int32_t t0n = u < nu ? a.unit_t0[u] : 0;
+    int32_t gn = u < nu ? a.unit_group[u] : 0;
     for (; u < nu; u += warps) {
         const int32_t r0 = r0n, t0 = t0n, grp = gn;
         if (u + warps < nu) {  // the next unit's header, ahead of its use
-            r0n = rec[u + warps];
-            t0n = unit_t0[u + warps];
-            gn = unit_group[u + warps];
+            r0n = a.rec[u + warps];
+            t0n = a.unit_t0[u + warps];
+            gn = a.unit_group[u + warps];
         }
         if (r0 < 0) continue;  // re-tested by the emit walk
-        const int32_t* r = stage + r0;
+        const int32_t* r = a.stage + r0;
         const int32_t nchunks = r[0];
         if (nchunks <= 0) continue;  // no candidates, no outputs
-        const int32_t nb = min(32, group_start[grp + 1] - t0);
+        const int32_t nb = min(32, a.group_start[grp + 1] - t0);
         const int32_t nm = nb * nchunks;
         const uint32_t* mk = reinterpret_cast<const uint32_t*>(r + 1);  // [query][chunk]
         const int32_t* cands = r + 1 + nm;                               // [chunk][32]
         int32_t total = 0;
         if (lane < nb) {
-            const int32_t row = qsidx[t0 + lane];
-            sm.qrow[w][lane] = query_ids ? query_ids[row] : row;
-            sm.qoff[w][lane] = offsets[row];
+            const int32_t row = a.qsidx[t0 + lane];
+            int32_t qrow = row;
+            if (a.query_ids) qrow = a.query_ids[row];
+            else if (a.local_index) qrow -= a.table[a.num_clouds == 1 ? 0 : a.group_cloud[grp]].query_base;
+            sm.qrow[w][lane] = qrow;
+            sm.qoff[w][lane] = a.offsets[row];
             for (int c = 0; c < nchunks; ++c) total += __popc(mk[lane * nchunks + c]);
         }
         const int32_t qinc = warp_inclusive_scan(total);
@@ -1102,9 +1456,9 @@ __global__ void __launch_bounds__(kExpandWarps * 32) expand_records_kernel(
                 const int32_t v = tab[o];
                 const int q = v >> 10;
                 const int64_t pos = sm.qoff[w][q] + (o - sm.qpre[w][q]);
-                if (pos < out_cap) {
-                    col_out[pos] = (int64_t)cands[v & 0x3ff];
-                    if (row_out) row_out[pos] = (int64_t)sm.qrow[w][q];
+                if (pos < a.out_cap) {
+                    a.col_out[pos] = (int64_t)cands[v & 0x3ff];
+                    if (a.row_out) a.row_out[pos] = (int64_t)sm.qrow[w][q];
                 }
             }
         } else {
@@ -1126,9 +1480,9 @@ __global__ void __launch_bounds__(kExpandWarps * 32) expand_records_kernel(
                 if (c >= nchunks) continue;
                 const int bit = __fns(mk[q * nchunks + c], 0, tq + 1);
                 const int64_t pos = sm.qoff[w][q] + (o - sm.qpre[w][q]);
-                if (pos < out_cap) {
-                    col_out[pos] = (int64_t)cands[c * 32 + bit];
-                    if (row_out) row_out[pos] = (int64_t)sm.qrow[w][q];
+                if (pos < a.out_cap) {
+                    a.col_out[pos] = (int64_t)cands[c * 32 + bit];
+                    if (a.row_out) a.row_out[pos] = (int64_t)sm.qrow[w][q];
                 }
             }
         }
@@ -1139,29 +1493,31 @@ __global__ void __launch_bounds__(kExpandWarps * 32) expand_records_kernel(
 // Serial walk for queries whose own cell differs from their group's (one thread per query).
 template <bool EMIT>
 __global__ void stray_kernel(WalkArgs a) {
-    if (a.g->error) return;
     const int32_t ns = *a.num_stray;
-    const int S = a.sp.dim == 1 ? 3 : (a.sp.dim == 2 ? 9 : 27);
-    const ExactCtx xc = exact_ctx(a.sp);
     for (int32_t s = blockIdx.x * blockDim.x + threadIdx.x; s < ns; s += gridDim.x * blockDim.x) {
         const int32_t t = a.stray[s];
         const float4 q = a.qsorted[t];
         const int32_t qorig = a.qsidx[t];
+        UnitCtx u;
+        load_unit_ctx(u, a, cloud_of(a.query_prefix, a.num_clouds, qorig));
+        if (u.error) continue;
+        const int S = u.dim == 1 ? 3 : (u.dim == 2 ? 9 : 27);
+        const ExactCtx xc = unit_exact_ctx(u, a.mode);
         int32_t qc[3];
-        point_cell(a.sp, a.g, q, qc);
+        cell_of(u.dim, u.dedupe, u.dmin, u.hcell, u.count, q, qc);
         int64_t pos = EMIT ? a.offsets[qorig] : 0;
         int32_t n = 0;
         for (int o = 0; o < S; ++o) {
             int32_t beg, cnt;
-            stencil_lookup(a, qc, o, beg, cnt);
+            stencil_lookup(a, u, qc, o, beg, cnt);
             for (int32_t j = beg; j < beg + cnt; ++j) {
                 const float4 cv = a.rsorted[j];
                 if (exact_pair_test(xc, q, q.w, cv, cv.w)) {
                     if (EMIT) {
                         if (pos < a.out_cap) {
                             const int32_t jl = a.rsidx[j];
-                            a.col_out[pos] = (int64_t)(a.ref_ids ? a.ref_ids[jl] : jl);
-                            if (a.row_out) a.row_out[pos] = a.query_ids ? a.query_ids[qorig] : qorig;
+                            a.col_out[pos] = (int64_t)(a.ref_ids ? a.ref_ids[jl] : jl - u.rshift);
+                            if (a.row_out) a.row_out[pos] = a.query_ids ? a.query_ids[qorig] : qorig - u.qshift;
                         }
                         ++pos;
                     } else {
@@ -1192,13 +1548,13 @@ struct OffsetOut {
     }
 };
 
-__global__ void info_kernel(const GridParams* g, const int64_t* total, const int32_t* num_stray,
-                            const QueryParams* qp, const unsigned long long* cursor, const int32_t* num_flagged,
+__global__ void info_kernel(const int32_t* bad_grids, const int64_t* total, const int32_t* num_stray,
+                            const int32_t* exact_clouds, const unsigned long long* cursor, const int32_t* num_flagged,
                             int64_t* info) {
     info[0] = *total;
-    info[1] = g->error;
+    info[1] = *bad_grids;
     info[2] = *num_stray;
-    info[3] = qp->exact_all;
+    info[3] = *exact_clouds;
     info[4] = (int64_t)*cursor;
     info[5] = *num_flagged;
     info[6] = 0;
@@ -1208,55 +1564,155 @@ __global__ void info_kernel(const GridParams* g, const int64_t* total, const int
 // ------------------------------------------------------------------------------------------
 // host orchestration
 
-static SearchParams make_params(const tcr_search_desc* d) {
-    SearchParams sp;
-    memset(&sp, 0, sizeof(sp));
-    sp.dim = d->dim;
-    sp.mode = d->mode;
-    sp.periodic_mask = d->periodic_mask;
-    sp.hash_len = (uint32_t)d->hash_map_length;
-    for (int k = 0; k < 3; ++k) {
-        sp.dmin[k] = k < d->dim ? d->domain_min[k] : 0.f;
-        sp.dmax[k] = k < d->dim ? d->domain_max[k] : 1.f;
-        sp.ext[k] = sp.dmax[k] - sp.dmin[k];
-    }
-    sp.n_query = d->n_query;
-    sp.n_ref = d->n_ref;
-    for (int k = 0; k < 3; ++k) sp.hcell_override[k] = d->hcell[0] > 0.0f ? (k < d->dim ? d->hcell[k] : 1.0f) : 0.0f;
-    sp.dedupe = d->clamped_grid ? 1 : 0;
-    return sp;
+// One search as the kernels see it: the cloud table plus what holds for all clouds.
+struct HostBatch {
+    int32_t C = 0, mode = 0, self = 0, local_index = 0;
+    std::vector<CloudParams> clouds;
+    int64_t nq = 0, nr = 0, map_total = 0;
+    const int32_t* query_ids = nullptr;
+    const int32_t* ref_ids = nullptr;
+    bool any_query_sup = false, any_ref_sup = false;
+    bool same_sorted = false;     // self search, no periodic dims, queries are the references (same arrays)
+    bool same_positions = false;  // self search, no periodic dims, same position arrays
+    int walk_class = 0;           // dim * 2 + (any periodic dim) when every cloud shares it, else 0
+    bool wide = false;            // 64-bit (cloud, cell) sort keys
+};
+
+// Validation shared by both descriptors.  level 0: sizes only; 1: query phases (the reference
+// supports come from the structure); 2: structure build.
+static int check_cloud(const char* who, int dim, int mode, int64_t L, int64_t nq, int64_t nr, const void* qpos,
+                       const void* qsup, const void* rpos, const void* rsup, int self, int level) {
+    if (dim < 1 || dim > 3) return set_error(TCR_ERR_INVALID, "%sdim must be 1, 2 or 3 (got %d)", who, dim);
+    if (mode < 0 || mode > 3) return set_error(TCR_ERR_INVALID, "%sinvalid mode %d", who, mode);
+    if (nq < 0 || nr < 0 || nq > 0x7fffffffLL || nr > 0x7ffffff0LL)
+        return set_error(TCR_ERR_INVALID, "%spoint counts must be in [0, 2^31)", who);
+    if (self && nq != nr) return set_error(TCR_ERR_INVALID, "%sself search needs one cloud", who);
+    if (level == 0) return TCR_OK;
+    if (L <= 0 || L > 0xffffffffLL) return set_error(TCR_ERR_INVALID, "%shashMapLength must be in [1, 2^32)", who);
+    if ((nq && !qpos) || (nr && !rpos)) return set_error(TCR_ERR_INVALID, "%smissing positions", who);
+    if ((mode == kGather || mode == kSymmetric || mode == kSuperSymmetric) && nq && !qsup)
+        return set_error(TCR_ERR_INVALID, "%sthis mode needs query supports", who);
+    if (level >= 2 && (mode == kScatter || mode == kSymmetric || mode == kSuperSymmetric) && nr && !rsup)
+        return set_error(TCR_ERR_INVALID, "%sthis mode needs reference supports", who);
+    return TCR_OK;
 }
 
-// need_ref_sup: the structure build reads reference supports; the query phases take them from
-// the structure and only need the query supports.
-static int validate(const tcr_search_desc* d, bool need_ref_sup = true) {
+static int finish_batch(HostBatch& b, int64_t map_min) {
+    int64_t qb = 0, rb = 0, mb = 0;
+    bool same_pos = b.self != 0, same_sorted = b.self != 0;
+    int cls = -1;
+    bool mixed = false;
+    b.any_query_sup = b.any_ref_sup = false;
+    for (CloudParams& cp : b.clouds) {
+        cp.query_base = (int32_t)qb;
+        cp.ref_base = (int32_t)rb;
+        qb += cp.n_query;
+        rb += cp.n_ref;
+        if (qb > 0x7ffffff0LL || rb > 0x7ffffff0LL)
+            return set_error(TCR_ERR_INVALID, "the clouds hold more than 2^31 query or reference points");
+        cp.map_cap = hash_capacity(cp.n_ref, map_min);
+        cp.map_base = mb;
+        mb += cp.map_cap;
+        same_pos = same_pos && cp.periodic_mask == 0 && cp.query_pos == cp.ref_pos;
+        same_sorted = same_sorted && cp.periodic_mask == 0 && cp.query_pos == cp.ref_pos && cp.query_sup == cp.ref_sup;
+        b.any_query_sup = b.any_query_sup || cp.query_sup != nullptr;
+        b.any_ref_sup = b.any_ref_sup || cp.ref_sup != nullptr;
+        const int c = cp.dim * 2 + (cp.periodic_mask != 0 ? 1 : 0);
+        if (cls < 0) cls = c;
+        else if (c != cls) mixed = true;
+    }
+    b.nq = qb;
+    b.nr = rb;
+    b.map_total = mb;
+    b.same_positions = same_pos;
+    b.same_sorted = same_sorted;
+    b.walk_class = mixed ? 0 : cls;
+    b.wide = b.C > 1;
+    return TCR_OK;
+}
+
+static void fill_domain(CloudParams& cp, int dim, const float* lo, const float* hi) {
+    for (int k = 0; k < 3; ++k) {
+        cp.dmin[k] = k < dim ? lo[k] : 0.f;
+        cp.dmax[k] = k < dim ? hi[k] : 1.f;
+        cp.ext[k] = cp.dmax[k] - cp.dmin[k];
+    }
+}
+
+static int batch_of_desc(const tcr_search_desc* d, int level, HostBatch& b) {
     if (!d) return set_error(TCR_ERR_INVALID, "null descriptor");
-    if (d->dim < 1 || d->dim > 3) return set_error(TCR_ERR_INVALID, "dim must be 1, 2 or 3 (got %d)", d->dim);
-    if (d->mode < 0 || d->mode > 3) return set_error(TCR_ERR_INVALID, "invalid mode %d", d->mode);
-    if (d->hash_map_length <= 0 || d->hash_map_length > 0xffffffffLL)
-        return set_error(TCR_ERR_INVALID, "hashMapLength must be in [1, 2^32)");
-    if (d->n_query < 0 || d->n_ref < 0 || d->n_query > 0x7fffffffLL || d->n_ref > 0x7ffffff0LL)
-        return set_error(TCR_ERR_INVALID, "point counts must be in [0, 2^31)");
-    if ((d->n_query && !d->query_pos) || (d->n_ref && !d->ref_pos))
-        return set_error(TCR_ERR_INVALID, "missing positions");
-    if ((d->mode == kGather || d->mode == kSymmetric || d->mode == kSuperSymmetric) && d->n_query && !d->query_sup)
-        return set_error(TCR_ERR_INVALID, "this mode needs query supports");
-    if (need_ref_sup && (d->mode == kScatter || d->mode == kSymmetric || d->mode == kSuperSymmetric) && d->n_ref &&
-        !d->ref_sup)
-        return set_error(TCR_ERR_INVALID, "this mode needs reference supports");
-    if (d->self_search && d->n_query != d->n_ref)
-        return set_error(TCR_ERR_INVALID, "self search needs one cloud");
+    int rc = check_cloud("", d->dim, d->mode, d->hash_map_length, d->n_query, d->n_ref, d->query_pos, d->query_sup,
+                         d->ref_pos, d->ref_sup, d->self_search, level);
+    if (rc) return rc;
     if (d->hcell[0] > 0.0f)
         for (int k = 0; k < d->dim; ++k)
             if (!(d->hcell[k] > 0.0f) || !(d->hcell[k] < 3.0e38f))
                 return set_error(TCR_ERR_INVALID, "cell size override must be positive and finite in every dimension");
-    return TCR_OK;
+    CloudParams cp;
+    memset(&cp, 0, sizeof(cp));
+    cp.dim = d->dim;
+    cp.mode = d->mode;
+    cp.periodic_mask = d->periodic_mask;
+    cp.hash_len = (uint32_t)d->hash_map_length;
+    fill_domain(cp, d->dim, d->domain_min, d->domain_max);
+    for (int k = 0; k < 3; ++k) cp.hcell_override[k] = d->hcell[0] > 0.0f ? (k < d->dim ? d->hcell[k] : 1.0f) : 0.0f;
+    cp.dedupe = d->clamped_grid ? 1 : 0;
+    cp.n_query = (int32_t)d->n_query;
+    cp.n_ref = (int32_t)d->n_ref;
+    cp.query_pos = d->query_pos;
+    cp.query_sup = d->query_sup;
+    cp.ref_pos = d->ref_pos;
+    cp.ref_sup = d->ref_sup;
+    b = HostBatch();
+    b.C = 1;
+    b.mode = d->mode;
+    b.self = d->self_search ? 1 : 0;
+    b.query_ids = d->query_ids;
+    b.ref_ids = d->ref_ids;
+    b.clouds.push_back(cp);
+    return finish_batch(b, kSingleMapMin);
 }
 
-// Self search on one cloud with no periodic dimension: the queries, wrapped once, are the
-// references, wrapped twice, so the sorted query array is the sorted reference array.
-static inline bool same_sorted_points(const tcr_search_desc* d) {
-    return d->self_search && d->periodic_mask == 0 && d->query_pos == d->ref_pos && d->query_sup == d->ref_sup;
+static int batch_of(const tcr_batch_desc* bd, int level, HostBatch& b) {
+    if (!bd) return set_error(TCR_ERR_INVALID, "null batch descriptor");
+    if (bd->n_clouds < 1 || bd->n_clouds > (1 << 22))
+        return set_error(TCR_ERR_INVALID, "n_clouds must be in [1, 2^22] (got %d)", bd->n_clouds);
+    if (!bd->clouds) return set_error(TCR_ERR_INVALID, "missing cloud table");
+    b = HostBatch();
+    b.C = bd->n_clouds;
+    b.mode = bd->mode;
+    b.self = bd->self_search ? 1 : 0;
+    b.local_index = bd->local_index ? 1 : 0;
+    b.query_ids = bd->query_ids;
+    b.ref_ids = bd->ref_ids;
+    b.clouds.resize(bd->n_clouds);
+    char who[48];
+    for (int k = 0; k < bd->n_clouds; ++k) {
+        const tcr_cloud_desc& c = bd->clouds[k];
+        snprintf(who, sizeof(who), "cloud %d: ", k);
+        int rc = check_cloud(who, c.dim, bd->mode, c.hash_map_length, c.n_query, c.n_ref, c.query_pos, c.query_sup,
+                             c.ref_pos, c.ref_sup, bd->self_search, level);
+        if (rc) return rc;
+        CloudParams& cp = b.clouds[k];
+        memset(&cp, 0, sizeof(cp));
+        cp.dim = c.dim;
+        cp.mode = bd->mode;
+        cp.periodic_mask = c.periodic_mask & ((1 << c.dim) - 1);
+        cp.hash_len = (uint32_t)c.hash_map_length;
+        fill_domain(cp, c.dim, c.domain_min, c.domain_max);
+        cp.n_query = (int32_t)c.n_query;
+        cp.n_ref = (int32_t)c.n_ref;
+        cp.query_pos = c.query_pos;
+        cp.query_sup = c.query_sup;
+        cp.ref_pos = c.ref_pos;
+        cp.ref_sup = c.ref_sup;
+    }
+    return finish_batch(b, kBatchMapMin);
+}
+
+static void batch_sizes(const HostBatch& b, int64_t* s, int64_t* w) {
+    if (s) carve_structure(nullptr, b.nr, b.C, b.map_total, s);
+    if (w) carve_scratch(nullptr, b.nq, b.nr, b.C, w);
 }
 
 static inline unsigned grid_for(int64_t n, int threads, int max_blocks = 148 * 16) {
@@ -1264,23 +1720,51 @@ static inline unsigned grid_for(int64_t n, int threads, int max_blocks = 148 * 1
     return (unsigned)std::max<int64_t>(1, std::min<int64_t>(b, max_blocks));
 }
 
-static WalkArgs make_walk(const SearchParams& sp, const Structure& S, const Scratch& W, bool self) {
+static int num_sms() {
+    int dev = 0, nsm = 148;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+    return nsm;
+}
+
+static int upload_table(const HostBatch& b, const Scratch& W, cudaStream_t st) {
+    for (int first = 0; first < b.C; first += kUploadChunk) {
+        CloudChunk ch;
+        memset(&ch, 0, sizeof(ch));
+        ch.first = first;
+        ch.count = std::min(kUploadChunk, b.C - first);
+        ch.n_clouds = b.C;
+        ch.query_total = (int32_t)b.nq;
+        ch.ref_total = (int32_t)b.nr;
+        memcpy(ch.p, &b.clouds[first], sizeof(CloudParams) * ch.count);
+        upload_clouds_kernel<<<1, 32, 0, st>>>(ch, W.table, W.query_prefix, W.ref_prefix);
+        note_launches(1);
+    }
+    TCR_CUDA(cudaGetLastError());
+    return TCR_OK;
+}
+
+static WalkArgs make_walk(const HostBatch& b, const Structure& S, const Scratch& W) {
     WalkArgs a;
     memset(&a, 0, sizeof(a));
-    a.sp = sp;
-    a.g = S.grid;
-    a.qp = W.qparams;
+    a.table = W.table;
+    a.grid = S.grid;
+    a.qparams = W.qparams;
+    a.query_prefix = W.query_prefix;
+    a.num_clouds = b.C;
+    a.local_index = b.local_index;
+    a.mode = b.mode;
+    a.no_stray_check = b.same_positions ? 1 : 0;
     a.rsorted = S.rsorted;
     a.rsidx = S.rsidx;
     a.cell_start = S.cell_start;
-    a.cell_coords = S.cell_coords;
     a.cell_bucket = S.cell_bucket;
     a.map = S.map;
-    a.map_cap = S.map_cap;
-    a.qsorted = W.qsorted;
-    a.qsidx = W.qsidx;
-    a.group_start = self ? S.cell_start : W.qgroup_start;
-    a.group_coords = self ? S.cell_coords : W.qgroup_coords;
+    a.qsorted = b.same_sorted ? S.rsorted : W.qsorted;
+    a.qsidx = b.same_sorted ? S.rsidx : W.qsidx;
+    a.group_start = b.self ? S.cell_start : W.qgroup_start;
+    a.group_coords = b.self ? S.cell_coords : W.qgroup_coords;
+    a.group_cloud = b.self ? S.cell_cloud : W.qgroup_cloud;
     a.unit_group = W.unit_group;
     a.unit_t0 = W.unit_t0;
     a.num_units = W.num_units;
@@ -1294,30 +1778,32 @@ static WalkArgs make_walk(const SearchParams& sp, const Structure& S, const Scra
     a.flagged = W.flagged;
     a.num_flagged = W.num_flagged;
     a.cursor = W.cursor;
+    a.query_ids = b.query_ids;
+    a.ref_ids = b.ref_ids;
     return a;
 }
 
-static int num_sms() {
-    int dev = 0, nsm = 148;
-    cudaGetDevice(&dev);
-    cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
-    return nsm;
-}
-
-// Dispatches a walk kernel template on (dim, any periodic dim, mode).
-template <template <int, bool, int> class K>
-static cudaError_t dispatch_walk(const WalkArgs& a, int dim, bool periodic, int mode, dim3 grid, dim3 block,
-                                 size_t smem, cudaStream_t st) {
-#define TCR_M(D, P)                                                                 \
-    switch (mode) {                                                                 \
-        case kGather: return K<D, P, kGather>::launch(a, grid, block, smem, st);    \
-        case kScatter: return K<D, P, kScatter>::launch(a, grid, block, smem, st);  \
-        case kSymmetric: return K<D, P, kSymmetric>::launch(a, grid, block, smem, st); \
-        default: return K<D, P, kSuperSymmetric>::launch(a, grid, block, smem, st); \
+// Dispatches a walk kernel template on the clouds' class (dim, any periodic dim) and the mode;
+// class 0 is the mixed walk.
+template <template <int, bool, int> class L>
+static cudaError_t dispatch_walk(const WalkArgs& a, int cls, int mode, dim3 grid, dim3 block, size_t smem,
+                                 cudaStream_t st) {
+#define TCR_M(D, P)                                                                    \
+    switch (mode) {                                                                    \
+        case kGather: return L<D, P, kGather>::launch(a, grid, block, smem, st);       \
+        case kScatter: return L<D, P, kScatter>::launch(a, grid, block, smem, st);     \
+        case kSymmetric: return L<D, P, kSymmetric>::launch(a, grid, block, smem, st); \
+        default: return L<D, P, kSuperSymmetric>::launch(a, grid, block, smem, st);    \
     }
-    if (dim == 1) { if (periodic) { TCR_M(1, true) } else { TCR_M(1, false) } }
-    if (dim == 2) { if (periodic) { TCR_M(2, true) } else { TCR_M(2, false) } }
-    if (periodic) { TCR_M(3, true) } else { TCR_M(3, false) }
+    switch (cls) {
+        case 2: TCR_M(1, false)
+        case 3: TCR_M(1, true)
+        case 4: TCR_M(2, false)
+        case 5: TCR_M(2, true)
+        case 6: TCR_M(3, false)
+        case 7: TCR_M(3, true)
+        default: TCR_M(0, true)
+    }
 #undef TCR_M
 }
 
@@ -1345,6 +1831,211 @@ static unsigned walk_blocks(int64_t nq) {
                                                                                              kWalkWarps));
 }
 
+template <typename K>
+static int build_impl(const HostBatch& b, const Structure& S, const Scratch& W, cudaStream_t st) {
+    const SortWorkspaceT<K> sw = sort_workspace<K>(W);
+    const int C = b.C;
+    const int64_t nr = b.nr, nq = b.nq;
+    int rc = upload_table(b, W, st);
+    if (rc) return rc;
+    grid_init_kernel<K><<<grid_for(C, 128), 128, 0, st>>>(S.grid, C, S.bad_grids, sw.state);
+    note_launches(1);
+    // computeGridSupport: which supports set hMax depends on the mode
+    if (b.any_ref_sup && nr > 0) {
+        support_stats_kernel<<<grid_for(nr, 256, num_sms() * 8), 256, 0, st>>>(
+            W.table, W.ref_prefix, C, nr, 0, reinterpret_cast<char*>(S.grid) + offsetof(GridParams, ref_stats),
+            (int64_t)sizeof(GridParams));
+        note_launches(1);
+    }
+    if (b.any_query_sup && nq > 0) {
+        support_stats_kernel<<<grid_for(nq, 256, num_sms() * 8), 256, 0, st>>>(
+            W.table, W.query_prefix, C, nq, 1,
+            reinterpret_cast<char*>(S.grid) + offsetof(GridParams, build_query_stats), (int64_t)sizeof(GridParams));
+        note_launches(1);
+    }
+    grid_params_kernel<<<grid_for(C, 128), 128, 0, st>>>(W.table, S.grid, C, S.bad_grids);
+    note_launches(1);
+    TCR_CUDA(cudaMemsetAsync(S.map, 0xff, sizeof(unsigned long long) * S.map_total, st));
+    TCR_CUDA(cudaMemsetAsync(S.num_cells, 0, sizeof(int32_t), st));
+    if (nr > 0) {
+        pack_points_kernel<K><<<grid_for(nr, 256), 256, 0, st>>>(W.table, S.grid, W.ref_prefix, C, nr, 0, 2, 1, W.pack,
+                                                                 sw.keys[0], sw.vals[0], sw.state);
+        note_launches(1);
+        TCR_CUDA(radix_sort_pairs<K>(sw, nr, st));
+        gather_sorted_kernel<K><<<grid_for(nr, 256), 256, 0, st>>>(W.pack, sw.vals[0], sw.vals[1], sw.state, nr,
+                                                                   S.rsorted, S.rsidx);
+        note_launches(1);
+        CellOut<K> co{W.table, S.grid, sw.keys[0], sw.keys[1], sw.state, S.rsorted, S.cell_start, S.cell_lin,
+                      S.cell_coords, S.cell_bucket, S.cell_cloud, S.map};
+        RunFlagIn<K> fi{sw.keys[0], sw.keys[1], sw.state};
+        TCR_CUDA(device_exclusive_scan<int32_t>(fi, co, nr, W.scan_tiles32, S.num_cells, st));
+    }
+    finish_cells_kernel<<<1, 1, 0, st>>>(S.cell_start, S.num_cells, nr);
+    note_launches(1);
+    TCR_CUDA(cudaGetLastError());
+    return TCR_OK;
+}
+
+template <typename K>
+static int count_impl(const HostBatch& b, const Structure& S, const Scratch& W, int32_t* stage, int64_t stage_cap,
+                      int64_t* offsets, int32_t* indptr_out, int64_t* row_entries_out, int64_t* info_out,
+                      cudaStream_t st) {
+    const int C = b.C;
+    const int64_t nq = b.nq;
+    int rc = upload_table(b, W, st);
+    if (rc) return rc;
+    count_init_kernel<<<grid_for(C, 128), 128, 0, st>>>(W, C);
+    note_launches(1);
+    if (b.any_query_sup && nq > 0) {
+        support_stats_kernel<<<grid_for(nq, 256, num_sms() * 8), 256, 0, st>>>(
+            W.table, W.query_prefix, C, nq, 1, reinterpret_cast<char*>(W.qparams) + offsetof(QueryParams, stats),
+            (int64_t)sizeof(QueryParams));
+        note_launches(1);
+    }
+    query_params_kernel<<<grid_for(C, 128), 128, 0, st>>>(W.table, S.grid, C, W.qparams, W.exact_clouds);
+    note_launches(1);
+    if (nq > 0) {
+        TCR_CUDA(cudaMemsetAsync(W.counts, 0, sizeof(int32_t) * nq, st));
+        const int32_t* gstart;
+        const int32_t* ngroups;
+        if (b.self) {
+            if (!b.same_sorted) {
+                pack_self_queries_kernel<<<grid_for(nq, 256), 256, 0, st>>>(W.table, S.grid, W.query_prefix, C, S.rsidx,
+                                                                            nq, W.qsorted, W.qsidx);
+                note_launches(1);
+            }
+            gstart = S.cell_start;
+            ngroups = S.num_cells;
+        } else {
+            // sort the queries by their own (cloud, cell)
+            const SortWorkspaceT<K> sw = sort_workspace<K>(W);
+            sort_state_init_kernel<K><<<1, 1, 0, st>>>(sw.state);
+            note_launches(1);
+            pack_points_kernel<K><<<grid_for(nq, 256), 256, 0, st>>>(W.table, S.grid, W.query_prefix, C, nq, 1, 1, 0,
+                                                                     W.pack, sw.keys[0], sw.vals[0], sw.state);
+            note_launches(1);
+            TCR_CUDA(radix_sort_pairs<K>(sw, nq, st));
+            gather_sorted_kernel<K><<<grid_for(nq, 256), 256, 0, st>>>(W.pack, sw.vals[0], sw.vals[1], sw.state, nq,
+                                                                       W.qsorted, W.qsidx);
+            note_launches(1);
+            QueryGroupOut<K> qo{W.table, S.grid, sw.keys[0], sw.keys[1], sw.state, W.qsorted,
+                                W.qgroup_start, W.qgroup_coords, W.qgroup_cloud};
+            RunFlagIn<K> fi{sw.keys[0], sw.keys[1], sw.state};
+            TCR_CUDA(device_exclusive_scan<int32_t>(fi, qo, nq, W.scan_tiles32, W.num_qgroups, st));
+            finish_cells_kernel<<<1, 1, 0, st>>>(W.qgroup_start, W.num_qgroups, nq);
+            note_launches(1);
+            gstart = W.qgroup_start;
+            ngroups = W.num_qgroups;
+        }
+        BoundedUnitCountIn ui{gstart, ngroups};
+        BoundedUnitOut uo{gstart, ngroups, W.unit_group, W.unit_t0};
+        TCR_CUDA(device_exclusive_scan<int32_t>(ui, uo, nq, W.scan_tiles32, W.num_units, st));
+        WalkArgs a = make_walk(b, S, W);
+        a.stage = stage;
+        a.stage_cap = stage_cap;
+        TCR_CUDA(dispatch_walk<CountLaunch>(a, b.walk_class, b.mode, dim3(walk_blocks(nq)), dim3(kWalkWarps * 32),
+                                            sizeof(WalkSmem), st));
+        note_launches(1);
+        stray_kernel<false><<<grid_for(nq, 128, num_sms() * 4), 128, 0, st>>>(a);
+        note_launches(1);
+    }
+    CountIn ci{W.counts, nq};
+    OffsetOut oo{nq, offsets, indptr_out, row_entries_out};
+    TCR_CUDA(device_exclusive_scan<int64_t>(ci, oo, nq + 1, W.scan_tiles64, W.total, st));
+    info_kernel<<<1, 1, 0, st>>>(S.bad_grids, W.total, W.num_stray, W.exact_clouds, W.cursor, W.num_flagged, W.info);
+    note_launches(1);
+    if (info_out) TCR_CUDA(cudaMemcpyAsync(info_out, W.info, 8 * sizeof(int64_t), cudaMemcpyDeviceToHost, st));
+    return TCR_OK;
+}
+
+static int emit_impl(const HostBatch& b, const Structure& S, const Scratch& W, const int32_t* stage,
+                     const int64_t* offsets, int64_t* row_out, int64_t* col_out, int64_t out_capacity,
+                     cudaStream_t st) {
+    const int64_t nq = b.nq;
+    if (out_capacity < 0 || (out_capacity > 0 && !col_out)) return set_error(TCR_ERR_INVALID, "bad output buffer");
+    if (nq <= 0) return TCR_OK;
+    WalkArgs a = make_walk(b, S, W);
+    a.offsets = offsets;
+    a.row_out = row_out;
+    a.col_out = col_out;
+    a.out_cap = out_capacity;
+    if (stage) {
+        const int nsm = num_sms();
+        const unsigned blocks = (unsigned)std::max<int64_t>(
+            1, std::min<int64_t>((int64_t)nsm * 16, (nq / 16 + kExpandWarps) / kExpandWarps));
+        ExpandArgs e;
+        e.stage = stage;
+        e.rec = W.rec;
+        e.num_units = W.num_units;
+        e.unit_t0 = W.unit_t0;
+        e.unit_group = W.unit_group;
+        e.group_start = a.group_start;
+        e.group_cloud = a.group_cloud;
+        e.qsidx = a.qsidx;
+        e.offsets = offsets;
+        e.query_ids = b.query_ids;
+        e.table = W.table;
+        e.num_clouds = b.C;
+        e.local_index = b.local_index;
+        e.row_out = row_out;
+        e.col_out = col_out;
+        e.out_cap = out_capacity;
+        TCR_CUDA(cudaFuncSetAttribute(expand_records_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      (int)sizeof(ExpandSmem)));
+        expand_records_kernel<<<blocks, kExpandWarps * 32, sizeof(ExpandSmem), st>>>(e);
+        note_launches(1);
+    }
+    TCR_CUDA(cudaMemsetAsync(W.work + 1, 0, sizeof(int32_t), st));
+    TCR_CUDA(dispatch_walk<EmitLaunch>(a, b.walk_class, b.mode, dim3(walk_blocks(nq)), dim3(kWalkWarps * 32), 0, st));
+    note_launches(1);
+    stray_kernel<true><<<grid_for(nq, 128, num_sms() * 4), 128, 0, st>>>(a);
+    note_launches(1);
+    return TCR_OK;
+}
+
+static int run_build(const HostBatch& b, void* structure, int64_t structure_bytes, void* scratch,
+                     int64_t scratch_bytes, void* stream) {
+    int64_t need_s = 0, need_w = 0;
+    batch_sizes(b, &need_s, &need_w);
+    if (!structure || !scratch || structure_bytes < need_s || scratch_bytes < need_w)
+        return set_error(TCR_ERR_INVALID, "workspace too small (structure %lld/%lld, scratch %lld/%lld)",
+                         (long long)structure_bytes, (long long)need_s, (long long)scratch_bytes, (long long)need_w);
+    const Structure S = carve_structure(structure, b.nr, b.C, b.map_total, nullptr);
+    const Scratch W = carve_scratch(scratch, b.nq, b.nr, b.C, nullptr);
+    cudaStream_t st = (cudaStream_t)stream;
+    return b.wide ? build_impl<unsigned long long>(b, S, W, st) : build_impl<uint32_t>(b, S, W, st);
+}
+
+static int run_count(const HostBatch& b, const void* structure, void* scratch, int64_t scratch_bytes, int32_t* stage,
+                     int64_t stage_capacity, int64_t* offsets, int32_t* indptr_out, int64_t* row_entries_out,
+                     int64_t* info_out, void* stream) {
+    int64_t need_w = 0;
+    batch_sizes(b, nullptr, &need_w);
+    if (!structure || !scratch || scratch_bytes < need_w || !offsets)
+        return set_error(TCR_ERR_INVALID, "workspace too small or offsets missing");
+    if (stage_capacity < 0 || stage_capacity > 0x7fffffffLL || (stage_capacity > 0 && !stage))
+        return set_error(TCR_ERR_INVALID, "stage capacity must be in [0, 2^31) with a buffer");
+    const Structure S = carve_structure(const_cast<void*>(structure), b.nr, b.C, b.map_total, nullptr);
+    const Scratch W = carve_scratch(scratch, b.nq, b.nr, b.C, nullptr);
+    cudaStream_t st = (cudaStream_t)stream;
+    return b.wide ? count_impl<unsigned long long>(b, S, W, stage, stage_capacity, offsets, indptr_out,
+                                                   row_entries_out, info_out, st)
+                  : count_impl<uint32_t>(b, S, W, stage, stage_capacity, offsets, indptr_out, row_entries_out,
+                                         info_out, st);
+}
+
+static int run_emit(const HostBatch& b, const void* structure, void* scratch, int64_t scratch_bytes,
+                    const int32_t* stage, const int64_t* offsets, int64_t* row_out, int64_t* col_out,
+                    int64_t out_capacity, void* stream) {
+    int64_t need_w = 0;
+    batch_sizes(b, nullptr, &need_w);
+    if (!structure || !scratch || scratch_bytes < need_w || !offsets)
+        return set_error(TCR_ERR_INVALID, "workspace too small or offsets missing");
+    const Structure S = carve_structure(const_cast<void*>(structure), b.nr, b.C, b.map_total, nullptr);
+    const Scratch W = carve_scratch(scratch, b.nq, b.nr, b.C, nullptr);
+    return emit_impl(b, S, W, stage, offsets, row_out, col_out, out_capacity, (cudaStream_t)stream);
+}
+
 }  // namespace tcr
 
 using namespace tcr;
@@ -1357,19 +2048,23 @@ int tcr_version(void) { return TCR_ABI_VERSION; }
 
 int64_t tcr_desc_bytes(void) { return (int64_t)sizeof(tcr_search_desc); }
 
+int64_t tcr_cloud_desc_bytes(void) { return (int64_t)sizeof(tcr_cloud_desc); }
+
+int64_t tcr_batch_desc_bytes(void) { return (int64_t)sizeof(tcr_batch_desc); }
+
 int64_t tcr_kernel_launches(void) { return (int64_t)__atomic_load_n(&g_launches, __ATOMIC_RELAXED); }
 
 int tcr_search_sizes(int64_t n_query, int64_t n_ref, int32_t dim, int64_t* structure_bytes, int64_t* scratch_bytes) {
     if (dim < 1 || dim > 3 || n_query < 0 || n_ref < 0) return set_error(TCR_ERR_INVALID, "invalid sizes");
-    if (structure_bytes) carve_structure(nullptr, n_ref, structure_bytes);
-    if (scratch_bytes) carve_scratch(nullptr, n_query, n_ref, scratch_bytes);
+    if (structure_bytes) carve_structure(nullptr, n_ref, 1, hash_capacity(n_ref, kSingleMapMin), structure_bytes);
+    if (scratch_bytes) carve_scratch(nullptr, n_query, n_ref, 1, scratch_bytes);
     return TCR_OK;
 }
 
 int tcr_structure_offsets(int64_t n_ref, int64_t* offsets, int32_t n) {
     if (n_ref < 0 || !offsets || n < TCR_STRUCT_NFIELDS) return set_error(TCR_ERR_INVALID, "invalid arguments");
     char* const base = reinterpret_cast<char*>(256);  // any non-null base; offsets are relative
-    Structure s = carve_structure(base, n_ref, nullptr);
+    const Structure s = carve_structure(base, n_ref, 1, hash_capacity(n_ref, kSingleMapMin), nullptr);
     auto off = [&](const void* p) { return (int64_t)((const char*)p - base); };
     offsets[TCR_STRUCT_GRID] = off(s.grid);
     offsets[TCR_STRUCT_NUM_CELLS] = off(s.num_cells);
@@ -1380,196 +2075,70 @@ int tcr_structure_offsets(int64_t n_ref, int64_t* offsets, int32_t n) {
     offsets[TCR_STRUCT_CELL_COORDS] = off(s.cell_coords);
     offsets[TCR_STRUCT_CELL_BUCKET] = off(s.cell_bucket);
     offsets[TCR_STRUCT_MAP] = off(s.map);
-    offsets[TCR_STRUCT_MAP_CAPACITY] = s.map_cap;
+    offsets[TCR_STRUCT_MAP_CAPACITY] = s.map_total;
     return TCR_OK;
 }
 
 int tcr_build_structure(const tcr_search_desc* d, void* structure, int64_t structure_bytes, void* scratch,
                         int64_t scratch_bytes, void* stream) {
-    int rc = validate(d);
+    HostBatch b;
+    int rc = batch_of_desc(d, 2, b);
     if (rc) return rc;
-    int64_t need_s = 0, need_w = 0;
-    carve_structure(nullptr, d->n_ref, &need_s);
-    carve_scratch(nullptr, d->n_query, d->n_ref, &need_w);
-    if (!structure || !scratch || structure_bytes < need_s || scratch_bytes < need_w)
-        return set_error(TCR_ERR_INVALID, "workspace too small (structure %lld/%lld, scratch %lld/%lld)",
-                         (long long)structure_bytes, (long long)need_s, (long long)scratch_bytes, (long long)need_w);
-    cudaStream_t st = (cudaStream_t)stream;
-    const SearchParams sp = make_params(d);
-    Structure S = carve_structure(structure, d->n_ref, nullptr);
-    Scratch W = carve_scratch(scratch, d->n_query, d->n_ref, nullptr);
-    const int64_t nr = d->n_ref, nq = d->n_query;
-    grid_init_kernel<<<1, 1, 0, st>>>(S.grid, W.sort.state);
-    note_launches(1);
-    // computeGridSupport: which supports set hMax depends on the mode
-    if (d->ref_sup && nr > 0) {
-        support_stats_kernel<<<grid_for(nr, 256, num_sms() * 8), 256, 0, st>>>(d->ref_sup, nr, &S.grid->ref_stats);
-        note_launches(1);
-    }
-    if (d->query_sup && nq > 0) {
-        support_stats_kernel<<<grid_for(nq, 256, num_sms() * 8), 256, 0, st>>>(d->query_sup, nq,
-                                                                                &S.grid->build_query_stats);
-        note_launches(1);
-    }
-    grid_params_kernel<<<1, 1, 0, st>>>(sp, S.grid, W.sort.state);
-    note_launches(1);
-    TCR_CUDA(cudaMemsetAsync(S.map, 0xff, sizeof(unsigned long long) * S.map_cap, st));
-    TCR_CUDA(cudaMemsetAsync(S.num_cells, 0, sizeof(int32_t), st));
-    if (nr > 0) {
-        pack_points_kernel<<<grid_for(nr, 256), 256, 0, st>>>(sp, S.grid, d->ref_pos, d->ref_sup, nr, 2, W.pack,
-                                                              W.sort.keys[0], W.sort.vals[0], W.sort.state, 1);
-        note_launches(1);
-        TCR_CUDA(radix_sort_pairs(W.sort, nr, st));
-        gather_sorted_kernel<<<grid_for(nr, 256), 256, 0, st>>>(S.grid, W.pack, W.sort.vals[0], W.sort.vals[1], W.sort.state,
-                                                                nr, S.rsorted, S.rsidx);
-        note_launches(1);
-        CellOut co{sp, S.grid, W.sort.keys[0], W.sort.keys[1], W.sort.state, S.rsorted, S.cell_start, S.cell_lin,
-                   S.cell_coords, S.cell_bucket, S.map, S.map_cap};
-        RunFlagIn fi{S.grid, W.sort.keys[0], W.sort.keys[1], W.sort.state};
-        TCR_CUDA(device_exclusive_scan<int32_t>(fi, co, nr, W.scan_tiles32, S.num_cells, st));
-    }
-    finish_cells_kernel<<<1, 1, 0, st>>>(S.cell_start, S.num_cells, nr);
-    note_launches(1);
-    TCR_CUDA(cudaGetLastError());
-    return TCR_OK;
+    return run_build(b, structure, structure_bytes, scratch, scratch_bytes, stream);
 }
 
 int tcr_count(const tcr_search_desc* d, const void* structure, void* scratch, int64_t scratch_bytes, int32_t* stage,
               int64_t stage_capacity, int64_t* offsets, int32_t* indptr_out, int64_t* row_entries_out, int64_t* info_out,
               void* stream) {
-    int rc = validate(d, false);
+    HostBatch b;
+    int rc = batch_of_desc(d, 1, b);
     if (rc) return rc;
-    int64_t need_w = 0;
-    carve_scratch(nullptr, d->n_query, d->n_ref, &need_w);
-    if (!structure || !scratch || scratch_bytes < need_w || !offsets)
-        return set_error(TCR_ERR_INVALID, "workspace too small or offsets missing");
-    if (stage_capacity < 0 || stage_capacity > 0x7fffffffLL || (stage_capacity > 0 && !stage))
-        return set_error(TCR_ERR_INVALID, "stage capacity must be in [0, 2^31) with a buffer");
-    cudaStream_t st = (cudaStream_t)stream;
-    const SearchParams sp = make_params(d);
-    Structure S = carve_structure(const_cast<void*>(structure), d->n_ref, nullptr);
-    Scratch W = carve_scratch(scratch, d->n_query, d->n_ref, nullptr);
-    const int64_t nq = d->n_query;
-    const bool self = d->self_search != 0;
-    TCR_CUDA(cudaMemsetAsync(W.work, 0, sizeof(int32_t) * 4, st));
-    TCR_CUDA(cudaMemsetAsync(W.num_stray, 0, sizeof(int32_t), st));
-    TCR_CUDA(cudaMemsetAsync(W.num_units, 0, sizeof(int32_t), st));
-    TCR_CUDA(cudaMemsetAsync(W.num_flagged, 0, sizeof(int32_t), st));
-    TCR_CUDA(cudaMemsetAsync(W.cursor, 0, sizeof(unsigned long long), st));
-    TCR_CUDA(cudaMemsetAsync(&W.qparams->stats, 0, sizeof(SupportStats), st));
-    if (d->query_sup && nq > 0) {
-        support_stats_kernel<<<grid_for(nq, 256, num_sms() * 8), 256, 0, st>>>(d->query_sup, nq, &W.qparams->stats);
-        note_launches(1);
-    }
-    query_params_kernel<<<1, 1, 0, st>>>(S.grid, d->mode, d->query_sup != nullptr, W.qparams);
-    note_launches(1);
-    if (nq > 0) {
-        TCR_CUDA(cudaMemsetAsync(W.counts, 0, sizeof(int32_t) * nq, st));
-        TCR_CUDA(cudaMemsetAsync(W.rec, 0xff, sizeof(int32_t) * nq, st));
-        const int32_t* gstart;
-        const int32_t* ngroups;
-        if (self) {
-            if (!same_sorted_points(d)) {
-                pack_self_queries_kernel<<<grid_for(nq, 256), 256, 0, st>>>(sp, S.grid, d->query_pos, d->query_sup,
-                                                                            S.rsidx, nq, W.qsorted, W.qsidx);
-                note_launches(1);
-            }
-            gstart = S.cell_start;
-            ngroups = S.num_cells;
-        } else {
-            // sort the queries by their own cells
-            sort_state_init_kernel<<<1, 1, 0, st>>>(W.sort.state);
-            note_launches(1);
-            pack_points_kernel<<<grid_for(nq, 256), 256, 0, st>>>(sp, S.grid, d->query_pos, d->query_sup, nq, 1,
-                                                                  W.pack, W.sort.keys[0], W.sort.vals[0],
-                                                                  W.sort.state, 0);
-            note_launches(1);
-            TCR_CUDA(radix_sort_pairs(W.sort, nq, st));
-            gather_sorted_kernel<<<grid_for(nq, 256), 256, 0, st>>>(S.grid, W.pack, W.sort.vals[0], W.sort.vals[1],
-                                                                    W.sort.state, nq, W.qsorted, W.qsidx);
-            note_launches(1);
-            QueryGroupOut qo{sp, S.grid, W.qsorted, W.qgroup_start, W.qgroup_coords};
-            RunFlagIn fi{S.grid, W.sort.keys[0], W.sort.keys[1], W.sort.state};
-            TCR_CUDA(device_exclusive_scan<int32_t>(fi, qo, nq, W.scan_tiles32, W.num_qgroups, st));
-            finish_cells_kernel<<<1, 1, 0, st>>>(W.qgroup_start, W.num_qgroups, nq);
-            note_launches(1);
-            gstart = W.qgroup_start;
-            ngroups = W.num_qgroups;
-        }
-        BoundedUnitCountIn ui{gstart, ngroups};
-        BoundedUnitOut uo{gstart, ngroups, W.unit_group, W.unit_t0, W.query_unit};
-        TCR_CUDA(device_exclusive_scan<int32_t>(ui, uo, nq, W.scan_tiles32, W.num_units, st));
-        WalkArgs a = make_walk(sp, S, W, self);
-        if (same_sorted_points(d)) {  // the sorted queries are the sorted references
-            a.qsorted = S.rsorted;
-            a.qsidx = S.rsidx;
-        }
-        a.query_ids = d->query_ids;
-        a.ref_ids = d->ref_ids;
-        a.stage = stage;
-        a.stage_cap = stage_capacity;
-        // identical positions: every query sits in its group's cell
-        a.no_stray_check = self && d->periodic_mask == 0 && d->query_pos == d->ref_pos;
-        TCR_CUDA(dispatch_walk<CountLaunch>(a, d->dim, d->periodic_mask != 0, d->mode, dim3(walk_blocks(nq)),
-                                            dim3(kWalkWarps * 32), sizeof(WalkSmem), st));
-        note_launches(1);
-        stray_kernel<false><<<grid_for(nq, 128, num_sms() * 4), 128, 0, st>>>(a);
-        note_launches(1);
-    }
-    CountIn ci{W.counts, nq};
-    OffsetOut oo{nq, offsets, indptr_out, row_entries_out};
-    TCR_CUDA(device_exclusive_scan<int64_t>(ci, oo, nq + 1, W.scan_tiles64, W.total, st));
-    info_kernel<<<1, 1, 0, st>>>(S.grid, W.total, W.num_stray, W.qparams, W.cursor, W.num_flagged, W.info);
-    note_launches(1);
-    if (info_out) TCR_CUDA(cudaMemcpyAsync(info_out, W.info, 8 * sizeof(int64_t), cudaMemcpyDeviceToHost, st));
-    return TCR_OK;
+    return run_count(b, structure, scratch, scratch_bytes, stage, stage_capacity, offsets, indptr_out, row_entries_out,
+                     info_out, stream);
 }
 
 int tcr_emit(const tcr_search_desc* d, const void* structure, void* scratch, int64_t scratch_bytes,
              const int32_t* stage, const int64_t* offsets, int64_t* row_out, int64_t* col_out, int64_t out_capacity,
              void* stream) {
-    int rc = validate(d, false);
+    HostBatch b;
+    int rc = batch_of_desc(d, 1, b);
     if (rc) return rc;
-    int64_t need_w = 0;
-    carve_scratch(nullptr, d->n_query, d->n_ref, &need_w);
-    if (!structure || !scratch || scratch_bytes < need_w || !offsets)
-        return set_error(TCR_ERR_INVALID, "workspace too small or offsets missing");
-    cudaStream_t st = (cudaStream_t)stream;
-    const SearchParams sp = make_params(d);
-    Structure S = carve_structure(const_cast<void*>(structure), d->n_ref, nullptr);
-    Scratch W = carve_scratch(scratch, d->n_query, d->n_ref, nullptr);
-    const int64_t nq = d->n_query;
-    if (nq <= 0) return TCR_OK;
-    WalkArgs a = make_walk(sp, S, W, d->self_search != 0);
-    if (same_sorted_points(d)) {
-        a.qsorted = S.rsorted;
-        a.qsidx = S.rsidx;
-    }
-    a.query_ids = d->query_ids;
-    a.ref_ids = d->ref_ids;
-    a.offsets = offsets;
-    a.row_out = row_out;
-    a.col_out = col_out;
-    a.out_cap = out_capacity;
-    if (out_capacity < 0 || (out_capacity > 0 && !col_out)) return set_error(TCR_ERR_INVALID, "bad output buffer");
-    if (stage) {
-        const int nsm = num_sms();
-        const unsigned blocks = (unsigned)std::max<int64_t>(1, std::min<int64_t>((int64_t)nsm * 16, (nq / 16 + kExpandWarps) / kExpandWarps));
-        const int32_t* group_start = d->self_search ? S.cell_start : W.qgroup_start;
-        TCR_CUDA(cudaFuncSetAttribute(expand_records_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                      (int)sizeof(ExpandSmem)));
-        expand_records_kernel<<<blocks, kExpandWarps * 32, sizeof(ExpandSmem), st>>>(
-            stage, W.rec, W.num_units, W.unit_t0, W.unit_group, group_start, a.qsidx, offsets, d->query_ids, row_out,
-            col_out, out_capacity);
-        note_launches(1);
-    }
-    TCR_CUDA(cudaMemsetAsync(W.work + 1, 0, sizeof(int32_t), st));
-    TCR_CUDA(dispatch_walk<EmitLaunch>(a, d->dim, d->periodic_mask != 0, d->mode, dim3(walk_blocks(nq)),
-                                       dim3(kWalkWarps * 32), 0, st));
-    note_launches(1);
-    stray_kernel<true><<<grid_for(nq, 128, num_sms() * 4), 128, 0, st>>>(a);
-    note_launches(1);
+    return run_emit(b, structure, scratch, scratch_bytes, stage, offsets, row_out, col_out, out_capacity, stream);
+}
+
+int tcr_batch_sizes(const tcr_batch_desc* bd, int64_t* structure_bytes, int64_t* scratch_bytes) {
+    HostBatch b;
+    int rc = batch_of(bd, 0, b);
+    if (rc) return rc;
+    batch_sizes(b, structure_bytes, scratch_bytes);
     return TCR_OK;
+}
+
+int tcr_batch_build_structure(const tcr_batch_desc* bd, void* structure, int64_t structure_bytes, void* scratch,
+                              int64_t scratch_bytes, void* stream) {
+    HostBatch b;
+    int rc = batch_of(bd, 2, b);
+    if (rc) return rc;
+    return run_build(b, structure, structure_bytes, scratch, scratch_bytes, stream);
+}
+
+int tcr_batch_count(const tcr_batch_desc* bd, const void* structure, void* scratch, int64_t scratch_bytes,
+                    int32_t* stage, int64_t stage_capacity, int64_t* offsets, int32_t* indptr_out,
+                    int64_t* row_entries_out, int64_t* info_out, void* stream) {
+    HostBatch b;
+    int rc = batch_of(bd, 1, b);
+    if (rc) return rc;
+    return run_count(b, structure, scratch, scratch_bytes, stage, stage_capacity, offsets, indptr_out, row_entries_out,
+                     info_out, stream);
+}
+
+int tcr_batch_emit(const tcr_batch_desc* bd, const void* structure, void* scratch, int64_t scratch_bytes,
+                   const int32_t* stage, const int64_t* offsets, int64_t* row_out, int64_t* col_out,
+                   int64_t out_capacity, void* stream) {
+    HostBatch b;
+    int rc = batch_of(bd, 1, b);
+    if (rc) return rc;
+    return run_emit(b, structure, scratch, scratch_bytes, stage, offsets, row_out, col_out, out_capacity, stream);
 }
 
 }  // extern "C"
@@ -1619,13 +2188,13 @@ extern "C" int tcr_search_noalloc(const tcr_search_desc* d, int64_t* offsets, in
                                   int64_t* row_entries_out, int64_t* row_out, int64_t* col_out,
                                   int64_t pair_capacity, int64_t* total_out, void* stream) {
     using namespace tcr;
-    int rc = validate(d);
+    HostBatch b;
+    int rc = batch_of_desc(d, 2, b);
     if (rc) return rc;
     if (!offsets || (pair_capacity > 0 && !col_out) || pair_capacity < 0)
         return set_error(TCR_ERR_INVALID, "offsets and a column buffer of pair_capacity entries are required");
     int64_t s_bytes = 0, w_bytes = 0;
-    carve_structure(nullptr, d->n_ref, &s_bytes);
-    carve_scratch(nullptr, d->n_query, d->n_ref, &w_bytes);
+    batch_sizes(b, &s_bytes, &w_bytes);
     if (s_bytes + w_bytes > kTcrStaticScratchBytes)
         return set_error(TCR_ERR_INVALID,
                          "tcr_search_noalloc: %lld query and %lld reference points need %lld bytes of scratch, "
