@@ -41,6 +41,7 @@ def parse():
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-batched", action="store_true", help="skip the batched-form measurement")
     return ap.parse_args()
 
 
@@ -53,6 +54,30 @@ def make_workload():
     h0 = (3 * 50 * dx ** 3 / (4 * np.pi)) ** (1 / 3)
     sup = h0 * (0.9 + 0.2 * torch.rand(N_POINTS))
     return pos.contiguous(), sup.to(torch.float32).contiguous()
+
+
+def make_batched_workload(seed=4, n_clouds=256):
+    """256 independent clouds: sizes log-uniform in [1e3, 2e5], half 2D and half 3D, uniform in
+    [-1, 1]^d, per-dimension periodicity Bernoulli(0.5), one support per cloud for about 32 (2D)
+    or 50 (3D) neighbours at the cloud's spacing dx = 2 / n^(1/d).  Returns per-cloud host
+    tensors (positions, supports) and descriptors."""
+    import numpy as np
+    import torch
+    rng = np.random.default_rng(seed)
+    sizes = np.exp(rng.uniform(np.log(1e3), np.log(2e5), n_clouds)).astype(np.int64)
+    dims = np.array([2] * (n_clouds // 2) + [3] * (n_clouds - n_clouds // 2))
+    rng.shuffle(dims)
+    per = rng.random((n_clouds, 3)) < 0.5
+    gen = torch.Generator().manual_seed(seed)
+    clouds = []
+    for k in range(n_clouds):
+        n, d = int(sizes[k]), int(dims[k])
+        dx = 2.0 / n ** (1.0 / d)
+        h = (32 * dx * dx / np.pi) ** 0.5 if d == 2 else (3 * 50 * dx ** 3 / (4 * np.pi)) ** (1 / 3)
+        x = (torch.rand(n, d, generator=gen) * 2 - 1).contiguous()
+        hx = torch.full((n,), float(h), dtype=torch.float32)
+        clouds.append(dict(x=x, h=hx, dim=d, periodic=[bool(v) for v in per[k, :d]]))
+    return clouds
 
 
 def config(pairs):
@@ -219,6 +244,138 @@ def run_reference(args):
     return 0
 
 
+def bench_batched(dev, stream, flush, steps, warmup, with_cpu):
+    """The batched form on the 256-cloud workload: one batched search per step (device-timed, L2
+    flushed between steps) against the per-call loop of radiusSearch over the same clouds on the
+    same GPU, plus the end-to-end batched call from pinned host memory."""
+    import numpy as np
+    import torch
+
+    import torchcompactradius_b200 as tcr
+    from torchcompactradius_b200 import batched
+
+    clouds = make_batched_workload()
+    C = len(clouds)
+    parts = {2: [c for c in clouds if c["dim"] == 2], 3: [c for c in clouds if c["dim"] == 3]}
+    host = {d: (torch.cat([c["x"] for c in parts[d]]).pin_memory(), torch.cat([c["h"] for c in parts[d]]).pin_memory())
+            for d in (2, 3)}
+    devx = {d: (host[d][0].to(dev), host[d][1].to(dev)) for d in (2, 3)}
+    table = batched.cloud_table(C)
+    off = {2: 0, 3: 0}
+    views = []
+    for k, c in enumerate(clouds):
+        d, n = c["dim"], c["x"].shape[0]
+        x, h = devx[d][0][off[d]:off[d] + n], devx[d][1][off[d]:off[d] + n]
+        off[d] += n
+        views.append((x, h))
+        table["dim"][k] = d
+        table["periodic_mask"][k] = sum(1 << i for i, p in enumerate(c["periodic"]) if p)
+        table["domain_min"][k, :d] = -1.0
+        table["domain_max"][k, :d] = 1.0
+        table["n_query"][k] = table["n_ref"][k] = n
+        table["query_pos"][k] = table["ref_pos"][k] = x.data_ptr()
+        table["query_sup"][k] = table["ref_sup"][k] = h.data_ptr()
+    n_points = int(table["n_query"].sum())
+    bufs = batched.BatchBuffers(dev)
+
+    def step():
+        return batched.run_batch(table, "gather", True, "csr", dev, buffers=bufs, stream=stream)
+
+    for _ in range(warmup):
+        out = step()
+    pairs = out["total"]
+    ms = []
+    for k in range(steps):
+        flush.fill_(k & 0xff)
+        s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        s.record(stream)
+        step()
+        e.record(stream)
+        e.synchronize()
+        ms.append(s.elapsed_time(e))
+    batched_value = pairs * len(ms) / (sum(ms) / 1e3)
+
+    # per-call loop: one radiusSearch per cloud through the public API, inputs already on the GPU
+    doms = [tcr.DomainDescription(torch.full((c["dim"],), -1.0), torch.full((c["dim"],), 1.0),
+                                  torch.tensor(c["periodic"]), c["dim"]) for c in clouds]
+
+    def per_call():
+        tot = 0
+        for (x, h), dom in zip(views, doms):
+            adj = tcr.radiusSearch(tcr.PointCloud(x, h), mode="gather", domain=dom, hashMapLength=4096,
+                                   algorithm="compact", format="csr")
+            tot += adj.indices.numel()
+        return tot
+
+    per_call()
+    pc_ms = []
+    for k in range(max(2, min(steps, 4))):
+        flush.fill_(k & 0xff)
+        s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        s.record(stream)
+        tot = per_call()
+        e.record(stream)
+        e.synchronize()
+        pc_ms.append(s.elapsed_time(e))
+    per_call_value = tot * len(pc_ms) / (sum(pc_ms) / 1e3)
+
+    # end to end: inputs from pinned host memory, batched search, CSR back to pinned host memory
+    out_idx = torch.empty(pairs, dtype=torch.int64, pin_memory=True)
+    out_ptr = torch.empty(n_points + 1, dtype=torch.int32, pin_memory=True)
+    e2e_ms = []
+    for k in range(max(3, min(steps, 10))):
+        flush.fill_(k & 0xff)
+        s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        s.record(stream)
+        for d in (2, 3):
+            devx[d][0].copy_(host[d][0], non_blocking=True)
+            devx[d][1].copy_(host[d][1], non_blocking=True)
+        o = step()
+        out_idx.copy_(o["col"], non_blocking=True)
+        out_ptr.copy_(o["indptr"], non_blocking=True)
+        e.record(stream)
+        e.synchronize()
+        e2e_ms.append(s.elapsed_time(e))
+    h2d = sum(host[d][0].numel() * 4 + host[d][1].numel() * 4 for d in (2, 3))
+    res = {"workload": "256 clouds, sizes log-uniform [1e3, 2e5] (seed 4), 128 2D + 128 3D, uniform in [-1,1]^d, "
+                       "per-dim periodicity Bernoulli(0.5), 32 (2D) / 50 (3D) neighbours, gather, CSR",
+           "clouds": C, "points": n_points, "pairs_per_step": pairs,
+           "value": batched_value, "unit": "pairs/s", "ms_per_step": statistics.mean(ms),
+           "p50_ms": statistics.median(ms), "p99_ms": sorted(ms)[min(len(ms) - 1, int(0.99 * len(ms)))],
+           "per_call": {"value": per_call_value, "unit": "pairs/s", "ms_per_batch": statistics.mean(pc_ms),
+                        "pairs_match": tot == pairs, "what": "loop of radiusSearch(algorithm='compact') per cloud"},
+           "speedup_vs_per_call": batched_value / per_call_value,
+           "e2e": {"value": pairs * len(e2e_ms) / (sum(e2e_ms) / 1e3), "unit": "pairs/s",
+                   "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": 8 * pairs + 4 * (n_points + 1),
+                   "ms_per_step": statistics.mean(e2e_ms)}}
+    if with_cpu:
+        res["cpu_baseline"] = cpu_baseline_batched(clouds)
+    return res
+
+
+def cpu_baseline_batched(clouds, budget_s=12.0):
+    """The reference's own CPU search, one call per cloud (its batched radius() fails), over the
+    first clouds of the workload until about budget_s seconds have passed."""
+    import torch
+    from oracle import ref_pipeline
+    if not ref_pipeline.available():
+        return None
+    torch.set_num_threads(os.cpu_count() or 1)
+    pairs, t, k = 0, 0.0, 0
+    for c in clouds:
+        d = c["dim"]
+        s = time.perf_counter()
+        o = ref_pipeline.radius_search(c["x"], c["h"], None, None, [-1.0] * d, [1.0] * d, c["periodic"], "gather",
+                                       4096, "csr")
+        t += time.perf_counter() - s
+        pairs += int(o[0].numel())
+        k += 1
+        if t > budget_s:
+            break
+    return {"value": pairs / t, "unit": "pairs/s", "cores": torch.get_num_threads(), "kind": "reference",
+            "sample": f"the first {k} of {len(clouds)} clouds, one reference call per cloud ({pairs} pairs)"}
+
+
 def run_b200(args):
     import torch
     import torch.distributed as dist
@@ -270,8 +427,9 @@ def run_b200(args):
     clk.start()
     barrier()
     torch.cuda.synchronize()
+    _lib.check(lib.tcr_profile_kernels(1), "tcr_profile_kernels")
     launches0 = lib.tcr_kernel_launches()
-    step_ms, emit_ms, count_ms, build_ms = [], [], [], []
+    step_ms, emit_ms, count_ms, build_ms, walk_ms, expand_ms = [], [], [], [], [], []
     for k in range(args.steps):
         flush.fill_(k & 0xff)  # L2 flush outside the step's events
         ev = {}
@@ -284,9 +442,12 @@ def run_b200(args):
         build_ms.append(ev["build"][0].elapsed_time(ev["build"][1]))
         count_ms.append(ev["count"][0].elapsed_time(ev["count"][1]))
         emit_ms.append(ev["emit"][0].elapsed_time(ev["emit"][1]))
+        walk_ms.append(_lib.profile_kernel_ms(_lib.PROFILE_COUNT_WALK))
+        expand_ms.append(_lib.profile_kernel_ms(_lib.PROFILE_EXPAND))
     torch.cuda.synchronize()
     barrier()
     launches = lib.tcr_kernel_launches() - launches0
+    _lib.check(lib.tcr_profile_kernels(0), "tcr_profile_kernels")
     clocks = clk.stop()
     total_ms = max_over_ranks(sum(step_ms))
     value = pairs * args.steps * world / (total_ms / 1e3)
@@ -317,12 +478,13 @@ def run_b200(args):
     e2e_value = pairs * len(e2e_ms) * world / (e2e_total / 1e3)
     ok = torch.equal(out_ptr, indptr.cpu()) and int(out_ent.sum()) == pairs
 
-    # ---- roofline of the dominant kernel (the emitting walk) ------------------------------
+    # ---- roofline of the dominant kernel (the count walk) and of the whole search ----------
     peak, peak_kind = measured_peak()
-    emit_bytes = 16 * N_POINTS + 8 * pairs  # inputs read once (4d+4 B/pt) + int64 CSR indices
-    emit_s = statistics.mean(emit_ms) / 1e3
-    achieved = emit_bytes / emit_s / 1e9
+    walk_bytes = 16 * N_POINTS + 4 * N_POINTS + 4 * N_POINTS  # sorted float4 points, sort index, counts
+    walk_s = statistics.mean(walk_ms) / 1e3
+    achieved = walk_bytes / walk_s / 1e9
     search_bytes = 16 * N_POINTS + 8 * pairs + 4 * (N_POINTS + 1) + 8 * N_POINTS
+    search_s = statistics.mean(step_ms) / 1e3
     traffic = ncu_traffic()
     line = {
         "metric": METRIC, "value": value, "unit": "pairs/s", "n_gpus": world, "steps": args.steps,
@@ -331,17 +493,25 @@ def run_b200(args):
         "p50_ms": statistics.median(step_ms), "p99_ms": sorted(step_ms)[min(len(step_ms) - 1,
                                                                          int(0.99 * len(step_ms)))],
         "phases_ms": {"build": statistics.mean(build_ms), "count": statistics.mean(count_ms),
-                      "emit": statistics.mean(emit_ms)},
+                      "emit": statistics.mean(emit_ms), "count_walk_kernel": statistics.mean(walk_ms),
+                      "expand_kernel": statistics.mean(expand_ms)},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-                     "traffic": traffic, "kernel": "walk_kernel<3,false,true> + stray_kernel<true> (emit)",
-                     "algorithmic_bytes_per_launch": emit_bytes, "peak_kind": peak_kind,
-                     "search_frac": search_bytes / (statistics.mean(step_ms) / 1e3) / 1e9 / peak},
+                     "traffic": traffic, "kernel": "walk_count_kernel<3,false,symmetric> (every pair test)",
+                     "algorithmic_bytes_per_launch": walk_bytes, "launch_ms": statistics.mean(walk_ms),
+                     "pair_tests_note": "bound by candidate tests, not HBM: see candidate_tests_per_s",
+                     "peak_kind": peak_kind},
+        "search_roofline": {"bound": "hbm", "algorithmic_bytes_per_search": search_bytes,
+                            "achieved": search_bytes / search_s / 1e9, "peak": peak, "unit": "GB/s",
+                            "frac": search_bytes / search_s / 1e9 / peak, "peak_kind": peak_kind},
         "e2e": {"value": e2e_value, "unit": "pairs/s", "h2d_bytes_per_step": 16 * N_POINTS,
                 "d2h_bytes_per_step": 8 * pairs + 4 * (N_POINTS + 1) + 8 * N_POINTS,
                 "ms_per_step": e2e_total / len(e2e_ms), "output_checked": bool(ok)},
         "gpu_launches": int(launches),
         "clocks": clocks,
     }
+    if world == 1 and not args.no_batched:
+        line["batched"] = bench_batched(dev, stream, flush, max(3, min(args.steps, 10)), 3,
+                                        rank == 0 and not args.no_cpu_baseline)
     if world > 1:
         dist.destroy_process_group()
     if rank == 0 and world == 1 and not args.no_cpu_baseline:

@@ -112,6 +112,16 @@ int64_t tcr_batch_desc_bytes(void);
  * for benchmarks; no reference counterpart). */
 int64_t tcr_kernel_launches(void);
 
+/* Per-launch timing of the heaviest kernels, for benchmarks (no reference counterpart).  While
+ * enabled, tcr_count / tcr_batch_count record a pair of CUDA events around the count walk launch
+ * and tcr_emit / tcr_batch_emit around the record expansion, on the launching stream, for calls
+ * on the device that was current at tcr_profile_kernels(1).  tcr_profile_kernel_ms waits for the
+ * last such launch and returns its duration in milliseconds. */
+#define TCR_PROFILE_COUNT_WALK 0
+#define TCR_PROFILE_EXPAND 1
+int tcr_profile_kernels(int32_t enable);
+int tcr_profile_kernel_ms(int32_t kernel, float* ms);
+
 /* Byte sizes of the persistent structure (reference-side cell table and hash map, kept for
  * reuse like the reference's CompactHashMap, compactHashing/datastructure.py:8-31) and of the
  * per-search scratch.  Host-only; no device work. */
@@ -163,7 +173,8 @@ int tcr_build_structure(const tcr_search_desc* d, void* structure, int64_t struc
  * indptr_out (device int32 [n_query+1]) and row_entries_out (device int64 [n_query]) are the
  * SparseCSR fields of util.py:321-358 and may be NULL.  info_out (host, 8 x int64, may be NULL)
  * receives, asynchronously on `stream`: {total pairs, grid error flag, queries walked serially,
- * exact-only mode, staging words the units asked for, units left for tcr_emit to re-test, 0, 0};
+ * exact-only mode, staging words the units asked for, units left for tcr_emit to re-test, units
+ * re-tested with exact decisions because a pair lay within the fast test's rounding band, 0};
  * a caller sizes the next search's staging list from entry 4. */
 int tcr_count(const tcr_search_desc* d, const void* structure, void* scratch, int64_t scratch_bytes, int32_t* stage,
               int64_t stage_capacity, int64_t* offsets, int32_t* indptr_out, int64_t* row_entries_out,

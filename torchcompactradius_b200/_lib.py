@@ -82,6 +82,8 @@ SIGNATURES = {
     "tcr_cloud_desc_bytes": (_i64, []),
     "tcr_batch_desc_bytes": (_i64, []),
     "tcr_kernel_launches": (_i64, []),
+    "tcr_profile_kernels": (ctypes.c_int, [_i32]),
+    "tcr_profile_kernel_ms": (ctypes.c_int, [_i32, ctypes.POINTER(ctypes.c_float)]),
     "tcr_search_sizes": (ctypes.c_int, [_i64, _i64, _i32, ctypes.POINTER(_i64), ctypes.POINTER(_i64)]),
     "tcr_structure_offsets": (ctypes.c_int, [_i64, ctypes.POINTER(_i64), _i32]),
     "tcr_build_structure": (ctypes.c_int, [_desc_p, _vp, _i64, _vp, _i64, _vp]),
@@ -142,3 +144,13 @@ def batch_sizes(bdesc):
     s, w = _i64(0), _i64(0)
     check(load().tcr_batch_sizes(ctypes.byref(bdesc), ctypes.byref(s), ctypes.byref(w)), "tcr_batch_sizes")
     return s.value, w.value
+
+
+PROFILE_COUNT_WALK = 0
+PROFILE_EXPAND = 1
+
+
+def profile_kernel_ms(kernel):
+    ms = ctypes.c_float(0.0)
+    check(load().tcr_profile_kernel_ms(kernel, ctypes.byref(ms)), "tcr_profile_kernel_ms")
+    return float(ms.value)

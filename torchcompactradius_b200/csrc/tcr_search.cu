@@ -63,7 +63,9 @@ static inline int64_t hash_capacity(int64_t n_ref, int64_t min_cap) {
 }
 constexpr int64_t kSingleMapMin = 1024;  // one search
 constexpr int64_t kBatchMapMin = 64;     // per cloud of a batch
-constexpr int kWorkCounters = 4;
+// Work counters: [0] count walk, [1] emit walk, [2 + cls] / [8 + cls] the count / emit walk of
+// one cloud class (cls = dim * 2 + periodic, 2..7) in a batch that mixes classes.
+constexpr int kWorkCounters = 16;
 
 struct Carve {
     char* base;
@@ -126,6 +128,7 @@ struct Scratch {
     int64_t* info;          // [8] see tcr_count
     int32_t* num_flagged;   // [1]
     int32_t* exact_clouds;  // [1] clouds whose every pair takes the exact test
+    int32_t* num_exact;     // [1] units the count walk re-tested with exact decisions
     unsigned long long* cursor;  // [1] staging fill
     float4* pack;           // [max(nq,nr)] packed input points before sorting
     void* keys[2];          // [max(nq,nr)] 64-bit slots (32-bit keys use the first half)
@@ -164,6 +167,7 @@ static Scratch carve_scratch(void* buf, int64_t nq, int64_t nr, int64_t C, int64
     s.info = c.take<int64_t>(8);
     s.num_flagged = c.take<int32_t>(1);
     s.exact_clouds = c.take<int32_t>(1);
+    s.num_exact = c.take<int32_t>(1);
     s.cursor = c.take<unsigned long long>(1);
     s.pack = c.take<float4>(nmax);
     s.keys[0] = c.take<unsigned long long>(nmax);
@@ -442,6 +446,7 @@ __global__ void count_init_kernel(Scratch W, int C) {
         *W.num_units = 0;
         *W.num_flagged = 0;
         *W.exact_clouds = 0;
+        *W.num_exact = 0;
         *W.cursor = 0ull;
     }
 }
@@ -796,6 +801,8 @@ struct WalkArgs {
     int32_t mode;
     int32_t no_stray_check;       // self search, no periodic dims, same positions: a query's cell is its
                                   // group's unless its cloud has points outside the grid (out_of_grid)
+    int32_t class_filter;         // >= 0: walk only units of clouds of this class (dim * 2 + periodic)
+    int32_t pad0;
     const float4* __restrict__ rsorted;
     const int32_t* __restrict__ rsidx;
     const int32_t* __restrict__ cell_start;
@@ -818,6 +825,7 @@ struct WalkArgs {
     int32_t* rec;                 // [units] offset of each unit's record in the staging list, -1 if not staged
     int32_t* flagged;             // [units] units to re-walk in the emit pass
     int32_t* num_flagged;
+    int32_t* num_exact;           // units re-tested with exact decisions
     unsigned long long* cursor;   // staging list fill
     int32_t* stage;               // staging list
     int64_t stage_cap;
@@ -931,30 +939,47 @@ __device__ __forceinline__ float pair_thr(float hq, float cw) {
     return fmaxf(hq, cw);
 }
 
+// Per-dimension constants of the fast periodic difference: the extent h, the half extent at which
+// a difference wraps (+inf on a non-periodic dimension, which never wraps) and the band around it
+// inside which the wrap decision is left to the exact test.
+struct WrapCtx {
+    float h[3], half[3], epsh[3];
+};
+__device__ __forceinline__ WrapCtx wrap_ctx(int periodic_mask, const float* ext) {
+    WrapCtx w;
+    for (int d = 0; d < 3; ++d) {
+        const bool p = (periodic_mask >> d) & 1;
+        w.h[d] = ext[d];
+        w.half[d] = p ? 0.5f * ext[d] : __int_as_float(0x7f800000);
+        w.epsh[d] = p ? kBandEps * ext[d] : 0.0f;
+    }
+    return w;
+}
+
+// Float difference q - c along dimension d, wrapped once into [-h/2, h/2] on a periodic dimension
+// (the reference's moduloOp decides exactly; a difference within the band of +-h/2 sets wrap_unc).
+template <bool PERIODIC>
+__device__ __forceinline__ float fast_diff(const WrapCtx& wc, int d, float q, float c, bool& wrap_unc) {
+    float diff = q - c;
+    if (PERIODIC) {
+        const float ad = fabsf(diff);
+        wrap_unc |= fabsf(ad - wc.half[d]) <= wc.epsh[d];
+        if (ad >= wc.half[d]) diff -= copysignf(wc.h[d], diff);
+    }
+    return diff;
+}
+
 // One (query, candidate) test.  in: decided; unc: needs the exact reference test.
 template <int DIM, bool PERIODIC, int MODE>
-__device__ __forceinline__ void lean_test(const ExactCtx& sp, const float4& q, const float4& c, float cw, float band,
+__device__ __forceinline__ void lean_test(const WrapCtx& wc, const float4& q, const float4& c, float cw, float band,
                                           bool& in, bool& unc) {
-    float d2;
     bool wrap_unc = false;
-    {
-        float dd[3];
+    float dd[3];
 #pragma unroll
-        for (int d = 0; d < DIM; ++d) {
-            float diff = comp(q, d) - comp(c, d);
-            if (PERIODIC && ((sp.periodic_mask >> d) & 1)) {
-                const float h = sp.ext[d];
-                const float half = 0.5f * h;
-                wrap_unc |= fabsf(fabsf(diff) - half) <= kBandEps * h;
-                if (diff >= half) diff -= h;
-                else if (diff < -half) diff += h;
-            }
-            dd[d] = diff;
-        }
-        d2 = dd[0] * dd[0];
-        if (DIM > 1) d2 = fmaf(dd[1], dd[1], d2);
-        if (DIM > 2) d2 = fmaf(dd[2], dd[2], d2);
-    }
+    for (int d = 0; d < DIM; ++d) dd[d] = fast_diff<PERIODIC>(wc, d, comp(q, d), comp(c, d), wrap_unc);
+    float d2 = dd[0] * dd[0];
+    if (DIM > 1) d2 = fmaf(dd[1], dd[1], d2);
+    if (DIM > 2) d2 = fmaf(dd[2], dd[2], d2);
     const float thr = pair_thr<MODE>(q.w, cw);
     const float r = fmaf(-thr, thr, d2);  // d2 - thr^2, one rounding; sign exact
     in = r < 0.0f;
@@ -962,6 +987,17 @@ __device__ __forceinline__ void lean_test(const ExactCtx& sp, const float4& q, c
 }
 
 constexpr int kWalkWarps = 4;
+// Resident blocks per SM the count walk is compiled for (registers <= 65536 / (128 * blocks)):
+// five (20 warps) measured fastest on non-periodic clouds, four (128 registers, no spills) on
+// periodic ones, whose wrap tests need more registers.
+#ifndef TCR_WALK_MIN_BLOCKS
+#define TCR_WALK_MIN_BLOCKS 5
+#endif
+#ifndef TCR_WALK_MIN_BLOCKS_PERIODIC
+#define TCR_WALK_MIN_BLOCKS_PERIODIC 4
+#endif
+constexpr int kWalkMinBlocks = TCR_WALK_MIN_BLOCKS;
+constexpr int kWalkMinBlocksPeriodic = TCR_WALK_MIN_BLOCKS_PERIODIC;
 constexpr int kSegChunks = 24;  // staged units: at most 24 chunks (768 candidates)
 constexpr int kMaskStride = kSegChunks + 1;  // padded rows: conflict-free per-lane reads
 
@@ -1004,21 +1040,11 @@ __device__ __forceinline__ float query_band(float hq, float rmax) {
 
 // Float test of query q (lane) against candidate c; r < 0 means inside.
 template <int DIM, bool PERIODIC, int MODE>
-__device__ __forceinline__ float lane_residual(const ExactCtx& sp, const float4& q, float qs, const float4& c,
+__device__ __forceinline__ float lane_residual(const WrapCtx& wc, const float4& q, float qs, const float4& c,
                                                bool& wrap_unc) {
     float dd[3];
 #pragma unroll
-    for (int d = 0; d < DIM; ++d) {
-        float diff = comp(q, d) - comp(c, d);
-        if (PERIODIC && ((sp.periodic_mask >> d) & 1)) {
-            const float h = sp.ext[d];
-            const float half = 0.5f * h;
-            wrap_unc |= fabsf(fabsf(diff) - half) <= kBandEps * h;
-            if (diff >= half) diff -= h;
-            else if (diff < -half) diff += h;
-        }
-        dd[d] = diff;
-    }
+    for (int d = 0; d < DIM; ++d) dd[d] = fast_diff<PERIODIC>(wc, d, comp(q, d), comp(c, d), wrap_unc);
     float d2 = dd[0] * dd[0];
     if (DIM > 1) d2 = fmaf(dd[1], dd[1], d2);
     if (DIM > 2) d2 = fmaf(dd[2], dd[2], d2);
@@ -1031,14 +1057,14 @@ __device__ __forceinline__ float lane_residual(const ExactCtx& sp, const float4&
 // Tests the lane's query against the Q candidates of its stream; returns the Q-bit hit mask and
 // ORs into `unc` whether any pair lies in the band (those units are redone with exact decisions).
 template <int DIM, bool PERIODIC, int MODE, int Q>
-__device__ __forceinline__ uint32_t stream_mask(const ExactCtx& sp, const float4* cand, const float4& q, float qs,
+__device__ __forceinline__ uint32_t stream_mask(const WrapCtx& wc, const float4* cand, const float4& q, float qs,
                                                 float band, bool& unc) {
     uint32_t m = 0;
 #pragma unroll
     for (int k = 0; k < Q; ++k) {
         const float4 c = cand[k];
         bool wrap_unc = false;
-        const float r = lane_residual<DIM, PERIODIC, MODE>(sp, q, qs, c, wrap_unc);
+        const float r = lane_residual<DIM, PERIODIC, MODE>(wc, q, qs, c, wrap_unc);
         if (r < 0.0f) m |= 1u << k;
         unc |= (fabsf(r) <= band) || wrap_unc;
     }
@@ -1049,12 +1075,12 @@ __device__ __forceinline__ uint32_t stream_mask(const ExactCtx& sp, const float4
 template <int DIM, bool PERIODIC, int MODE>
 __device__ __noinline__ uint32_t stream_mask_exact(ExactCtx xc, const float4* cand, int n, float4 q, float qs,
                                                    float band) {
-    const ExactCtx& sp = xc;
+    const WrapCtx wc = wrap_ctx(xc.periodic_mask, xc.ext);
     uint32_t m = 0;
     for (int k = 0; k < n; ++k) {
         const float4 c = cand[k];
         bool wrap_unc = false;
-        const float r = lane_residual<DIM, PERIODIC, MODE>(sp, q, qs, c, wrap_unc);
+        const float r = lane_residual<DIM, PERIODIC, MODE>(wc, q, qs, c, wrap_unc);
         bool in = r < 0.0f;
         if ((fabsf(r) <= band) || wrap_unc) in = exact_pair_test(xc, q, q.w, c, c.w);
         if (in) m |= 1u << k;
@@ -1073,7 +1099,7 @@ __device__ __forceinline__ void count_unit(const WalkArgs& a, WalkSmem& sm, int3
                                            int w) {
     constexpr int S = DIM == 1 ? 3 : (DIM == 2 ? 9 : 27);
     const UnitCtx& u = sm.u[w];
-    const ExactCtx xc = unit_exact_ctx(u, MODE);
+    const WrapCtx wc = wrap_ctx(u.periodic_mask, u.ext);
     const float rmax = u.rmax;
     const bool exact_all = u.exact_all != 0;
     const int32_t rshift = u.rshift;
@@ -1155,13 +1181,14 @@ __device__ __forceinline__ void count_unit(const WalkArgs& a, WalkSmem& sm, int3
             __syncwarp();
             uint32_t m;
             if (exact) {
-                m = stream_mask_exact<DIM, PERIODIC, MODE>(xc, my_cand, Q, myq, qs, band) << (Q == 32 ? 0 : Q * ls);
+                m = stream_mask_exact<DIM, PERIODIC, MODE>(unit_exact_ctx(u, MODE), my_cand, Q, myq, qs, band)
+                    << (Q == 32 ? 0 : Q * ls);
             } else if (Q == 32) {
-                m = stream_mask<DIM, PERIODIC, MODE, 32>(xc, my_cand, myq, qs, band, unc);
+                m = stream_mask<DIM, PERIODIC, MODE, 32>(wc, my_cand, myq, qs, band, unc);
             } else if (Q == 16) {
-                m = stream_mask<DIM, PERIODIC, MODE, 16>(xc, my_cand, myq, qs, band, unc) << (16 * ls);
+                m = stream_mask<DIM, PERIODIC, MODE, 16>(wc, my_cand, myq, qs, band, unc) << (16 * ls);
             } else {
-                m = stream_mask<DIM, PERIODIC, MODE, 8>(xc, my_cand, myq, qs, band, unc) << (8 * ls);
+                m = stream_mask<DIM, PERIODIC, MODE, 8>(wc, my_cand, myq, qs, band, unc) << (8 * ls);
             }
             if (Q <= 16) m |= __shfl_xor_sync(0xffffffffu, m, 16);
             if (Q == 8) m |= __shfl_xor_sync(0xffffffffu, m, 8);
@@ -1172,6 +1199,7 @@ __device__ __forceinline__ void count_unit(const WalkArgs& a, WalkSmem& sm, int3
             __syncwarp();
         }
         if (exact || !__any_sync(0xffffffffu, unc)) break;
+        if (lane == 0) atomicAdd(a.num_exact, 1);  // the unit is walked again with exact decisions
     }
     if (active) a.counts[qorig] = qcount;
     bool staged = false;
@@ -1203,41 +1231,57 @@ __device__ __forceinline__ void count_unit(const WalkArgs& a, WalkSmem& sm, int3
     __syncwarp();
 }
 
-// Units come from one counter.  DIM == 0: the clouds differ in dimension or periodicity, and
-// each unit runs the body of its own cloud's class.
+// Class (dim * 2 + any periodic dim) of a cloud, the key of the walk kernels' template.
+__device__ __forceinline__ int cloud_class(const CloudParams& cp) { return cp.dim * 2 + (cp.periodic_mask ? 1 : 0); }
+
+// Next units of a warp.  Without a class filter one unit per atomic; with one (a batch that mixes
+// classes runs one launch per class) a chunk of 32 consecutive units, of which the units of other
+// classes are dropped by one ballot -- units of a cloud are consecutive, so chunks rarely mix.
+__device__ __forceinline__ uint32_t next_units(const WalkArgs& a, int32_t* counter, const int32_t* list,
+                                               int32_t nlist, int lane, int32_t& base) {
+    const bool filter = a.class_filter >= 0;
+    int32_t b = 0;
+    if (lane == 0) b = atomicAdd(counter, filter ? 32 : 1);
+    base = __shfl_sync(0xffffffffu, b, 0);
+    if (base >= nlist) return 0u;
+    if (!filter) return 1u;
+    bool mine = false;
+    if (base + lane < nlist) {
+        const int32_t unit = list ? list[base + lane] : base + lane;
+        const int32_t grp = a.unit_group[unit];
+        mine = cloud_class(a.table[a.group_cloud[grp]]) == a.class_filter;
+    }
+    return __ballot_sync(0xffffffffu, mine);  // bit k: unit base + k belongs to this launch
+}
+
 template <int DIM, bool PERIODIC, int MODE>
-__global__ void __launch_bounds__(kWalkWarps * 32) walk_count_kernel(WalkArgs a) {
+__global__ void __launch_bounds__(kWalkWarps * 32, PERIODIC ? kWalkMinBlocksPeriodic : kWalkMinBlocks)
+    walk_count_kernel(WalkArgs a) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     WalkSmem& sm = *reinterpret_cast<WalkSmem*>(smem_raw);
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
     const int32_t nunits = *a.num_units;
+    int32_t* counter = a.class_filter >= 0 ? &a.work[2 + a.class_filter] : &a.work[0];
     int cur = -1;
     for (;;) {
-        int32_t unit = 0;
-        if (lane == 0) unit = atomicAdd(&a.work[0], 1);
-        unit = __shfl_sync(0xffffffffu, unit, 0);
-        if (unit >= nunits) break;
-        const int32_t grp = a.unit_group[unit];
-        const int cloud = a.num_clouds == 1 ? 0 : a.group_cloud[grp];
-        if (cloud != cur) {
-            if (lane == 0) load_unit_ctx(sm.u[w], a, cloud);
-            cur = cloud;
-            __syncwarp();
-        }
-        if (sm.u[w].error) {  // no grid: nothing found, nothing staged
-            if (lane == 0) a.rec[unit] = -1;
-            continue;
-        }
-        if constexpr (DIM == 0) {
-            switch (sm.u[w].dim * 2 + (sm.u[w].periodic_mask != 0 ? 1 : 0)) {
-                case 2: count_unit<1, false, MODE>(a, sm, unit, grp, lane, w); break;
-                case 3: count_unit<1, true, MODE>(a, sm, unit, grp, lane, w); break;
-                case 4: count_unit<2, false, MODE>(a, sm, unit, grp, lane, w); break;
-                case 5: count_unit<2, true, MODE>(a, sm, unit, grp, lane, w); break;
-                case 6: count_unit<3, false, MODE>(a, sm, unit, grp, lane, w); break;
-                default: count_unit<3, true, MODE>(a, sm, unit, grp, lane, w); break;
+        int32_t base;
+        uint32_t todo = next_units(a, counter, nullptr, nunits, lane, base);
+        if (base >= nunits) break;
+        while (todo) {
+            const int32_t unit = base + (__ffs(todo) - 1);
+            todo &= todo - 1;
+            const int32_t grp = a.unit_group[unit];
+            const int cloud = a.num_clouds == 1 ? 0 : a.group_cloud[grp];
+            if (cloud != cur) {
+                __syncwarp();
+                if (lane == 0) load_unit_ctx(sm.u[w], a, cloud);
+                cur = cloud;
+                __syncwarp();
             }
-        } else {
+            if (sm.u[w].error) {  // no grid: nothing found, nothing staged
+                if (lane == 0) a.rec[unit] = -1;
+                continue;
+            }
             count_unit<DIM, PERIODIC, MODE>(a, sm, unit, grp, lane, w);
         }
     }
@@ -1256,7 +1300,7 @@ __device__ __forceinline__ void emit_unit(const WalkArgs& a, EmitSmem& sm, int32
                                           int w) {
     constexpr int S = DIM == 1 ? 3 : (DIM == 2 ? 9 : 27);
     const UnitCtx& u = sm.u[w];
-    const ExactCtx xc = unit_exact_ctx(u, MODE);
+    const WrapCtx wc = wrap_ctx(u.periodic_mask, u.ext);
     const float qmax = u.qmax;
     const bool exact_all = u.exact_all != 0;
     const unsigned lt = (1u << lane) - 1u;
@@ -1301,9 +1345,9 @@ __device__ __forceinline__ void emit_unit(const WalkArgs& a, EmitSmem& sm, int32
         for (int qi = 0; qi < nb; ++qi) {
             const float4 q = sm.q[w][qi];
             bool in, unc;
-            lean_test<DIM, PERIODIC, MODE>(xc, q, cv, cw, band, in, unc);
+            lean_test<DIM, PERIODIC, MODE>(wc, q, cv, cw, band, in, unc);
             const uint32_t ub = __ballot_sync(0xffffffffu, unc);
-            if (ub) in = unc ? exact_pair_test(xc, q, q.w, cv, cv.w) : in;
+            if (ub) in = unc ? exact_pair_test(unit_exact_ctx(u, MODE), q, q.w, cv, cv.w) : in;
             const uint32_t b = __ballot_sync(0xffffffffu, in);
             const int64_t qb = __shfl_sync(0xffffffffu, obase, qi);
             int32_t qrow = __shfl_sync(0xffffffffu, qorig, qi);
@@ -1326,31 +1370,24 @@ __global__ void __launch_bounds__(kWalkWarps * 32) walk_emit_kernel(WalkArgs a) 
     __shared__ EmitSmem sm;
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
     const int32_t nlist = *a.num_list;
+    int32_t* counter = a.class_filter >= 0 ? &a.work[8 + a.class_filter] : &a.work[1];
     int cur = -1;
     for (;;) {
-        int32_t li = 0;
-        if (lane == 0) li = atomicAdd(&a.work[1], 1);
-        li = __shfl_sync(0xffffffffu, li, 0);
-        if (li >= nlist) break;
-        const int32_t unit = a.unit_list[li];
-        const int32_t grp = a.unit_group[unit];
-        const int cloud = a.num_clouds == 1 ? 0 : a.group_cloud[grp];
-        if (cloud != cur) {
-            if (lane == 0) load_unit_ctx(sm.u[w], a, cloud);
-            cur = cloud;
-            __syncwarp();
-        }
-        if (sm.u[w].error) continue;
-        if constexpr (DIM == 0) {
-            switch (sm.u[w].dim * 2 + (sm.u[w].periodic_mask != 0 ? 1 : 0)) {
-                case 2: emit_unit<1, false, MODE>(a, sm, unit, grp, lane, w); break;
-                case 3: emit_unit<1, true, MODE>(a, sm, unit, grp, lane, w); break;
-                case 4: emit_unit<2, false, MODE>(a, sm, unit, grp, lane, w); break;
-                case 5: emit_unit<2, true, MODE>(a, sm, unit, grp, lane, w); break;
-                case 6: emit_unit<3, false, MODE>(a, sm, unit, grp, lane, w); break;
-                default: emit_unit<3, true, MODE>(a, sm, unit, grp, lane, w); break;
+        int32_t base;
+        uint32_t todo = next_units(a, counter, a.unit_list, nlist, lane, base);
+        if (base >= nlist) break;
+        while (todo) {
+            const int32_t unit = a.unit_list[base + (__ffs(todo) - 1)];
+            todo &= todo - 1;
+            const int32_t grp = a.unit_group[unit];
+            const int cloud = a.num_clouds == 1 ? 0 : a.group_cloud[grp];
+            if (cloud != cur) {
+                __syncwarp();
+                if (lane == 0) load_unit_ctx(sm.u[w], a, cloud);
+                cur = cloud;
+                __syncwarp();
             }
-        } else {
+            if (sm.u[w].error) continue;
             emit_unit<DIM, PERIODIC, MODE>(a, sm, unit, grp, lane, w);
         }
     }
@@ -1550,14 +1587,14 @@ struct OffsetOut {
 
 __global__ void info_kernel(const int32_t* bad_grids, const int64_t* total, const int32_t* num_stray,
                             const int32_t* exact_clouds, const unsigned long long* cursor, const int32_t* num_flagged,
-                            int64_t* info) {
+                            const int32_t* num_exact, int64_t* info) {
     info[0] = *total;
     info[1] = *bad_grids;
     info[2] = *num_stray;
     info[3] = *exact_clouds;
     info[4] = (int64_t)*cursor;
     info[5] = *num_flagged;
-    info[6] = 0;
+    info[6] = *num_exact;
     info[7] = 0;
 }
 
@@ -1575,6 +1612,7 @@ struct HostBatch {
     bool same_sorted = false;     // self search, no periodic dims, queries are the references (same arrays)
     bool same_positions = false;  // self search, no periodic dims, same position arrays
     int walk_class = 0;           // dim * 2 + (any periodic dim) when every cloud shares it, else 0
+    uint32_t class_mask = 0;      // bit cls: some cloud with queries has class cls
     bool wide = false;            // 64-bit (cloud, cell) sort keys
 };
 
@@ -1603,6 +1641,7 @@ static int finish_batch(HostBatch& b, int64_t map_min) {
     int cls = -1;
     bool mixed = false;
     b.any_query_sup = b.any_ref_sup = false;
+    b.class_mask = 0;
     for (CloudParams& cp : b.clouds) {
         cp.query_base = (int32_t)qb;
         cp.ref_base = (int32_t)rb;
@@ -1620,6 +1659,7 @@ static int finish_batch(HostBatch& b, int64_t map_min) {
         const int c = cp.dim * 2 + (cp.periodic_mask != 0 ? 1 : 0);
         if (cls < 0) cls = c;
         else if (c != cls) mixed = true;
+        if (cp.n_query > 0) b.class_mask |= 1u << c;
     }
     b.nq = qb;
     b.nr = rb;
@@ -1727,6 +1767,22 @@ static int num_sms() {
     return nsm;
 }
 
+// Optional per-launch timing of the two heaviest kernels (count walk, record expansion): events
+// recorded around the launch on its own stream; read back with tcr_profile_kernel_ms.
+static std::mutex g_prof_mu;
+static int g_prof_on = 0;
+static int g_prof_dev = -1;
+static cudaEvent_t g_prof_ev[2][2] = {{nullptr, nullptr}, {nullptr, nullptr}};
+static int g_prof_recorded[2] = {0, 0};
+
+static void prof_mark(int kernel, int end, cudaStream_t st) {
+    if (!g_prof_on) return;
+    std::lock_guard<std::mutex> lk(g_prof_mu);
+    int dev = -1;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev != g_prof_dev) return;
+    if (cudaEventRecord(g_prof_ev[kernel][end], st) == cudaSuccess && end) g_prof_recorded[kernel] = 1;
+}
+
 static int upload_table(const HostBatch& b, const Scratch& W, cudaStream_t st) {
     for (int first = 0; first < b.C; first += kUploadChunk) {
         CloudChunk ch;
@@ -1777,14 +1833,14 @@ static WalkArgs make_walk(const HostBatch& b, const Structure& S, const Scratch&
     a.rec = W.rec;
     a.flagged = W.flagged;
     a.num_flagged = W.num_flagged;
+    a.num_exact = W.num_exact;
     a.cursor = W.cursor;
     a.query_ids = b.query_ids;
     a.ref_ids = b.ref_ids;
     return a;
 }
 
-// Dispatches a walk kernel template on the clouds' class (dim, any periodic dim) and the mode;
-// class 0 is the mixed walk.
+// Dispatches a walk kernel template on a cloud class (dim * 2 + any periodic dim) and the mode.
 template <template <int, bool, int> class L>
 static cudaError_t dispatch_walk(const WalkArgs& a, int cls, int mode, dim3 grid, dim3 block, size_t smem,
                                  cudaStream_t st) {
@@ -1801,8 +1857,7 @@ static cudaError_t dispatch_walk(const WalkArgs& a, int cls, int mode, dim3 grid
         case 4: TCR_M(2, false)
         case 5: TCR_M(2, true)
         case 6: TCR_M(3, false)
-        case 7: TCR_M(3, true)
-        default: TCR_M(0, true)
+        default: TCR_M(3, true)
     }
 #undef TCR_M
 }
@@ -1824,6 +1879,26 @@ struct EmitLaunch {
         return cudaGetLastError();
     }
 };
+
+// One walk launch for a batch of one class; one per class present (each filtering its units)
+// when the clouds mix classes.
+template <template <int, bool, int> class L>
+static cudaError_t launch_walks(const HostBatch& b, WalkArgs a, dim3 grid, dim3 block, size_t smem,
+                                cudaStream_t st) {
+    if (b.walk_class != 0) {
+        a.class_filter = -1;
+        note_launches(1);
+        return dispatch_walk<L>(a, b.walk_class, b.mode, grid, block, smem, st);
+    }
+    for (int cls = 2; cls <= 7; ++cls) {
+        if (!((b.class_mask >> cls) & 1)) continue;
+        a.class_filter = cls;
+        note_launches(1);
+        cudaError_t e = dispatch_walk<L>(a, cls, b.mode, grid, block, smem, st);
+        if (e != cudaSuccess) return e;
+    }
+    return cudaSuccess;
+}
 
 static unsigned walk_blocks(int64_t nq) {
     const int64_t max_units = (nq + kUnit - 1) / kUnit + 1;
@@ -1933,16 +2008,17 @@ static int count_impl(const HostBatch& b, const Structure& S, const Scratch& W, 
         WalkArgs a = make_walk(b, S, W);
         a.stage = stage;
         a.stage_cap = stage_cap;
-        TCR_CUDA(dispatch_walk<CountLaunch>(a, b.walk_class, b.mode, dim3(walk_blocks(nq)), dim3(kWalkWarps * 32),
-                                            sizeof(WalkSmem), st));
-        note_launches(1);
+        prof_mark(TCR_PROFILE_COUNT_WALK, 0, st);
+        TCR_CUDA(launch_walks<CountLaunch>(b, a, dim3(walk_blocks(nq)), dim3(kWalkWarps * 32), sizeof(WalkSmem), st));
+        prof_mark(TCR_PROFILE_COUNT_WALK, 1, st);
         stray_kernel<false><<<grid_for(nq, 128, num_sms() * 4), 128, 0, st>>>(a);
         note_launches(1);
     }
     CountIn ci{W.counts, nq};
     OffsetOut oo{nq, offsets, indptr_out, row_entries_out};
     TCR_CUDA(device_exclusive_scan<int64_t>(ci, oo, nq + 1, W.scan_tiles64, W.total, st));
-    info_kernel<<<1, 1, 0, st>>>(S.bad_grids, W.total, W.num_stray, W.exact_clouds, W.cursor, W.num_flagged, W.info);
+    info_kernel<<<1, 1, 0, st>>>(S.bad_grids, W.total, W.num_stray, W.exact_clouds, W.cursor, W.num_flagged,
+                                 W.num_exact, W.info);
     note_launches(1);
     if (info_out) TCR_CUDA(cudaMemcpyAsync(info_out, W.info, 8 * sizeof(int64_t), cudaMemcpyDeviceToHost, st));
     return TCR_OK;
@@ -1982,12 +2058,13 @@ static int emit_impl(const HostBatch& b, const Structure& S, const Scratch& W, c
         e.out_cap = out_capacity;
         TCR_CUDA(cudaFuncSetAttribute(expand_records_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                       (int)sizeof(ExpandSmem)));
+        prof_mark(TCR_PROFILE_EXPAND, 0, st);
         expand_records_kernel<<<blocks, kExpandWarps * 32, sizeof(ExpandSmem), st>>>(e);
+        prof_mark(TCR_PROFILE_EXPAND, 1, st);
         note_launches(1);
     }
-    TCR_CUDA(cudaMemsetAsync(W.work + 1, 0, sizeof(int32_t), st));
-    TCR_CUDA(dispatch_walk<EmitLaunch>(a, b.walk_class, b.mode, dim3(walk_blocks(nq)), dim3(kWalkWarps * 32), 0, st));
-    note_launches(1);
+    TCR_CUDA(cudaMemsetAsync(W.work, 0, sizeof(int32_t) * kWorkCounters, st));
+    TCR_CUDA(launch_walks<EmitLaunch>(b, a, dim3(walk_blocks(nq)), dim3(kWalkWarps * 32), 0, st));
     stray_kernel<true><<<grid_for(nq, 128, num_sms() * 4), 128, 0, st>>>(a);
     note_launches(1);
     return TCR_OK;
@@ -2053,6 +2130,38 @@ int64_t tcr_cloud_desc_bytes(void) { return (int64_t)sizeof(tcr_cloud_desc); }
 int64_t tcr_batch_desc_bytes(void) { return (int64_t)sizeof(tcr_batch_desc); }
 
 int64_t tcr_kernel_launches(void) { return (int64_t)__atomic_load_n(&g_launches, __ATOMIC_RELAXED); }
+
+int tcr_profile_kernels(int32_t enable) {
+    std::lock_guard<std::mutex> lk(g_prof_mu);
+    if (!enable) {
+        g_prof_on = 0;
+        return TCR_OK;
+    }
+    int dev = 0;
+    TCR_CUDA(cudaGetDevice(&dev));
+    if (dev != g_prof_dev) {
+        for (auto& pair : g_prof_ev)
+            for (auto& e : pair) {
+                if (e) cudaEventDestroy(e);
+                e = nullptr;
+            }
+        for (auto& pair : g_prof_ev)
+            for (auto& e : pair) TCR_CUDA(cudaEventCreate(&e));
+        g_prof_dev = dev;
+    }
+    g_prof_recorded[0] = g_prof_recorded[1] = 0;
+    g_prof_on = 1;
+    return TCR_OK;
+}
+
+int tcr_profile_kernel_ms(int32_t kernel, float* ms) {
+    if (kernel < 0 || kernel > 1 || !ms) return set_error(TCR_ERR_INVALID, "invalid kernel id or output");
+    std::lock_guard<std::mutex> lk(g_prof_mu);
+    if (!g_prof_recorded[kernel]) return set_error(TCR_ERR_INVALID, "no profiled launch of kernel %d", kernel);
+    TCR_CUDA(cudaEventSynchronize(g_prof_ev[kernel][1]));
+    TCR_CUDA(cudaEventElapsedTime(ms, g_prof_ev[kernel][0], g_prof_ev[kernel][1]));
+    return TCR_OK;
+}
 
 int tcr_search_sizes(int64_t n_query, int64_t n_ref, int32_t dim, int64_t* structure_bytes, int64_t* scratch_bytes) {
     if (dim < 1 || dim > 3 || n_query < 0 || n_ref < 0) return set_error(TCR_ERR_INVALID, "invalid sizes");
