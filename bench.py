@@ -353,6 +353,119 @@ def bench_batched(dev, stream, flush, steps, warmup, with_cpu):
     return res
 
 
+def make_served_workload(seed=5, n_scenes=64, rate=2000.0, seconds=1.0):
+    """64 persistent 3D scenes (sizes log-uniform in [1e3, 1e6], uniform in the periodic box
+    [-1, 1]^3, one support per scene for about 50 neighbours) and a Poisson arrival trace
+    (rate per second over `seconds`), each request naming a scene uniformly at random."""
+    import numpy as np
+    import torch
+    rng = np.random.default_rng(seed)
+    sizes = np.exp(rng.uniform(np.log(1e3), np.log(1e6), n_scenes)).astype(np.int64)
+    gen = torch.Generator().manual_seed(seed)
+    scenes = []
+    for n in sizes:
+        dx = 2.0 / float(n) ** (1.0 / 3.0)
+        h = (3 * 50 * dx ** 3 / (4 * np.pi)) ** (1 / 3)
+        scenes.append((torch.rand(int(n), 3, generator=gen) * 2 - 1, float(h)))
+    t, arrivals = 0.0, []
+    while True:
+        t += rng.exponential(1.0 / rate)
+        if t >= seconds:
+            break
+        arrivals.append((t, int(rng.integers(0, n_scenes))))
+    return scenes, arrivals
+
+
+def bench_served(dev, seconds=1.0):
+    """The served form: requests arrive on a Poisson trace; each jitters its scene by
+    N(0, (0.05 h)^2) per coordinate and searches it (gather, COO).  The search server (resident
+    scenes, incremental re-sort, HBM-budget admission, continuous batching on two streams) and the
+    per-call path (one radiusSearch per request, in arrival order) replay the same trace;
+    latency = completion - arrival, host clock."""
+    import torch
+
+    import torchcompactradius_b200 as tcr
+    from torchcompactradius_b200.serving import Request, Scene, SearchServer
+
+    scenes, arrivals = make_served_workload(seconds=seconds)
+    dom = tcr.DomainDescription(torch.full((3,), -1.0), torch.full((3,), 1.0), torch.tensor([True] * 3), 3)
+
+    def pct(v, q):
+        v = sorted(v)
+        return v[min(len(v) - 1, int(q * len(v)))]
+
+    # ---- served -------------------------------------------------------------------------
+    srv = SearchServer(dev, mode="gather", hbm_budget=40e9, slots=2)
+    for x, h in scenes:
+        srv.add_scene(Scene(x.to(dev), torch.full((x.shape[0],), h, device=dev), dom, expected_neighbours=50))
+    with srv:
+        for k in range(len(scenes)):  # warm-up: one search per scene (first build, caches)
+            srv.search(k, timeout=120)
+        srv.batches = srv.batched_requests = 0
+        torch.cuda.synchronize()
+        reqs = []
+        counted = []
+
+        def consume(r):  # count the pairs and drop the result as soon as a request completes
+            counted.append(r.result.row.numel())
+            r.result = None
+
+        t0 = time.perf_counter()
+        for ta, k in arrivals:
+            while time.perf_counter() - t0 < ta:
+                time.sleep(0.0001)
+            reqs.append(srv.submit(Request(k, arrival=t0 + ta, jitter=0.05 * scenes[k][1], on_done=consume)))
+        for r in reqs:
+            r.wait(300)
+        pairs = sum(counted)
+        t_end = max(r.finish for r in reqs)
+        lat = [1e3 * r.latency for r in reqs]
+        queue = [1e3 * (r.admitted - r.arrival) for r in reqs]
+        service = [1e3 * (r.finish - r.admitted) for r in reqs]
+        served = {"value": pairs / (t_end - t0), "unit": "pairs/s", "requests": len(reqs),
+                  "p50_ms": pct(lat, 0.5), "p99_ms": pct(lat, 0.99), "batches": srv.batches,
+                  "mean_batch": srv.batched_requests / max(srv.batches, 1), "seconds": t_end - t0,
+                  "queue_p50_ms": pct(queue, 0.5), "queue_p99_ms": pct(queue, 0.99),
+                  "service_p50_ms": pct(service, 0.5), "service_p99_ms": pct(service, 0.99)}
+        # capacity: the whole trace submitted at once
+        counted.clear()
+        srv.batches = srv.batched_requests = 0
+        t0 = time.perf_counter()
+        reqs = [srv.submit(Request(k, arrival=t0, jitter=0.05 * scenes[k][1], on_done=consume)) for _, k in arrivals]
+        for r in reqs:
+            r.wait(300)
+        t_end = max(r.finish for r in reqs)
+        served_capacity = {"value": sum(counted) / (t_end - t0), "unit": "pairs/s", "seconds": t_end - t0,
+                           "batches": srv.batches, "mean_batch": srv.batched_requests / max(srv.batches, 1)}
+
+    # ---- per call -----------------------------------------------------------------------
+    pos = [x.to(dev) for x, h in scenes]
+    sup = [torch.full((x.shape[0],), h, device=dev) for x, h in scenes]
+    for k in range(len(scenes)):
+        tcr.radiusSearch(tcr.PointCloud(pos[k], sup[k]), mode="gather", domain=dom, algorithm="compact")
+    torch.cuda.synchronize()
+    lat, pairs = [], 0
+    t0 = time.perf_counter()
+    for ta, k in arrivals:
+        while time.perf_counter() - t0 < ta:
+            time.sleep(0.0001)
+        pos[k] = pos[k] + torch.randn(pos[k].shape, device=dev) * (0.05 * scenes[k][1])
+        adj = tcr.radiusSearch(tcr.PointCloud(pos[k], sup[k]), mode="gather", domain=dom, algorithm="compact")
+        pairs += adj.row.numel()  # radiusSearch returns after the host has read the pair count
+        lat.append(1e3 * (time.perf_counter() - (t0 + ta)))
+    t_end = time.perf_counter()
+    per_call = {"value": pairs / (t_end - t0), "unit": "pairs/s", "requests": len(arrivals),
+                "p50_ms": pct(lat, 0.5), "p99_ms": pct(lat, 0.99), "seconds": t_end - t0,
+                "note": "falls behind the arrivals, so value is its capacity"}
+    return {"workload": f"64 persistent 3D scenes, sizes log-uniform [1e3, 1e6] (seed 5), periodic [-1,1]^3, "
+                        f"50 neighbours, gather, COO; Poisson arrivals 2000/s for {seconds:g} s, each request "
+                        f"jitters its scene by N(0, (0.05 h)^2); 40 GB admission budget, 2 worker streams",
+            "points": int(sum(x.shape[0] for x, h in scenes)),
+            "served": served, "served_capacity": served_capacity, "per_call": per_call,
+            "speedup_vs_per_call": served_capacity["value"] / per_call["value"],
+            "p99_ratio_per_call_over_served": per_call["p99_ms"] / served["p99_ms"]}
+
+
 def cpu_baseline_batched(clouds, budget_s=12.0):
     """The reference's own CPU search, one call per cloud (its batched radius() fails), over the
     first clouds of the workload until about budget_s seconds have passed."""
@@ -512,6 +625,8 @@ def run_b200(args):
     if world == 1 and not args.no_batched:
         line["batched"] = bench_batched(dev, stream, flush, max(3, min(args.steps, 10)), 3,
                                         rank == 0 and not args.no_cpu_baseline)
+        del flush
+        line["served"] = bench_served(dev)
     if world > 1:
         dist.destroy_process_group()
     if rank == 0 and world == 1 and not args.no_cpu_baseline:

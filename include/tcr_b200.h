@@ -94,6 +94,19 @@ typedef struct tcr_batch_desc {
     const tcr_cloud_desc* clouds;  /* HOST array [n_clouds] */
     const int32_t* query_ids;      /* device [total queries] or NULL */
     const int32_t* ref_ids;        /* device [total references] or NULL */
+    /* Incremental re-sort (optional).  ref_lin_hint (device int32 [total references]): the
+     * reference points are given in the cell order of an earlier build of the same grid, and
+     * ref_lin_hint[i] is the linear cell point i had there; the build then sorts only the points
+     * that changed cell and merges them into the rest.  The result is the one of a full build for
+     * any hint (a hint that does not hold makes the build fall back to the full sort on the device).
+     * ref_lin_out (device int32 [total references]): receives the linear cell of every point in
+     * the new cell order (reference slot k of cloud c is the cloud's k-th point in cell order), the
+     * hint of the next build once the caller has put its points in that order. */
+    const int32_t* ref_lin_hint;
+    int32_t* ref_lin_out;
+    /* Optional (device int32 [total references]): the global input index of every reference point
+     * in the new cell order -- the permutation that puts a cloud's points in that order. */
+    int32_t* ref_order_out;
 } tcr_batch_desc;
 
 /* Message of the last failing call on this thread. */
@@ -174,7 +187,9 @@ int tcr_build_structure(const tcr_search_desc* d, void* structure, int64_t struc
  * SparseCSR fields of util.py:321-358 and may be NULL.  info_out (host, 8 x int64, may be NULL)
  * receives, asynchronously on `stream`: {total pairs, grid error flag, queries walked serially,
  * exact-only mode, staging words the units asked for, units left for tcr_emit to re-test, units
- * re-tested with exact decisions because a pair lay within the fast test's rounding band, 0};
+ * re-tested with exact decisions because a pair lay within the fast test's rounding band, and
+ * for a batch built with a linear-cell hint the points its incremental re-sort sorted (-1: it fell
+ * back to the full sort; -2: no hint)};
  * a caller sizes the next search's staging list from entry 4. */
 int tcr_count(const tcr_search_desc* d, const void* structure, void* scratch, int64_t scratch_bytes, int32_t* stage,
               int64_t stage_capacity, int64_t* offsets, int32_t* indptr_out, int64_t* row_entries_out,

@@ -68,6 +68,9 @@ class BatchDesc(ctypes.Structure):
         ("clouds", ctypes.POINTER(CloudDesc)),
         ("query_ids", ctypes.c_void_p),
         ("ref_ids", ctypes.c_void_p),
+        ("ref_lin_hint", ctypes.c_void_p),
+        ("ref_lin_out", ctypes.c_void_p),
+        ("ref_order_out", ctypes.c_void_p),
     ]
 
 

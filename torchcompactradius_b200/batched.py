@@ -40,8 +40,10 @@ def cloud_table(n):
     return t
 
 
-def batch_desc(table, mode, self_search, local_index=True, query_ids=None, ref_ids=None):
-    """tcr_batch_desc over a cloud table (the table must stay alive while the descriptor is used)."""
+def batch_desc(table, mode, self_search, local_index=True, query_ids=None, ref_ids=None, lin_hint=None,
+               lin_out=None, order_out=None):
+    """tcr_batch_desc over a cloud table (the table must stay alive while the descriptor is used).
+    lin_hint / lin_out / order_out: the incremental re-sort arrays of include/tcr_b200.h."""
     if table.dtype != CLOUD_DTYPE or not table.flags["C_CONTIGUOUS"]:
         raise TypeError("the cloud table must be a contiguous CLOUD_DTYPE array")
     if CLOUD_DTYPE.itemsize != _lib.load().tcr_cloud_desc_bytes():
@@ -54,6 +56,9 @@ def batch_desc(table, mode, self_search, local_index=True, query_ids=None, ref_i
     b.clouds = ctypes.cast(table.ctypes.data, ctypes.POINTER(_lib.CloudDesc))
     b.query_ids = None if query_ids is None else query_ids.data_ptr()
     b.ref_ids = None if ref_ids is None else ref_ids.data_ptr()
+    b.ref_lin_hint = None if lin_hint is None else lin_hint.data_ptr()
+    b.ref_lin_out = None if lin_out is None else lin_out.data_ptr()
+    b.ref_order_out = None if order_out is None else order_out.data_ptr()
     return b
 
 
@@ -73,13 +78,14 @@ class BatchBuffers:
 
 
 def run_batch(table, mode, self_search, fmt, device, local_index=True, query_ids=None, ref_ids=None,
-              buffers: Optional[BatchBuffers] = None, events=None, stream=None):
+              buffers: Optional[BatchBuffers] = None, events=None, stream=None, lin_hint=None, lin_out=None,
+              order_out=None, fresh_outputs=False):
     """Runs build, count and emit of one batch on `stream` (default: torch's current stream) and
     synchronises once.  Returns a dict with the global outputs: ``row`` (COO) or None, ``col``,
     ``offsets`` (int64 [Nq+1]), ``indptr`` (int32, CSR) or None, ``counts`` (int64 [Nq]), ``total``.
     """
     lib = _lib.load()
-    b = batch_desc(table, mode, self_search, local_index, query_ids, ref_ids)
+    b = batch_desc(table, mode, self_search, local_index, query_ids, ref_ids, lin_hint, lin_out, order_out)
     s_bytes, w_bytes = _lib.batch_sizes(b)
     nq = int(table["n_query"].sum())
     stream = stream or torch.cuda.current_stream(device)
@@ -93,8 +99,15 @@ def run_batch(table, mode, self_search, fmt, device, local_index=True, query_ids
     cap = int(min(0x7fffffff, _pairs_per_query[0] * 1.25 * nq + 4096))
     stage_cap = int(min(0x7fffffff, _stage_per_query[0] * 1.1 * nq + 65536))
     stage = bufs.get("stage", stage_cap, torch.int32)
-    col = bufs.get("col", cap, torch.int64)
-    row = bufs.get("row", cap, torch.int64) if fmt == "coo" else None
+    if fresh_outputs:  # outputs owned by the caller, not reused by the next search on these buffers
+        offsets = torch.empty(nq + 1, dtype=torch.int64, device=device)
+        counts = torch.empty(max(nq, 0), dtype=torch.int64, device=device)
+        indptr = torch.empty(nq + 1, dtype=torch.int32, device=device) if fmt == "csr" else None
+        col = torch.empty(cap, dtype=torch.int64, device=device)
+        row = torch.empty(cap, dtype=torch.int64, device=device) if fmt == "coo" else None
+    else:
+        col = bufs.get("col", cap, torch.int64)
+        row = bufs.get("row", cap, torch.int64) if fmt == "coo" else None
     info = bufs._bufs.get("info")
     if info is None:
         info = torch.zeros(8, dtype=torch.int64, pin_memory=True)
@@ -130,8 +143,12 @@ def run_batch(table, mode, self_search, fmt, device, local_index=True, query_ids
     if fmt == "csr" and total > 0x7fffffff:
         raise ValueError(f"{total} pairs do not fit the int32 indptr of SparseCSR")
     if total > cap:  # the estimate was short: emit again into exact buffers (the count is kept)
-        col = bufs.get("col", total, torch.int64)
-        row = bufs.get("row", total, torch.int64) if fmt == "coo" else None
+        if fresh_outputs:
+            col = torch.empty(total, dtype=torch.int64, device=device)
+            row = torch.empty(total, dtype=torch.int64, device=device) if fmt == "coo" else None
+        else:
+            col = bufs.get("col", total, torch.int64)
+            row = bufs.get("row", total, torch.int64) if fmt == "coo" else None
         _lib.check(lib.tcr_batch_emit(ctypes.byref(b), _ptr(sbuf), _ptr(scratch), w_bytes, _ptr(stage),
                                       _ptr(offsets), _ptr(row), _ptr(col), total, sptr), "tcr_batch_emit")
     return dict(row=None if row is None else row[:total], col=col[:total], offsets=offsets, indptr=indptr,

@@ -148,9 +148,17 @@ struct Scratch {
     int32_t* stray;         // [nq]
     int32_t* rec;           // [nq] per unit: offset of its record in the staging list (-1: not staged)
     int32_t* flagged;       // [nq] units re-walked by the emit pass
+    // incremental re-sort (builds given the previous cell of every reference point), else null
+    int32_t* stay;          // [nr] 1: the point is still in its previous cell
+    void* stay_keys;        // [nr] keys of the unmoved points, input order (sorted when the hint holds)
+    int32_t* stay_idx;      // [nr]
+    void* moved_keys[2];    // [nr] keys of the moved points (sorted in place)
+    int32_t* moved_vals[2]; // [nr]
+    void* moved_state;      // SortState of the moved points' sort
+    int32_t* inc_count;     // [2] unmoved points, hint broken (1: fall back to the full sort)
 };
 
-static Scratch carve_scratch(void* buf, int64_t nq, int64_t nr, int64_t C, int64_t* bytes) {
+static Scratch carve_scratch(void* buf, int64_t nq, int64_t nr, int64_t C, bool incremental, int64_t* bytes) {
     Carve c{(char*)buf, 0};
     Scratch s;
     const int64_t nmax = std::max<int64_t>(std::max<int64_t>(nq, nr), 1);
@@ -190,6 +198,16 @@ static Scratch carve_scratch(void* buf, int64_t nq, int64_t nr, int64_t C, int64
     s.stray = c.take<int32_t>(q);
     s.rec = c.take<int32_t>(q);
     s.flagged = c.take<int32_t>(q);
+    const int64_t ni = incremental ? std::max<int64_t>(nr, 1) : 0;
+    s.stay = incremental ? c.take<int32_t>(ni) : nullptr;
+    s.stay_keys = incremental ? c.take<unsigned long long>(ni) : nullptr;
+    s.stay_idx = incremental ? c.take<int32_t>(ni) : nullptr;
+    for (int k = 0; k < 2; ++k) {
+        s.moved_keys[k] = incremental ? c.take<unsigned long long>(ni) : nullptr;
+        s.moved_vals[k] = incremental ? c.take<int32_t>(ni) : nullptr;
+    }
+    s.moved_state = incremental ? c.take<SortState64>(1) : nullptr;
+    s.inc_count = incremental ? c.take<int32_t>(2) : nullptr;
     if (bytes) *bytes = c.off;
     return s;
 }
@@ -531,11 +549,13 @@ __device__ __forceinline__ void load_point_ctx(PointCtx& p, const CloudParams* _
 // Wrap (twice for the reference cloud, cppSearch.py:221 after neighborhood.py:203; once for a
 // query cloud), pack to float4 and emit the (cloud, linear cell) key.  A cloud without a valid
 // grid gets one constant key (its points form one cell that no walk visits).
+// hint (incremental build): the point's previous linear cell; stay[i] = it is still there.
 template <typename K>
 __global__ void pack_points_kernel(const CloudParams* __restrict__ table, GridParams* grid,
                                    const int32_t* __restrict__ prefix, int C, int64_t n, int query_side, int wraps,
                                    int track_grid, float4* __restrict__ pack, K* __restrict__ keys,
-                                   int32_t* __restrict__ vals, SortStateT<K>* st) {
+                                   int32_t* __restrict__ vals, SortStateT<K>* st,
+                                   const int32_t* __restrict__ hint = nullptr, int32_t* __restrict__ stay = nullptr) {
     K kmin = ~(K)0, kmax = 0;
     const int64_t per = (n + gridDim.x - 1) / gridDim.x;
     const int64_t lo = (int64_t)blockIdx.x * per;
@@ -560,6 +580,7 @@ __global__ void pack_points_kernel(const CloudParams* __restrict__ table, GridPa
         }
         K key;
         make_key(key, p.cloud, lin ^ 0x80000000u);
+        if (stay) stay[i] = (!p.error && hint[i] == (int32_t)lin) ? 1 : 0;
         pack[i] = v;
         keys[i] = key;
         vals[i] = (int32_t)i;
@@ -673,16 +694,126 @@ struct CellOut {
     }
 };
 
+// lin_out (optional): the linear cell of each sorted point, the hint of the next incremental build;
+// order_out (optional): a copy of the sort index.
 template <typename K>
 __global__ void gather_sorted_kernel(const float4* __restrict__ pack, const int32_t* vals0, const int32_t* vals1,
                                      const SortStateT<K>* st, int64_t n, float4* __restrict__ sorted,
-                                     int32_t* __restrict__ sidx) {
+                                     int32_t* __restrict__ sidx, const K* keys0 = nullptr, const K* keys1 = nullptr,
+                                     int32_t* __restrict__ lin_out = nullptr,
+                                     int32_t* __restrict__ order_out = nullptr) {
     const int32_t* v = st->sel[key_passes<K>()] ? vals1 : vals0;
+    const K* k = st->sel[key_passes<K>()] ? keys1 : keys0;
     const int64_t stride = (int64_t)gridDim.x * blockDim.x;
     for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
         const int32_t p = v[i];
         sorted[i] = pack[p];
         sidx[i] = p;
+        if (lin_out) lin_out[i] = (int32_t)(key_low(k[i]) ^ 0x80000000u);
+        if (order_out) order_out[i] = p;
+    }
+}
+
+// ------------------------------------------------------------------------------------------
+// incremental re-sort
+//
+// A build may be given the reference points in the cell order of a previous build, with each
+// point's previous linear cell (the hint).  The points still in their cell ("unmoved") then form
+// a subsequence already sorted by (key, input index); only the moved points are radix-sorted, and
+// the two sorted lists are merged by (key, input index) -- exactly the stable sort of the input.
+// The unmoved subsequence is verified on the device; if it is not sorted (a wrong hint), or too
+// many points moved, the full radix sort runs instead.  Every kernel reads the decision from the
+// device, so the build enqueues without a host round trip.
+
+struct StayIn {
+    const int32_t* stay;
+    __device__ int32_t operator()(int64_t i) const { return stay[i]; }
+};
+template <typename K>
+struct StayOut {
+    const K* keys;        // the pack output, input order
+    K* stay_keys;
+    int32_t* stay_idx;
+    K* moved_keys;
+    int32_t* moved_vals;
+    __device__ void operator()(int64_t i, int32_t ex, int32_t flag) const {
+        if (flag) {
+            stay_keys[ex] = keys[i];
+            stay_idx[ex] = (int32_t)i;
+        } else {
+            moved_keys[i - ex] = keys[i];
+            moved_vals[i - ex] = (int32_t)i;
+        }
+    }
+};
+
+template <typename K>
+__global__ void inc_check_kernel(const K* __restrict__ stay_keys, const int32_t* n_stay, int32_t* bad) {
+    const int64_t n = *n_stay;
+    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    bool ok = true;
+    for (int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; k + 1 < n; k += stride)
+        ok &= stay_keys[k] <= stay_keys[k + 1];
+    if (!__all_sync(0xffffffffu, ok) && (threadIdx.x & 31) == 0) atomicOr(bad, 1);
+}
+
+// Chooses the path: the moved points' sort and the merge, or the full sort (one thread).
+template <typename K>
+__global__ void inc_decide_kernel(SortStateT<K>* full, SortStateT<K>* moved, const int32_t* counts, int64_t n) {
+    const int64_t n_stay = counts[0];
+    const bool fallback = counts[1] != 0 || 2 * n_stay < n;  // wrong hint, or most points moved
+    sort_state_reset(moved);
+    if (fallback) {
+        moved->key_min = moved->key_max = 0;  // no moved sort
+        return;
+    }
+    moved->key_min = full->key_min;  // a superset of the moved keys' range
+    moved->key_max = full->key_max;
+    moved->n_dev = n - n_stay;
+    full->key_min = full->key_max = 0;  // no full sort: the merge writes the sorted keys in place
+}
+
+// Number of list entries ordered before (key, idx); the list is sorted by (key, idx).
+template <typename K>
+__device__ __forceinline__ int64_t count_before(const K* keys, const int32_t* idx, int64_t n, K key, int32_t i) {
+    int64_t lo = 0, hi = n;
+    while (lo < hi) {
+        const int64_t mid = (lo + hi) >> 1;
+        const K km = keys[mid];
+        if (km < key || (km == key && idx[mid] < i)) lo = mid + 1;
+        else hi = mid;
+    }
+    return lo;
+}
+
+// Merges the unmoved and the sorted moved points into keys/vals (input buffer 0 of the full sort,
+// whose passes are all skipped on this path).
+template <typename K>
+__global__ void inc_merge_kernel(const K* __restrict__ stay_keys, const int32_t* __restrict__ stay_idx,
+                                 const K* moved_k0, const K* moved_k1, const int32_t* moved_v0,
+                                 const int32_t* moved_v1, const SortStateT<K>* moved, const int32_t* counts,
+                                 int64_t n, K* __restrict__ keys, int32_t* __restrict__ vals) {
+    if (counts[1] != 0 || 2 * (int64_t)counts[0] < n) return;  // the full sort runs instead
+    const int64_t n_stay = counts[0], n_moved = n - n_stay;
+    const int s = moved->sel[key_passes<K>()];
+    const K* mk = s ? moved_k1 : moved_k0;
+    const int32_t* mv = s ? moved_v1 : moved_v0;
+    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < n; t += stride) {
+        K key;
+        int32_t i;
+        int64_t pos;
+        if (t < n_stay) {
+            key = stay_keys[t];
+            i = stay_idx[t];
+            pos = t + count_before(mk, mv, n_moved, key, i);
+        } else {
+            key = mk[t - n_stay];
+            i = mv[t - n_stay];
+            pos = (t - n_stay) + count_before(stay_keys, stay_idx, n_stay, key, i);
+        }
+        keys[pos] = key;
+        vals[pos] = i;
     }
 }
 
@@ -1587,7 +1718,7 @@ struct OffsetOut {
 
 __global__ void info_kernel(const int32_t* bad_grids, const int64_t* total, const int32_t* num_stray,
                             const int32_t* exact_clouds, const unsigned long long* cursor, const int32_t* num_flagged,
-                            const int32_t* num_exact, int64_t* info) {
+                            const int32_t* num_exact, const int32_t* inc_count, int64_t n_ref, int64_t* info) {
     info[0] = *total;
     info[1] = *bad_grids;
     info[2] = *num_stray;
@@ -1595,7 +1726,8 @@ __global__ void info_kernel(const int32_t* bad_grids, const int64_t* total, cons
     info[4] = (int64_t)*cursor;
     info[5] = *num_flagged;
     info[6] = *num_exact;
-    info[7] = 0;
+    // incremental build: points sorted by the small sort (-1: the full sort ran); -2: no hint
+    info[7] = inc_count ? ((inc_count[1] != 0 || 2 * (int64_t)inc_count[0] < n_ref) ? -1 : n_ref - inc_count[0]) : -2;
 }
 
 // ------------------------------------------------------------------------------------------
@@ -1614,6 +1746,9 @@ struct HostBatch {
     int walk_class = 0;           // dim * 2 + (any periodic dim) when every cloud shares it, else 0
     uint32_t class_mask = 0;      // bit cls: some cloud with queries has class cls
     bool wide = false;            // 64-bit (cloud, cell) sort keys
+    const int32_t* lin_hint = nullptr;  // incremental build: previous linear cell of every reference point
+    int32_t* lin_out = nullptr;         // receives the linear cell of every sorted reference point
+    int32_t* order_out = nullptr;       // receives the input index of every sorted reference point
 };
 
 // Validation shared by both descriptors.  level 0: sizes only; 1: query phases (the reference
@@ -1725,6 +1860,9 @@ static int batch_of(const tcr_batch_desc* bd, int level, HostBatch& b) {
     b.local_index = bd->local_index ? 1 : 0;
     b.query_ids = bd->query_ids;
     b.ref_ids = bd->ref_ids;
+    b.lin_hint = bd->ref_lin_hint;
+    b.lin_out = bd->ref_lin_out;
+    b.order_out = bd->ref_order_out;
     b.clouds.resize(bd->n_clouds);
     char who[48];
     for (int k = 0; k < bd->n_clouds; ++k) {
@@ -1752,7 +1890,7 @@ static int batch_of(const tcr_batch_desc* bd, int level, HostBatch& b) {
 
 static void batch_sizes(const HostBatch& b, int64_t* s, int64_t* w) {
     if (s) carve_structure(nullptr, b.nr, b.C, b.map_total, s);
-    if (w) carve_scratch(nullptr, b.nq, b.nr, b.C, w);
+    if (w) carve_scratch(nullptr, b.nq, b.nr, b.C, b.lin_hint != nullptr, w);
 }
 
 static inline unsigned grid_for(int64_t n, int threads, int max_blocks = 148 * 16) {
@@ -1933,12 +2071,35 @@ static int build_impl(const HostBatch& b, const Structure& S, const Scratch& W, 
     TCR_CUDA(cudaMemsetAsync(S.map, 0xff, sizeof(unsigned long long) * S.map_total, st));
     TCR_CUDA(cudaMemsetAsync(S.num_cells, 0, sizeof(int32_t), st));
     if (nr > 0) {
+        const bool inc = b.lin_hint != nullptr;
         pack_points_kernel<K><<<grid_for(nr, 256), 256, 0, st>>>(W.table, S.grid, W.ref_prefix, C, nr, 0, 2, 1, W.pack,
-                                                                 sw.keys[0], sw.vals[0], sw.state);
+                                                                 sw.keys[0], sw.vals[0], sw.state,
+                                                                 inc ? b.lin_hint : nullptr, inc ? W.stay : nullptr);
         note_launches(1);
+        if (inc) {
+            SortWorkspaceT<K> mw = sw;
+            mw.keys[0] = reinterpret_cast<K*>(W.moved_keys[0]);
+            mw.keys[1] = reinterpret_cast<K*>(W.moved_keys[1]);
+            mw.vals[0] = W.moved_vals[0];
+            mw.vals[1] = W.moved_vals[1];
+            mw.state = reinterpret_cast<SortStateT<K>*>(W.moved_state);
+            TCR_CUDA(cudaMemsetAsync(W.inc_count, 0, 2 * sizeof(int32_t), st));
+            StayOut<K> so{sw.keys[0], reinterpret_cast<K*>(W.stay_keys), W.stay_idx, mw.keys[0], mw.vals[0]};
+            TCR_CUDA(device_exclusive_scan<int32_t>(StayIn{W.stay}, so, nr, W.scan_tiles32, W.inc_count, st));
+            inc_check_kernel<K><<<grid_for(nr, 256), 256, 0, st>>>(reinterpret_cast<const K*>(W.stay_keys),
+                                                                   W.inc_count, W.inc_count + 1);
+            inc_decide_kernel<K><<<1, 1, 0, st>>>(sw.state, mw.state, W.inc_count, nr);
+            note_launches(2);
+            TCR_CUDA(radix_sort_pairs<K>(mw, nr, st));
+            inc_merge_kernel<K><<<grid_for(nr, 256), 256, 0, st>>>(
+                reinterpret_cast<const K*>(W.stay_keys), W.stay_idx, mw.keys[0], mw.keys[1], mw.vals[0], mw.vals[1],
+                mw.state, W.inc_count, nr, sw.keys[0], sw.vals[0]);
+            note_launches(1);
+        }
         TCR_CUDA(radix_sort_pairs<K>(sw, nr, st));
         gather_sorted_kernel<K><<<grid_for(nr, 256), 256, 0, st>>>(W.pack, sw.vals[0], sw.vals[1], sw.state, nr,
-                                                                   S.rsorted, S.rsidx);
+                                                                   S.rsorted, S.rsidx, sw.keys[0], sw.keys[1],
+                                                                   b.lin_out, b.order_out);
         note_launches(1);
         CellOut<K> co{W.table, S.grid, sw.keys[0], sw.keys[1], sw.state, S.rsorted, S.cell_start, S.cell_lin,
                       S.cell_coords, S.cell_bucket, S.cell_cloud, S.map};
@@ -2018,7 +2179,7 @@ static int count_impl(const HostBatch& b, const Structure& S, const Scratch& W, 
     OffsetOut oo{nq, offsets, indptr_out, row_entries_out};
     TCR_CUDA(device_exclusive_scan<int64_t>(ci, oo, nq + 1, W.scan_tiles64, W.total, st));
     info_kernel<<<1, 1, 0, st>>>(S.bad_grids, W.total, W.num_stray, W.exact_clouds, W.cursor, W.num_flagged,
-                                 W.num_exact, W.info);
+                                 W.num_exact, b.lin_hint && b.nr > 0 ? W.inc_count : nullptr, b.nr, W.info);
     note_launches(1);
     if (info_out) TCR_CUDA(cudaMemcpyAsync(info_out, W.info, 8 * sizeof(int64_t), cudaMemcpyDeviceToHost, st));
     return TCR_OK;
@@ -2078,7 +2239,7 @@ static int run_build(const HostBatch& b, void* structure, int64_t structure_byte
         return set_error(TCR_ERR_INVALID, "workspace too small (structure %lld/%lld, scratch %lld/%lld)",
                          (long long)structure_bytes, (long long)need_s, (long long)scratch_bytes, (long long)need_w);
     const Structure S = carve_structure(structure, b.nr, b.C, b.map_total, nullptr);
-    const Scratch W = carve_scratch(scratch, b.nq, b.nr, b.C, nullptr);
+    const Scratch W = carve_scratch(scratch, b.nq, b.nr, b.C, b.lin_hint != nullptr, nullptr);
     cudaStream_t st = (cudaStream_t)stream;
     return b.wide ? build_impl<unsigned long long>(b, S, W, st) : build_impl<uint32_t>(b, S, W, st);
 }
@@ -2093,7 +2254,7 @@ static int run_count(const HostBatch& b, const void* structure, void* scratch, i
     if (stage_capacity < 0 || stage_capacity > 0x7fffffffLL || (stage_capacity > 0 && !stage))
         return set_error(TCR_ERR_INVALID, "stage capacity must be in [0, 2^31) with a buffer");
     const Structure S = carve_structure(const_cast<void*>(structure), b.nr, b.C, b.map_total, nullptr);
-    const Scratch W = carve_scratch(scratch, b.nq, b.nr, b.C, nullptr);
+    const Scratch W = carve_scratch(scratch, b.nq, b.nr, b.C, b.lin_hint != nullptr, nullptr);
     cudaStream_t st = (cudaStream_t)stream;
     return b.wide ? count_impl<unsigned long long>(b, S, W, stage, stage_capacity, offsets, indptr_out,
                                                    row_entries_out, info_out, st)
@@ -2109,7 +2270,7 @@ static int run_emit(const HostBatch& b, const void* structure, void* scratch, in
     if (!structure || !scratch || scratch_bytes < need_w || !offsets)
         return set_error(TCR_ERR_INVALID, "workspace too small or offsets missing");
     const Structure S = carve_structure(const_cast<void*>(structure), b.nr, b.C, b.map_total, nullptr);
-    const Scratch W = carve_scratch(scratch, b.nq, b.nr, b.C, nullptr);
+    const Scratch W = carve_scratch(scratch, b.nq, b.nr, b.C, b.lin_hint != nullptr, nullptr);
     return emit_impl(b, S, W, stage, offsets, row_out, col_out, out_capacity, (cudaStream_t)stream);
 }
 
@@ -2166,7 +2327,7 @@ int tcr_profile_kernel_ms(int32_t kernel, float* ms) {
 int tcr_search_sizes(int64_t n_query, int64_t n_ref, int32_t dim, int64_t* structure_bytes, int64_t* scratch_bytes) {
     if (dim < 1 || dim > 3 || n_query < 0 || n_ref < 0) return set_error(TCR_ERR_INVALID, "invalid sizes");
     if (structure_bytes) carve_structure(nullptr, n_ref, 1, hash_capacity(n_ref, kSingleMapMin), structure_bytes);
-    if (scratch_bytes) carve_scratch(nullptr, n_query, n_ref, 1, scratch_bytes);
+    if (scratch_bytes) carve_scratch(nullptr, n_query, n_ref, 1, false, scratch_bytes);
     return TCR_OK;
 }
 

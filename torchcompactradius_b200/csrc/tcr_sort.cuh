@@ -24,7 +24,8 @@ template <typename K>
 struct SortStateT {
     K key_min, key_max;   // reduced by the producer of the keys
     int32_t sel[9];       // sel[p]: which buffer (0/1) holds the input of pass p
-    int32_t pad[3];
+    int32_t pad;
+    int64_t n_dev;        // >= 0: sort only the first n_dev keys (a count known on the device only)
     uint32_t seen[8][8];  // per pass: bitmap of the digit values the histogram met
 };
 using SortState32 = SortStateT<uint32_t>;
@@ -42,6 +43,7 @@ __device__ __forceinline__ void sort_state_reset(SortStateT<K>* st) {
     st->key_min = ~(K)0;
     st->key_max = 0;
     st->sel[0] = 0;
+    st->n_dev = -1;
     for (int p = 0; p < 8; ++p)
         for (int i = 0; i < 8; ++i) st->seen[p][i] = 0u;
 }
@@ -73,6 +75,7 @@ __global__ void __launch_bounds__(kSortThreads) radix_hist_kernel(const K* keys0
                                                                   int pass, int64_t ntiles, SortStateT<K>* st,
                                                                   int32_t* hist) {
     if (!pass_needed(st, shift)) return;
+    if (st->n_dev >= 0 && st->n_dev < n) n = st->n_dev;
     const K* keys = st->sel[pass] ? keys1 : keys0;
     __shared__ int32_t sh[kBins];
     for (int i = threadIdx.x; i < kBins; i += kSortThreads) sh[i] = 0;
@@ -104,6 +107,7 @@ __global__ void __launch_bounds__(kSortThreads) radix_scatter_kernel(K* keys0, K
         if (blockIdx.x == 0 && threadIdx.x == 0) st->sel[pass + 1] = s;
         return;
     }
+    if (st->n_dev >= 0 && st->n_dev < n) n = st->n_dev;
     const K* kin = s ? keys1 : keys0;
     const int32_t* vin = s ? vals1 : vals0;
     K* kout = s ? keys0 : keys1;
@@ -229,7 +233,7 @@ inline int64_t sort_tiles(int64_t n) { return (n + kSortTile - 1) / kSortTile; }
 inline int64_t sort_hist_elems(int64_t n) { return (int64_t)kBins * sort_tiles(n); }
 
 // Sorts keys[sel0]/vals[sel0] (sel0 = state->sel[0], set by the producer, which also reduced the
-// key range and cleared the digit bitmaps).  The result lives in buffer state->sel[key_passes<K>()]
+// key range and cleared the digit bitmaps), n keys or state->n_dev when that is set and smaller.  The result lives in buffer state->sel[key_passes<K>()]
 // after the call; consumers read the selector on the device.
 template <typename K>
 inline cudaError_t radix_sort_pairs(const SortWorkspaceT<K>& w, int64_t n, cudaStream_t st) {
