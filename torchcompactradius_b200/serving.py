@@ -4,28 +4,29 @@ A scene is a point cloud that lives on the device across requests -- one simulat
 training scene whose points move a little between timesteps.  A request advances a scene (adds a
 displacement to its points) and asks for its adjacency.  The server
 
-* keeps every scene on the device in the cell order of its last search, with each point's user
-  index and linear cell: the next search of the scene re-sorts incrementally (only the points
-  that changed cell are sorted and merged, ``tcr_batch_desc.ref_lin_hint``) instead of
-  rebuilding from scratch;
+* keeps every scene in a device arena (one per dimension: positions, supports, user indices and
+  linear cells of all scenes in fixed segments), in the cell order of the scene's last search, so
+  the next search re-sorts incrementally: only the points that changed cell are sorted and merged
+  (``tcr_batch_desc.ref_lin_hint``) instead of rebuilding from scratch;
 * admits pending requests in arrival order while their estimated device memory fits the HBM
   budget and their scene has no request in flight (a scene's requests run in order);
 * runs each admitted group as one batched search (``tcr_batch_*``: one set of launches for all
   its scenes) on one of ``slots`` worker streams, so a group admitted while another is still on
   the GPU runs beside it: requests that arrive during a search are admitted as soon as a slot and
-  memory free up (continuous batching), not after the queue drains.
+  memory free up (continuous batching), not after the queue drains.  The host work of a group is
+  a fixed number of vectorised operations over the arena, whatever the number of scenes in it.
 
 Results are in the scene's user numbering (``SparseCOO`` rows and columns are the indices the
-scene was created with; rows come grouped in the scene's cell order), ready for use on the default
+scene was given with; rows come grouped in the scene's cell order), ready for use on the default
 stream when the request completes, and a request's result does not depend on what it was batched
-with: the batched engine gives each cloud exactly its single-search result.  The reference has no serving
-layer; each request there is one ``radiusSearch`` call (src/torchCompactRadius/neighborhood.py:
-136-309) that rebuilds its structure.
+with: the batched engine gives each cloud exactly its single-search result.  The reference has no
+serving layer; each request there is one ``radiusSearch`` call (src/torchCompactRadius/
+neighborhood.py:136-309) that rebuilds its structure.
 """
 import collections
 import threading
 import time
-from typing import List, Optional
+from typing import Dict, List, Optional
 
 import numpy as np
 import torch
@@ -41,33 +42,21 @@ BYTES_PER_PAIR = 22
 
 
 class Scene:
-    """A persistent cloud on the device, stored in the cell order of its last search."""
+    """What a scene starts from: positions [n, dim], supports [n], its domain and hashMapLength."""
 
     def __init__(self, positions: torch.Tensor, supports: torch.Tensor, domain: DomainDescription,
-                 hashMapLength: int = 4096, device=None, expected_neighbours: float = 64.0):
-        device = _require_cuda(torch.device(device) if device is not None else positions.device)
-        self.device = device
+                 hashMapLength: int = 4096, expected_neighbours: float = 64.0):
+        if positions.dim() != 2 or not 1 <= positions.shape[1] <= 3:
+            raise ValueError("positions must be [n, dim] with dim 1, 2 or 3")
+        if supports.shape[0] != positions.shape[0]:
+            raise ValueError("one support per point")
+        self.positions = positions
+        self.supports = supports
         self.dim = int(positions.shape[1])
         self.n = int(positions.shape[0])
-        self.pos = _as_f32(positions, device).clone()          # stored order
-        self.sup = _as_f32(supports, device).clone()
-        self.ids = torch.arange(self.n, dtype=torch.int32, device=device)  # user index of stored point k
-        self.lin = None                                        # linear cell of stored point k (the hint)
         self.lo, self.hi, self.mask = _domain_host(domain, self.dim)
         self.hashMapLength = int(hashMapLength)
         self.expected_neighbours = float(expected_neighbours)
-        self.steps = 0
-
-    def positions(self) -> torch.Tensor:
-        """Current positions in user order."""
-        out = torch.empty_like(self.pos)
-        out.index_copy_(0, self.ids.long(), self.pos)
-        return out
-
-    def supports(self) -> torch.Tensor:
-        out = torch.empty_like(self.sup)
-        out.index_copy_(0, self.ids.long(), self.sup)
-        return out
 
     def bytes_estimate(self) -> int:
         return int(self.n * (BYTES_PER_POINT + BYTES_PER_PAIR * self.expected_neighbours))
@@ -75,15 +64,14 @@ class Scene:
 
 class Request:
     """Advance scene `scene` by `displacement` (user order [n, dim], or None) -- or by Gaussian
-    noise of standard deviation `jitter` drawn on the device from `seed` -- and search it."""
+    noise of standard deviation `jitter` drawn on the device -- and search it."""
 
     def __init__(self, scene: int, displacement: Optional[torch.Tensor] = None, arrival: Optional[float] = None,
-                 jitter: Optional[float] = None, seed: Optional[int] = None, on_done=None):
+                 jitter: Optional[float] = None, on_done=None):
         self.scene = scene
-        self.on_done = on_done  # called by the worker with the request when it completes
         self.displacement = displacement
-        self.jitter = jitter  # instead of a displacement: N(0, jitter^2) per coordinate, drawn on the device
-        self.seed = seed
+        self.jitter = jitter
+        self.on_done = on_done  # called by the worker with the request when it completes
         self.arrival = time.perf_counter() if arrival is None else arrival
         self.admitted = None
         self.finish = None
@@ -103,6 +91,26 @@ class Request:
         return None if self.finish is None else self.finish - self.arrival
 
 
+class _Arena:
+    """The scenes of one dimension on the device, each in a fixed segment."""
+
+    def __init__(self, dim, scenes, device):
+        self.dim = dim
+        n = np.array([s.n for s in scenes], dtype=np.int64)
+        self.base = np.zeros(len(scenes) + 1, dtype=np.int64)
+        np.cumsum(n, out=self.base[1:])
+        total = int(self.base[-1])
+        self.pos = torch.empty(max(total, 1), dim, dtype=torch.float32, device=device)
+        self.sup = torch.empty(max(total, 1), dtype=torch.float32, device=device)
+        self.ids = torch.empty(max(total, 1), dtype=torch.int32, device=device)
+        self.lin = torch.full((max(total, 1),), -1, dtype=torch.int32, device=device)  # no hint yet
+        for k, s in enumerate(scenes):
+            a, b = int(self.base[k]), int(self.base[k + 1])
+            self.pos[a:b] = _as_f32(s.positions, device)
+            self.sup[a:b] = _as_f32(s.supports, device)
+            self.ids[a:b] = torch.arange(s.n, dtype=torch.int32, device=device)
+
+
 class SearchServer:
     """Continuous-batching search server over persistent scenes (see the module docstring)."""
 
@@ -115,6 +123,9 @@ class SearchServer:
         self.slots = int(slots)
         self.max_batch = int(max_batch)
         self.scenes: List[Scene] = []
+        self._arenas: Dict[int, _Arena] = {}
+        self._tables = {}
+        self._where = []  # scene -> (dim, index within its arena)
         self._pending = collections.deque()
         self._busy = set()
         self._in_use = 0
@@ -126,15 +137,55 @@ class SearchServer:
 
     # -- setup ----------------------------------------------------------------------------
     def add_scene(self, scene: Scene) -> int:
+        """Adds a scene (before start())."""
+        if self._running:
+            raise RuntimeError("add scenes before starting the server")
         if scene.bytes_estimate() > self.hbm_budget:
             raise ValueError("the scene alone exceeds the HBM budget")
         self.scenes.append(scene)
         return len(self.scenes) - 1
 
+    def _build_arenas(self):
+        self._where = [None] * len(self.scenes)
+        self._arenas, self._tables = {}, {}
+        for dim in (1, 2, 3):
+            ks = [k for k, s in enumerate(self.scenes) if s.dim == dim]
+            if not ks:
+                continue
+            ar = _Arena(dim, [self.scenes[k] for k in ks], self.device)
+            t = cloud_table(len(ks))
+            for j, k in enumerate(ks):
+                s = self.scenes[k]
+                self._where[k] = (dim, j)
+                t["dim"][j] = dim
+                t["periodic_mask"][j] = s.mask
+                t["domain_min"][j, :dim] = s.lo
+                t["domain_max"][j, :dim] = s.hi
+                t["hash_map_length"][j] = s.hashMapLength
+                t["n_query"][j] = t["n_ref"][j] = s.n
+                a = int(ar.base[j])
+                t["query_pos"][j] = t["ref_pos"][j] = ar.pos.data_ptr() + 4 * dim * a
+                t["query_sup"][j] = t["ref_sup"][j] = ar.sup.data_ptr() + 4 * a
+            self._arenas[dim] = ar
+            self._tables[dim] = t
+        torch.cuda.synchronize(self.device)
+
+    def positions(self, scene: int) -> torch.Tensor:
+        """A scene's current positions in user order (call while it has no request in flight)."""
+        if not self._where:
+            return self.scenes[scene].positions
+        dim, j = self._where[scene]
+        ar = self._arenas[dim]
+        a, b = int(ar.base[j]), int(ar.base[j + 1])
+        out = torch.empty_like(ar.pos[a:b])
+        out.index_copy_(0, ar.ids[a:b].long(), ar.pos[a:b])
+        return out
+
     def start(self):
         with self._cv:
             if self._running:
                 return self
+            self._build_arenas()
             self._running = True
         for slot in range(self.slots):
             t = threading.Thread(target=self._worker, args=(slot,), daemon=True)
@@ -190,7 +241,7 @@ class SearchServer:
         try:
             torch.cuda.set_device(self.device)
             stream = torch.cuda.Stream(self.device)
-            bufs = BatchBuffers(self.device)
+            bufs = {d: BatchBuffers(self.device) for d in (1, 2, 3)}
         except BaseException as ex:  # no worker: fail what waits instead of leaving it hanging
             with self._cv:
                 while self._pending:
@@ -209,7 +260,10 @@ class SearchServer:
                 if not batch:
                     return
             try:
-                self._run(batch, stream, bufs)
+                for dim in (1, 2, 3):
+                    group = [r for r in batch if self.scenes[r.scene].dim == dim]
+                    if group:
+                        self._run(group, dim, stream, bufs[dim])
             except BaseException as ex:  # the requests report it; the server keeps serving
                 for r in batch:
                     r.error = ex
@@ -231,68 +285,58 @@ class SearchServer:
                             r.error = ex
                     r._done.set()
 
-    def _run(self, batch, stream, bufs):
+    def _run(self, group, dim, stream, bufs):
+        """One batched search over the scenes of `group` (all of dimension dim)."""
         dev = self.device
-        for r in batch:
+        ar = self._arenas[dim]
+        for r in group:
             r.admitted = time.perf_counter()
-        scenes = [self.scenes[r.scene] for r in batch]
+        js = np.array([self._where[r.scene][1] for r in group], dtype=np.int64)
+        n = ar.base[js + 1] - ar.base[js]
+        bb = np.zeros(len(js) + 1, dtype=np.int64)  # batch bases
+        np.cumsum(n, out=bb[1:])
+        T = int(bb[-1])
+        table = np.ascontiguousarray(self._tables[dim][js])
         user = torch.cuda.default_stream(dev)
-        stream.wait_stream(user)  # displacements and scenes made on the caller's stream are ready
-        for sc in scenes:  # scene arrays move between worker streams: no reuse before this one is done
-            for t in (sc.pos, sc.sup, sc.ids, sc.lin):
-                if t is not None:
-                    t.record_stream(stream)
+        stream.wait_stream(user)  # explicit displacements made on the caller's stream are ready
         with torch.cuda.stream(stream):
-            for r, sc in zip(batch, scenes):
+            # arena index of every batch slot: arena base of its scene + its offset in the scene
+            # (expanded from per-scene values on the device)
+            ns = torch.as_tensor(n, device=dev)
+            shift = torch.repeat_interleave(torch.as_tensor(ar.base[js] - bb[:-1], device=dev), ns, output_size=T)
+            dst = torch.arange(T, device=dev) + shift
+            jit = np.array([r.jitter or 0.0 for r in group], dtype=np.float32)
+            if jit.any():
+                sig = torch.repeat_interleave(torch.as_tensor(jit, device=dev), ns, output_size=T)
+                ar.pos.index_add_(0, dst, torch.randn(T, dim, device=dev) * sig[:, None])
+            for k, r in enumerate(group):
                 if r.displacement is not None:
+                    a, b = int(ar.base[js[k]]), int(ar.base[js[k] + 1])
                     d = r.displacement.to(device=dev, dtype=torch.float32, non_blocking=True)
-                    sc.pos.add_(d.index_select(0, sc.ids.long()))
-                elif r.jitter:
-                    g = torch.Generator(device=dev)
-                    g.manual_seed(int(r.seed) if r.seed is not None else int(time.perf_counter_ns()))
-                    d = torch.randn(sc.pos.shape, generator=g, device=dev) * float(r.jitter)
-                    sc.pos.add_(d.index_select(0, sc.ids.long()))
-            C = len(scenes)
-            table = cloud_table(C)
-            n = np.array([sc.n for sc in scenes], dtype=np.int64)
-            base = np.zeros(C + 1, dtype=np.int64)
-            np.cumsum(n, out=base[1:])
-            for k, sc in enumerate(scenes):
-                table["dim"][k] = sc.dim
-                table["periodic_mask"][k] = sc.mask
-                table["domain_min"][k, :sc.dim] = sc.lo
-                table["domain_max"][k, :sc.dim] = sc.hi
-                table["hash_map_length"][k] = sc.hashMapLength
-                table["n_query"][k] = table["n_ref"][k] = sc.n
-                table["query_pos"][k] = table["ref_pos"][k] = sc.pos.data_ptr() if sc.n else 0
-                table["query_sup"][k] = table["ref_sup"][k] = sc.sup.data_ptr() if sc.n else 0
-            total = int(base[-1])
-            ids = torch.cat([sc.ids for sc in scenes]) if C > 1 else scenes[0].ids
-            hint = None
-            if any(sc.lin is not None for sc in scenes):
-                hint = torch.cat([sc.lin if sc.lin is not None else
-                                  torch.full((sc.n,), -1, dtype=torch.int32, device=dev) for sc in scenes])
-            lin_out = torch.empty(max(total, 1), dtype=torch.int32, device=dev)
-            order_out = torch.empty(max(total, 1), dtype=torch.int32, device=dev)
+                    ar.pos[a:b] += d.index_select(0, ar.ids[a:b].long())
+            ids = ar.ids.index_select(0, dst)
+            hint = ar.lin.index_select(0, dst)
+            lin_out = bufs.get("lin_out", T, torch.int32)
+            order_out = bufs.get("order_out", T, torch.int32)
             out = run_batch(table, self.mode, True, "coo", dev, local_index=False, query_ids=ids, ref_ids=ids,
                             buffers=bufs, stream=stream, lin_hint=hint, lin_out=lin_out, order_out=order_out,
                             fresh_outputs=True)
             for t in (out["row"], out["col"]):
                 t.record_stream(user)  # results are read on the default stream
-            offs = out["offsets"].index_select(0, torch.as_tensor(base, device=dev)).cpu().tolist()
-            for k, (r, sc) in enumerate(zip(batch, scenes)):
-                p0, p1 = offs[k], offs[k + 1]
-                r.result = SparseCOO(out["row"][p0:p1], out["col"][p0:p1], sc.n, sc.n)
-                # keep the scene in its new cell order: the next search re-sorts incrementally
-                perm = (order_out[int(base[k]):int(base[k + 1])] - int(base[k])).long()
-                sc.pos = sc.pos.index_select(0, perm)
-                sc.sup = sc.sup.index_select(0, perm)
-                sc.ids = sc.ids.index_select(0, perm)
-                sc.lin = lin_out[int(base[k]):int(base[k + 1])].clone()
-                sc.steps += 1
+            # keep every scene in its new cell order (the next search re-sorts incrementally)
+            src = order_out.long() + shift
+            ar.pos.index_copy_(0, dst, ar.pos.index_select(0, src))
+            ar.sup.index_copy_(0, dst, ar.sup.index_select(0, src))
+            ar.ids.index_copy_(0, dst, ar.ids.index_select(0, src))
+            ar.lin.index_copy_(0, dst, lin_out)
+            offs = out["offsets"].index_select(0, torch.as_tensor(bb, device=dev)).cpu().tolist()
+            for k, r in enumerate(group):
+                m = int(n[k])
+                r.result = SparseCOO(out["row"][offs[k]:offs[k + 1]], out["col"][offs[k]:offs[k + 1]], m, m)
             stream.synchronize()
 
     # -- convenience ----------------------------------------------------------------------
-    def search(self, scene: int, displacement: Optional[torch.Tensor] = None, timeout=None) -> SparseCOO:
+    def search(self, scene: int, displacement: Optional[torch.Tensor] = None, timeout=None,
+               jitter: Optional[float] = None) -> SparseCOO:
         """Submits one request and waits for it."""
-        return self.submit(Request(scene, displacement)).wait(timeout)
+        return self.submit(Request(scene, displacement, jitter=jitter)).wait(timeout)
