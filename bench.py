@@ -489,6 +489,35 @@ def cpu_baseline_batched(clouds, budget_s=12.0):
             "sample": f"the first {k} of {len(clouds)} clouds, one reference call per cloud ({pairs} pairs)"}
 
 
+class Ranks:
+    """The multi-GPU plumbing of the bench: one process per GPU, every rank an independent replica
+    of the workload; the only collectives are a barrier around the timed region and a max-reduce of
+    each rank's device time (whole-job value = pairs of all ranks / the slowest rank's time)."""
+
+    def __init__(self, world, device=None):
+        self.world = world
+        self.device = device
+
+    def barrier(self):
+        if self.world > 1:
+            import torch.distributed as dist
+            dist.barrier()
+
+    def max(self, v):
+        if self.world == 1:
+            return v
+        import torch
+        import torch.distributed as dist
+        t = torch.tensor([float(v)], dtype=torch.float64, device=self.device)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    def value(self, pairs_per_rank, steps, total_ms_this_rank):
+        """pairs/s of the whole job: every rank did `pairs_per_rank` pairs per step."""
+        slowest = self.max(total_ms_this_rank)
+        return pairs_per_rank * steps * self.world / (slowest / 1e3), slowest
+
+
 def run_b200(args):
     import torch
     import torch.distributed as dist
@@ -506,16 +535,9 @@ def run_b200(args):
         from datetime import timedelta
         dist.init_process_group("nccl", timeout=timedelta(seconds=120), device_id=dev)
 
-    def barrier():
-        if world > 1:
-            dist.barrier()
-
-    def max_over_ranks(v):
-        if world == 1:
-            return v
-        t = torch.tensor([v], dtype=torch.float64, device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item())
+    ranks = Ranks(world, dev)
+    barrier = ranks.barrier
+    max_over_ranks = ranks.max
 
     pos_h, sup_h = make_workload()
     pos_pin, sup_pin = pos_h.pin_memory(), sup_h.pin_memory()
@@ -562,8 +584,7 @@ def run_b200(args):
     launches = lib.tcr_kernel_launches() - launches0
     _lib.check(lib.tcr_profile_kernels(0), "tcr_profile_kernels")
     clocks = clk.stop()
-    total_ms = max_over_ranks(sum(step_ms))
-    value = pairs * args.steps * world / (total_ms / 1e3)
+    value, total_ms = ranks.value(pairs, args.steps, sum(step_ms))
 
     # ---- end to end through the public API (pinned host in, host out) ----------------------
     nq = N_POINTS
