@@ -9,11 +9,15 @@ symmetric mode, CSR output -- 51,798,992 pairs per step.
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
 
 Prints one JSON line.  `value` is pairs/s with inputs resident in HBM and L2 flushed (a 256 MiB
-write) between timed steps, timed with CUDA events on the launching stream (max over ranks
-under torchrun; every rank runs an independent replica, "replicas only").  `e2e` is the same
-metric through the public API with the inputs copied from pinned host memory and the whole
-CSR result copied back every step.  `roofline` covers the dominant kernel (the emitting
-candidate walk), `cpu_baseline` the reference's own CPU operators on this host.
+write) between timed steps, each step one whole search (build + count + emit) recorded once as a
+CUDA graph and replayed, timed with CUDA events on the launching stream (max over ranks under
+torchrun; every rank runs an independent replica, "replicas only").  `e2e` is the same metric
+through the public radiusSearch with the inputs copied from pinned host memory and the whole CSR
+result copied back every step.  `roofline` covers the dominant kernel (the count walk, timed live
+inside the replays), `search_roofline` the whole search, `cpu_baseline` the reference's own CPU
+operators on this host.  `batched`, `graphs` and `served` measure the other forms: 256 clouds per
+launch against the per-call loop, graph replay against the eager API, and a request trace served
+with continuous batching against per-call searches.
 """
 import argparse
 import json
@@ -466,6 +470,74 @@ def bench_served(dev, seconds=1.0):
             "p99_ratio_per_call_over_served": per_call["p99_ms"] / served["p99_ms"]}
 
 
+def make_small_workload(seed=0):
+    """The reference's CPU-runnable case: 64 x 64 cell centres in the periodic [-1, 1]^2, jittered by
+    U(-0.1 dx, 0.1 dx), dx = 2/64, uniform support sqrt(32 dx^2 / pi) (about 32 neighbours)."""
+    import numpy as np
+    import torch
+    g = torch.Generator().manual_seed(seed)
+    dx = 2.0 / 64
+    c = -1.0 + dx * (torch.arange(64, dtype=torch.float32) + 0.5)
+    pos = torch.stack(torch.meshgrid(c, c, indexing="ij"), -1).reshape(-1, 2)
+    pos = pos + (torch.rand(pos.shape, generator=g) * 0.2 - 0.1) * dx
+    h = torch.full((pos.shape[0],), float((32 * dx * dx / np.pi) ** 0.5))
+    return pos.contiguous(), h
+
+
+def bench_graphs(dev, flush, steps=200):
+    """CUDA-graph replay (graphs.StaticSearch) against the eager public API: host-observed latency
+    of one search of the small 2D workload, and device time of the 1M-point search."""
+    import torch
+
+    import torchcompactradius_b200 as tcr
+    from torchcompactradius_b200.graphs import StaticSearch
+
+    def pct(v, q):
+        v = sorted(v)
+        return v[min(len(v) - 1, int(q * len(v)))]
+
+    pos, h = make_small_workload()
+    pos, h = pos.to(dev), h.to(dev)
+    dom = tcr.DomainDescription(torch.full((2,), -1.0), torch.full((2,), 1.0), torch.tensor([True, True]), 2)
+    ss = StaticSearch(tcr.PointCloud(pos, h), dom, mode="gather", format="coo")
+    eager, graph = [], []
+    for k in range(steps + 10):
+        t = time.perf_counter()
+        a = tcr.radiusSearch(tcr.PointCloud(pos, h), mode="gather", domain=dom, algorithm="compact", format="coo")
+        t1 = time.perf_counter()
+        b = ss.run()
+        t2 = time.perf_counter()
+        if k >= 10:
+            eager.append(1e3 * (t1 - t))
+            graph.append(1e3 * (t2 - t1))
+    same = torch.equal(a.row, b.row) and torch.equal(a.col, b.col)
+    small = {"workload": "4096-point jittered 64x64 grid, periodic [-1,1]^2, gather, COO (host-observed latency "
+                         "per search, output on the device)", "pairs": int(a.row.numel()),
+             "eager_p50_ms": pct(eager, 0.5), "eager_p99_ms": pct(eager, 0.99),
+             "graph_p50_ms": pct(graph, 0.5), "graph_p99_ms": pct(graph, 0.99), "same_result": bool(same)}
+    pos_h, sup_h = make_workload()
+    p1, h1 = pos_h.to(dev), sup_h.to(dev)
+    dom3 = tcr.DomainDescription(torch.full((3,), -1.0), torch.full((3,), 1.0), torch.tensor([False] * 3), 3)
+    big = StaticSearch(tcr.PointCloud(p1, h1), dom3, mode="symmetric", format="csr")
+    stream = big.plan.stream
+    ms = []
+    for k in range(13):
+        flush.fill_(k & 0xff)
+        torch.cuda.synchronize()
+        s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        s.record(stream)
+        with torch.cuda.stream(stream):
+            big.plan.graph.replay()
+        e.record(stream)
+        e.synchronize()
+        if k >= 3:
+            ms.append(s.elapsed_time(e))
+    pairs = int(big.run().indices.numel())
+    return {"small": small,
+            "big": {"workload": WORKLOAD, "graph_replay_ms": statistics.mean(ms),
+                    "value": pairs / (statistics.mean(ms) / 1e3), "unit": "pairs/s"}}
+
+
 def cpu_baseline_batched(clouds, budget_s=12.0):
     """The reference's own CPU search, one call per cloud (its batched radius() fails), over the
     first clouds of the workload until about budget_s seconds have passed."""
@@ -524,6 +596,7 @@ def run_b200(args):
 
     import torchcompactradius_b200 as tcr
     from torchcompactradius_b200 import _lib
+    from torchcompactradius_b200.graphs import StaticSearch
     from torchcompactradius_b200.search import compact_search
 
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -557,33 +630,55 @@ def run_b200(args):
     pairs = int(col.numel())
     torch.cuda.synchronize()
 
-    # ---- device-resident timing -----------------------------------------------------------
-    clk = Clocks(local)
-    clk.start()
-    barrier()
-    torch.cuda.synchronize()
+    # ---- phases of the eager path (public API) ------------------------------------------------
     _lib.check(lib.tcr_profile_kernels(1), "tcr_profile_kernels")
-    launches0 = lib.tcr_kernel_launches()
-    step_ms, emit_ms, count_ms, build_ms, walk_ms, expand_ms = [], [], [], [], [], []
-    for k in range(args.steps):
-        flush.fill_(k & 0xff)  # L2 flush outside the step's events
+    eager_ms, build_ms, count_ms, emit_ms = [], [], [], []
+    for k in range(max(3, min(args.steps, 10))):
+        flush.fill_(k & 0xff)
         ev = {}
         s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        l0 = lib.tcr_kernel_launches()
         s.record(stream)
         device_step(ev)
         e.record(stream)
         e.synchronize()
-        step_ms.append(s.elapsed_time(e))
+        per_search_launches = lib.tcr_kernel_launches() - l0
+        eager_ms.append(s.elapsed_time(e))
         build_ms.append(ev["build"][0].elapsed_time(ev["build"][1]))
         count_ms.append(ev["count"][0].elapsed_time(ev["count"][1]))
         emit_ms.append(ev["emit"][0].elapsed_time(ev["emit"][1]))
+
+    # ---- device-resident timing: the search recorded once as a CUDA graph and replayed --------
+    # (graphs.StaticSearch; profiling is on while it records, so the count walk and expansion
+    # launches carry their timing events inside the graph)
+    plan = StaticSearch(tcr.PointCloud(pos_d, sup_d), dom, mode="symmetric", format="csr")
+    pstream = plan.plan.stream
+    for _ in range(3):
+        plan.run()
+    clk = Clocks(local)
+    clk.start()
+    barrier()
+    torch.cuda.synchronize()
+    step_ms, walk_ms, expand_ms = [], [], []
+    for k in range(args.steps):
+        flush.fill_(k & 0xff)  # L2 flush outside the step's events
+        torch.cuda.current_stream(dev).synchronize()
+        s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        s.record(pstream)
+        with torch.cuda.stream(pstream):
+            plan.plan.graph.replay()
+        e.record(pstream)
+        e.synchronize()
+        step_ms.append(s.elapsed_time(e))
         walk_ms.append(_lib.profile_kernel_ms(_lib.PROFILE_COUNT_WALK))
         expand_ms.append(_lib.profile_kernel_ms(_lib.PROFILE_EXPAND))
     torch.cuda.synchronize()
     barrier()
-    launches = lib.tcr_kernel_launches() - launches0
-    _lib.check(lib.tcr_profile_kernels(0), "tcr_profile_kernels")
+    launches = per_search_launches * args.steps  # kernel nodes of the recorded search, per replay
     clocks = clk.stop()
+    _lib.check(lib.tcr_profile_kernels(0), "tcr_profile_kernels")
+    replay = plan.run()
+    assert replay.indices.numel() == pairs and torch.equal(replay.indptr, indptr)
     value, total_ms = ranks.value(pairs, args.steps, sum(step_ms))
 
     # ---- end to end through the public API (pinned host in, host out) ----------------------
@@ -626,9 +721,12 @@ def run_b200(args):
         "vs_baseline": None, "dtype": "f32", "data": "synthetic", "impl": "b200", "config": config(pairs),
         "p50_ms": statistics.median(step_ms), "p99_ms": sorted(step_ms)[min(len(step_ms) - 1,
                                                                          int(0.99 * len(step_ms)))],
+        "execution": "build+count+emit recorded once as a CUDA graph (graphs.StaticSearch) and replayed per step",
+        "eager_ms_per_step": statistics.mean(eager_ms),
         "phases_ms": {"build": statistics.mean(build_ms), "count": statistics.mean(count_ms),
                       "emit": statistics.mean(emit_ms), "count_walk_kernel": statistics.mean(walk_ms),
-                      "expand_kernel": statistics.mean(expand_ms)},
+                      "expand_kernel": statistics.mean(expand_ms), "of": "phases of the eager path; kernels of the "
+                      "timed replays"},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                      "traffic": traffic, "kernel": "walk_count_kernel<3,false,symmetric> (every pair test)",
                      "algorithmic_bytes_per_launch": walk_bytes, "launch_ms": statistics.mean(walk_ms),
@@ -646,6 +744,7 @@ def run_b200(args):
     if world == 1 and not args.no_batched:
         line["batched"] = bench_batched(dev, stream, flush, max(3, min(args.steps, 10)), 3,
                                         rank == 0 and not args.no_cpu_baseline)
+        line["graphs"] = bench_graphs(dev, flush)
         del flush
         line["served"] = bench_served(dev)
     if world > 1:

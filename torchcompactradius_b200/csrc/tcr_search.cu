@@ -1918,7 +1918,12 @@ static void prof_mark(int kernel, int end, cudaStream_t st) {
     std::lock_guard<std::mutex> lk(g_prof_mu);
     int dev = -1;
     if (cudaGetDevice(&dev) != cudaSuccess || dev != g_prof_dev) return;
-    if (cudaEventRecord(g_prof_ev[kernel][end], st) == cudaSuccess && end) g_prof_recorded[kernel] = 1;
+    // External: under stream capture the record becomes an event node of the graph, so replays
+    // of a recorded search time the kernel too
+    cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+    if (cudaStreamIsCapturing(st, &cs) != cudaSuccess) return;
+    const unsigned flags = cs == cudaStreamCaptureStatusActive ? cudaEventRecordExternal : cudaEventRecordDefault;
+    if (cudaEventRecordWithFlags(g_prof_ev[kernel][end], st, flags) == cudaSuccess && end) g_prof_recorded[kernel] = 1;
 }
 
 static int upload_table(const HostBatch& b, const Scratch& W, cudaStream_t st) {
@@ -2000,11 +2005,25 @@ static cudaError_t dispatch_walk(const WalkArgs& a, int cls, int mode, dim3 grid
 #undef TCR_M
 }
 
+// Raises a kernel's dynamic shared memory limit once per device (not a stream operation, so a
+// search can be recorded into a CUDA graph after its first eager run).
+template <typename F>
+static cudaError_t ensure_smem(F* kernel, int bytes, uint64_t* done_mask) {
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return e;
+    const uint64_t bit = 1ull << (dev & 63);
+    if (__atomic_load_n(done_mask, __ATOMIC_ACQUIRE) & bit) return cudaSuccess;
+    e = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+    if (e == cudaSuccess) __atomic_fetch_or(done_mask, bit, __ATOMIC_ACQ_REL);
+    return e;
+}
+
 template <int D, bool P, int M>
 struct CountLaunch {
     static cudaError_t launch(const WalkArgs& a, dim3 g, dim3 b, size_t smem, cudaStream_t st) {
-        cudaError_t e = cudaFuncSetAttribute(walk_count_kernel<D, P, M>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                             (int)smem);
+        static uint64_t done = 0;
+        cudaError_t e = ensure_smem(walk_count_kernel<D, P, M>, (int)smem, &done);
         if (e != cudaSuccess) return e;
         walk_count_kernel<D, P, M><<<g, b, smem, st>>>(a);
         return cudaGetLastError();
@@ -2217,8 +2236,8 @@ static int emit_impl(const HostBatch& b, const Structure& S, const Scratch& W, c
         e.row_out = row_out;
         e.col_out = col_out;
         e.out_cap = out_capacity;
-        TCR_CUDA(cudaFuncSetAttribute(expand_records_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                      (int)sizeof(ExpandSmem)));
+        static uint64_t expand_attr_done = 0;
+        TCR_CUDA(ensure_smem(expand_records_kernel, (int)sizeof(ExpandSmem), &expand_attr_done));
         prof_mark(TCR_PROFILE_EXPAND, 0, st);
         expand_records_kernel<<<blocks, kExpandWarps * 32, sizeof(ExpandSmem), st>>>(e);
         prof_mark(TCR_PROFILE_EXPAND, 1, st);
