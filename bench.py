@@ -46,6 +46,8 @@ def parse():
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-batched", action="store_true", help="skip the batched-form measurement")
+    ap.add_argument("--profile-searches", type=int, default=0,
+                    help="only run this many eager searches of the workload (a small case for ncu captures)")
     return ap.parse_args()
 
 
@@ -100,8 +102,8 @@ def measured_peak():
 
 
 def ncu_traffic():
-    """dram bytes per launch of the emitting walk from the committed ncu summary, if any."""
-    p = os.path.join(REPO, "profiles", "walk_emit_3d_1m.txt")
+    """dram bytes per launch of the count walk from the committed ncu summary, if any."""
+    p = os.path.join(REPO, "profiles", "walk_count_3d_1m.txt")
     try:
         with open(p) as f:
             m = re.search(r"dram_bytes_per_launch_full_size:\s*([0-9.eE+]+)", f.read())
@@ -250,10 +252,13 @@ def run_reference(args):
 
 def bench_batched(dev, stream, flush, steps, warmup, with_cpu):
     """The batched form on the 256-cloud workload: one batched search per step (device-timed, L2
-    flushed between steps) against the per-call loop of radiusSearch over the same clouds on the
-    same GPU, plus the end-to-end batched call from pinned host memory."""
+    flushed between steps, walk parameters autotuned on it first) against the per-call loop of
+    radiusSearch over the same clouds on the same GPU, plus the end-to-end batched call from pinned
+    host memory."""
     import numpy as np
     import torch
+
+    from torchcompactradius_b200.tuning import Autotuner
 
     import torchcompactradius_b200 as tcr
     from torchcompactradius_b200 import batched
@@ -288,6 +293,8 @@ def bench_batched(dev, stream, flush, steps, warmup, with_cpu):
     for _ in range(warmup):
         out = step()
     pairs = out["total"]
+    tuner = Autotuner(reps=2)
+    tuned = tuner.tune(step, key="batched")
     ms = []
     for k in range(steps):
         flush.fill_(k & 0xff)
@@ -344,6 +351,8 @@ def bench_batched(dev, stream, flush, steps, warmup, with_cpu):
     res = {"workload": "256 clouds, sizes log-uniform [1e3, 2e5] (seed 4), 128 2D + 128 3D, uniform in [-1,1]^d, "
                        "per-dim periodicity Bernoulli(0.5), 32 (2D) / 50 (3D) neighbours, gather, CSR",
            "clouds": C, "points": n_points, "pairs_per_step": pairs,
+           "tuning": {"chosen": {"queries_per_unit": tuned[0], "walk_blocks_per_sm": tuned[1]},
+                      "ms_per_step": {f"{c[0]}q/{c[1]}b": round(v, 3) for c, v in tuner.timings["batched"].items()}},
            "value": batched_value, "unit": "pairs/s", "ms_per_step": statistics.mean(ms),
            "p50_ms": statistics.median(ms), "p99_ms": sorted(ms)[min(len(ms) - 1, int(0.99 * len(ms)))],
            "per_call": {"value": per_call_value, "unit": "pairs/s", "ms_per_batch": statistics.mean(pc_ms),
@@ -598,6 +607,7 @@ def run_b200(args):
     from torchcompactradius_b200 import _lib
     from torchcompactradius_b200.graphs import StaticSearch
     from torchcompactradius_b200.search import compact_search
+    from torchcompactradius_b200.tuning import Autotuner, set_tuning
 
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -629,6 +639,11 @@ def run_b200(args):
         col, indptr, entries = device_step()
     pairs = int(col.numel())
     torch.cuda.synchronize()
+    # the walks' run-time parameters, picked on this workload (no result depends on them)
+    tuner = Autotuner(reps=3)
+    tuned = tuner.tune(lambda: device_step(), key="headline")
+    tuning = {"chosen": {"queries_per_unit": tuned[0], "walk_blocks_per_sm": tuned[1]},
+              "ms_per_search": {f"{c[0]}q/{c[1]}b": round(v, 4) for c, v in tuner.timings["headline"].items()}}
 
     # ---- phases of the eager path (public API) ------------------------------------------------
     _lib.check(lib.tcr_profile_kernels(1), "tcr_profile_kernels")
@@ -740,10 +755,12 @@ def run_b200(args):
                 "ms_per_step": e2e_total / len(e2e_ms), "output_checked": bool(ok)},
         "gpu_launches": int(launches),
         "clocks": clocks,
+        "tuning": tuning,
     }
     if world == 1 and not args.no_batched:
         line["batched"] = bench_batched(dev, stream, flush, max(3, min(args.steps, 10)), 3,
                                         rank == 0 and not args.no_cpu_baseline)
+        set_tuning(0, 0)  # the other forms run with the defaults
         line["graphs"] = bench_graphs(dev, flush)
         del flush
         line["served"] = bench_served(dev)
@@ -762,8 +779,23 @@ def run_b200(args):
     return 0
 
 
+def profile_searches(n):
+    """n eager searches of the 1M-point workload through the public engine, nothing else."""
+    import torch
+    from torchcompactradius_b200.search import compact_search
+    pos, sup = make_workload()
+    p, h = pos.cuda(), sup.cuda()
+    for _ in range(n):
+        (col, _, _), _ = compact_search(p, h, p, h, [-1.0] * 3, [1.0] * 3, 0, "symmetric", 4096, "csr", True)
+    torch.cuda.synchronize()
+    print(json.dumps({"profile_searches": n, "pairs": int(col.numel())}))
+    return 0
+
+
 def main():
     args = parse()
+    if args.profile_searches:
+        return profile_searches(args.profile_searches)
     if args.impl == "reference":
         return run_reference(args)
     return run_b200(args)

@@ -135,6 +135,12 @@ int64_t tcr_kernel_launches(void);
 int tcr_profile_kernels(int32_t enable);
 int tcr_profile_kernel_ms(int32_t kernel, float* ms);
 
+/* Run-time tuning for later searches of this process (no reference counterpart; the autotuner of
+ * torchcompactradius_b200.tuning picks them): queries per work unit of the walks -- 32, 16 or 8,
+ * i.e. 1, 2 or 4 lanes per query -- and resident walk blocks per SM (1..64).  0 keeps the default
+ * (32, 12).  No setting changes a result; a search uses the unit size in force at its tcr_count. */
+int tcr_set_tuning(int32_t unit_queries, int32_t walk_blocks_per_sm);
+
 /* Byte sizes of the persistent structure (reference-side cell table and hash map, kept for
  * reuse like the reference's CompactHashMap, compactHashing/datastructure.py:8-31) and of the
  * per-search scratch.  Host-only; no device work. */

@@ -142,3 +142,12 @@ def test_coo_csr_helpers():
     assert csr.rowEntries.dtype == torch.int64 and csr.rowEntries.tolist() == [2, 0, 3, 0]
     back = csr_to_coo(csr)
     assert back.row.tolist() == row.tolist() and back.col.tolist() == col.tolist()
+
+
+def test_tuning_is_validated():
+    from torchcompactradius_b200 import _lib
+    lib = _lib.load()
+    assert lib.tcr_set_tuning(12, 0) == -1 and b"unit_queries" in lib.tcr_last_error()
+    assert lib.tcr_set_tuning(0, 65) == -1
+    assert lib.tcr_set_tuning(16, 8) == 0
+    assert lib.tcr_set_tuning(0, 0) == 0  # back to the defaults

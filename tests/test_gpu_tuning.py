@@ -1,0 +1,50 @@
+"""Tuning never changes a result: every (queries per unit, blocks per SM) setting gives the same
+CSR, and the autotuner leaves one of its candidates in force."""
+import numpy as np
+import pytest
+import torch
+
+pytestmark = pytest.mark.gpu
+
+
+def _search(x, h, dom, mode):
+    import torchcompactradius_b200 as tcr
+    return tcr.radiusSearch(tcr.PointCloud(x, h), mode=mode, domain=dom, algorithm="compact", format="csr")
+
+
+@pytest.mark.parametrize("dim,periodic,mode", [(3, False, "symmetric"), (2, True, "gather"), (3, True, "scatter")])
+def test_every_setting_gives_the_same_result(dim, periodic, mode):
+    import torchcompactradius_b200 as tcr
+    from torchcompactradius_b200.tuning import CANDIDATES, set_tuning
+    g = torch.Generator().manual_seed(dim)
+    n = 30000
+    x = (torch.rand(n, dim, generator=g) * 2 - 1).cuda()
+    dx = 2.0 / n ** (1.0 / dim)
+    h0 = (32 * dx * dx / np.pi) ** 0.5 if dim == 2 else (3 * 50 * dx ** 3 / (4 * np.pi)) ** (1 / 3)
+    h = (h0 * (0.9 + 0.2 * torch.rand(n, generator=g))).cuda()
+    dom = tcr.DomainDescription(torch.full((dim,), -1.0), torch.full((dim,), 1.0), torch.tensor([periodic] * dim), dim)
+    try:
+        set_tuning(32, 12)
+        ref = _search(x, h, dom, mode)
+        for cfg in CANDIDATES + [(8, 1), (16, 64)]:
+            set_tuning(*cfg)
+            got = _search(x, h, dom, mode)
+            assert torch.equal(got.indices, ref.indices) and torch.equal(got.indptr, ref.indptr), cfg
+    finally:
+        set_tuning(0, 0)
+
+
+def test_autotuner_picks_a_candidate_and_remembers_it():
+    import torchcompactradius_b200 as tcr
+    from torchcompactradius_b200.tuning import Autotuner, set_tuning, signature
+    x = (torch.rand(50000, 3) * 2 - 1).cuda()
+    h = torch.full((50000,), 0.06).cuda()
+    dom = tcr.DomainDescription(torch.full((3,), -1.0), torch.full((3,), 1.0), torch.tensor([False] * 3), 3)
+    tuner = Autotuner(reps=2)
+    key = signature([3], [False], 50000, "gather", 50)
+    try:
+        best = tuner.tune(lambda: _search(x, h, dom, "gather"), key)
+        assert best in tuner.candidates and len(tuner.timings[key]) == len(tuner.candidates)
+        assert tuner.tune(lambda: None, key) == best  # remembered: no timing the second time
+    finally:
+        set_tuning(0, 0)

@@ -86,6 +86,7 @@ SIGNATURES = {
     "tcr_batch_desc_bytes": (_i64, []),
     "tcr_kernel_launches": (_i64, []),
     "tcr_profile_kernels": (ctypes.c_int, [_i32]),
+    "tcr_set_tuning": (ctypes.c_int, [_i32, _i32]),
     "tcr_profile_kernel_ms": (ctypes.c_int, [_i32, ctypes.POINTER(ctypes.c_float)]),
     "tcr_search_sizes": (ctypes.c_int, [_i64, _i64, _i32, ctypes.POINTER(_i64), ctypes.POINTER(_i64)]),
     "tcr_structure_offsets": (ctypes.c_int, [_i64, ctypes.POINTER(_i64), _i32]),

@@ -67,6 +67,12 @@ constexpr int64_t kBatchMapMin = 64;     // per cloud of a batch
 // one cloud class (cls = dim * 2 + periodic, 2..7) in a batch that mixes classes.
 constexpr int kWorkCounters = 16;
 
+// Run-time tuning (tcr_set_tuning): queries per work unit -- 32, 16 or 8, i.e. 1, 2 or 4 lanes of
+// the walk per query -- and resident walk blocks per SM.  Neither changes a result: a query's
+// candidates and their order do not depend on how queries are grouped into units.
+static int g_unit_cap = 32;
+static int g_walk_blocks_per_sm = 12;
+
 struct Carve {
     char* base;
     int64_t off;
@@ -129,6 +135,7 @@ struct Scratch {
     int32_t* num_flagged;   // [1]
     int32_t* exact_clouds;  // [1] clouds whose every pair takes the exact test
     int32_t* num_exact;     // [1] units the count walk re-tested with exact decisions
+    int32_t* unit_cap;      // [1] queries per work unit of this search (set by the count phase)
     unsigned long long* cursor;  // [1] staging fill
     float4* pack;           // [max(nq,nr)] packed input points before sorting
     void* keys[2];          // [max(nq,nr)] 64-bit slots (32-bit keys use the first half)
@@ -176,6 +183,7 @@ static Scratch carve_scratch(void* buf, int64_t nq, int64_t nr, int64_t C, bool 
     s.num_flagged = c.take<int32_t>(1);
     s.exact_clouds = c.take<int32_t>(1);
     s.num_exact = c.take<int32_t>(1);
+    s.unit_cap = c.take<int32_t>(1);
     s.cursor = c.take<unsigned long long>(1);
     s.pack = c.take<float4>(nmax);
     s.keys[0] = c.take<unsigned long long>(nmax);
@@ -453,7 +461,7 @@ __global__ void query_params_kernel(const CloudParams* __restrict__ table, const
 }
 
 // Zeroes the per-search counters and the per-cloud query statistics.
-__global__ void count_init_kernel(Scratch W, int C) {
+__global__ void count_init_kernel(Scratch W, int C, int unit_cap) {
     for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < C; c += gridDim.x * blockDim.x) {
         W.qparams[c].stats.max_key = 0;
         W.qparams[c].stats.bad = 0;
@@ -465,6 +473,7 @@ __global__ void count_init_kernel(Scratch W, int C) {
         *W.num_flagged = 0;
         *W.exact_clouds = 0;
         *W.num_exact = 0;
+        *W.unit_cap = unit_cap;
         *W.cursor = 0ull;
     }
 }
@@ -870,17 +879,16 @@ struct QueryGroupOut {
     }
 };
 
-constexpr int kUnit = 32;  // queries per work unit (one warp)
-
 // Group count comes from a device scalar; the scan kernels are launched over the upper bound
-// and read the true count through the functor.
+// and read the true count through the functor.  A unit holds at most `cap` (<= 32) queries.
 struct BoundedUnitCountIn {
     const int32_t* group_start;
     const int32_t* num_groups;
+    int32_t cap;
     __device__ int32_t operator()(int64_t g) const {
         if (g >= *num_groups) return 0;
         int32_t n = group_start[g + 1] - group_start[g];
-        return (n + kUnit - 1) / kUnit;
+        return (n + cap - 1) / cap;
     }
 };
 struct BoundedUnitOut {
@@ -888,12 +896,13 @@ struct BoundedUnitOut {
     const int32_t* num_groups;
     int32_t* unit_group;
     int32_t* unit_t0;
+    int32_t cap;
     __device__ void operator()(int64_t g, int32_t ex, int32_t nunits) const {
         if (g >= *num_groups) return;
         const int32_t s = group_start[g];
         for (int32_t u = 0; u < nunits; ++u) {
             unit_group[ex + u] = (int32_t)g;
-            unit_t0[ex + u] = s + u * kUnit;
+            unit_t0[ex + u] = s + u * cap;
         }
     }
 };
@@ -947,6 +956,7 @@ struct WalkArgs {
     const int32_t* __restrict__ unit_group;
     const int32_t* __restrict__ unit_t0;
     const int32_t* __restrict__ num_units;
+    const int32_t* __restrict__ unit_cap;   // queries per unit
     const int32_t* __restrict__ unit_list;  // emit re-walk: the units to walk
     const int32_t* __restrict__ num_list;
     int32_t* work;
@@ -1236,7 +1246,7 @@ __device__ __forceinline__ void count_unit(const WalkArgs& a, WalkSmem& sm, int3
     const int32_t rshift = u.rshift;
     const float4 nan4 = make_float4(__int_as_float(0x7fc00000), 0.f, 0.f, 0.f);
     const int32_t t0 = a.unit_t0[unit];
-    const int32_t nb = min(32, a.group_start[grp + 1] - t0);
+    const int32_t nb = min(*a.unit_cap, a.group_start[grp + 1] - t0);
     const int32_t gc[3] = {a.group_coords[3 * grp], a.group_coords[3 * grp + 1], a.group_coords[3 * grp + 2]};
     int32_t beg = 0, cnt = 0;
     if (lane < S) stencil_lookup(a, u, gc, lane, beg, cnt);
@@ -1437,7 +1447,7 @@ __device__ __forceinline__ void emit_unit(const WalkArgs& a, EmitSmem& sm, int32
     const unsigned lt = (1u << lane) - 1u;
     const float4 nan4 = make_float4(__int_as_float(0x7fc00000), 0.f, 0.f, 0.f);
     const int32_t t0 = a.unit_t0[unit];
-    const int32_t nb = min(32, a.group_start[grp + 1] - t0);
+    const int32_t nb = min(*a.unit_cap, a.group_start[grp + 1] - t0);
     const int32_t gc[3] = {a.group_coords[3 * grp], a.group_coords[3 * grp + 1], a.group_coords[3 * grp + 2]};
     int32_t beg = 0, cnt = 0;
     if (lane < S) stencil_lookup(a, u, gc, lane, beg, cnt);
@@ -1542,6 +1552,7 @@ struct ExpandArgs {
     const int32_t* __restrict__ stage;
     const int32_t* __restrict__ rec;
     const int32_t* __restrict__ num_units;
+    const int32_t* __restrict__ unit_cap;
     const int32_t* __restrict__ unit_t0;
     const int32_t* __restrict__ unit_group;
     const int32_t* __restrict__ group_start;
@@ -1579,7 +1590,7 @@ __global__ void __launch_bounds__(kExpandWarps * 32) expand_records_kernel(Expan
         const int32_t* r = a.stage + r0;
         const int32_t nchunks = r[0];
         if (nchunks <= 0) continue;  // no candidates, no outputs
-        const int32_t nb = min(32, a.group_start[grp + 1] - t0);
+        const int32_t nb = min(*a.unit_cap, a.group_start[grp + 1] - t0);
         const int32_t nm = nb * nchunks;
         const uint32_t* mk = reinterpret_cast<const uint32_t*>(r + 1);  // [query][chunk]
         const int32_t* cands = r + 1 + nm;                               // [chunk][32]
@@ -1967,6 +1978,7 @@ static WalkArgs make_walk(const HostBatch& b, const Structure& S, const Scratch&
     a.unit_group = W.unit_group;
     a.unit_t0 = W.unit_t0;
     a.num_units = W.num_units;
+    a.unit_cap = W.unit_cap;
     a.unit_list = W.flagged;
     a.num_list = W.num_flagged;
     a.work = W.work;
@@ -2057,10 +2069,12 @@ static cudaError_t launch_walks(const HostBatch& b, WalkArgs a, dim3 grid, dim3 
     return cudaSuccess;
 }
 
+// Persistent walk grid: the blocks loop over units through an atomic counter, so the size only
+// sets the parallelism -- about two units per query group's worth of full units per warp.
 static unsigned walk_blocks(int64_t nq) {
-    const int64_t max_units = (nq + kUnit - 1) / kUnit + 1;
-    return (unsigned)std::max<int64_t>(1, std::min<int64_t>((int64_t)num_sms() * 12, (max_units + kWalkWarps - 1) /
-                                                                                             kWalkWarps));
+    const int64_t max_units = 2 * nq / g_unit_cap + 1;
+    return (unsigned)std::max<int64_t>(1, std::min<int64_t>((int64_t)num_sms() * g_walk_blocks_per_sm,
+                                                            (max_units + kWalkWarps - 1) / kWalkWarps));
 }
 
 template <typename K>
@@ -2139,7 +2153,8 @@ static int count_impl(const HostBatch& b, const Structure& S, const Scratch& W, 
     const int64_t nq = b.nq;
     int rc = upload_table(b, W, st);
     if (rc) return rc;
-    count_init_kernel<<<grid_for(C, 128), 128, 0, st>>>(W, C);
+    const int unit_cap = g_unit_cap;
+    count_init_kernel<<<grid_for(C, 128), 128, 0, st>>>(W, C, unit_cap);
     note_launches(1);
     if (b.any_query_sup && nq > 0) {
         support_stats_kernel<<<grid_for(nq, 256, num_sms() * 8), 256, 0, st>>>(
@@ -2182,8 +2197,8 @@ static int count_impl(const HostBatch& b, const Structure& S, const Scratch& W, 
             gstart = W.qgroup_start;
             ngroups = W.num_qgroups;
         }
-        BoundedUnitCountIn ui{gstart, ngroups};
-        BoundedUnitOut uo{gstart, ngroups, W.unit_group, W.unit_t0};
+        BoundedUnitCountIn ui{gstart, ngroups, unit_cap};
+        BoundedUnitOut uo{gstart, ngroups, W.unit_group, W.unit_t0, unit_cap};
         TCR_CUDA(device_exclusive_scan<int32_t>(ui, uo, nq, W.scan_tiles32, W.num_units, st));
         WalkArgs a = make_walk(b, S, W);
         a.stage = stage;
@@ -2223,6 +2238,7 @@ static int emit_impl(const HostBatch& b, const Structure& S, const Scratch& W, c
         e.stage = stage;
         e.rec = W.rec;
         e.num_units = W.num_units;
+        e.unit_cap = W.unit_cap;
         e.unit_t0 = W.unit_t0;
         e.unit_group = W.unit_group;
         e.group_start = a.group_start;
@@ -2340,6 +2356,16 @@ int tcr_profile_kernel_ms(int32_t kernel, float* ms) {
     if (!g_prof_recorded[kernel]) return set_error(TCR_ERR_INVALID, "no profiled launch of kernel %d", kernel);
     TCR_CUDA(cudaEventSynchronize(g_prof_ev[kernel][1]));
     TCR_CUDA(cudaEventElapsedTime(ms, g_prof_ev[kernel][0], g_prof_ev[kernel][1]));
+    return TCR_OK;
+}
+
+int tcr_set_tuning(int32_t unit_queries, int32_t walk_blocks_per_sm) {
+    if (unit_queries != 0 && unit_queries != 8 && unit_queries != 16 && unit_queries != 32)
+        return set_error(TCR_ERR_INVALID, "unit_queries must be 8, 16 or 32 (0: default 32)");
+    if (walk_blocks_per_sm < 0 || walk_blocks_per_sm > 64)
+        return set_error(TCR_ERR_INVALID, "walk_blocks_per_sm must be in [1, 64] (0: default 12)");
+    g_unit_cap = unit_queries ? unit_queries : 32;
+    g_walk_blocks_per_sm = walk_blocks_per_sm ? walk_blocks_per_sm : 12;
     return TCR_OK;
 }
 
