@@ -399,6 +399,7 @@ def bench_served(dev, seconds=1.0):
 
     import torchcompactradius_b200 as tcr
     from torchcompactradius_b200.serving import Request, Scene, SearchServer
+    from torchcompactradius_b200.tuning import Autotuner
 
     scenes, arrivals = make_served_workload(seconds=seconds)
     dom = tcr.DomainDescription(torch.full((3,), -1.0), torch.full((3,), 1.0), torch.tensor([True] * 3), 3)
@@ -414,6 +415,13 @@ def bench_served(dev, seconds=1.0):
     with srv:
         for k in range(len(scenes)):  # warm-up: one search per scene (first build, caches)
             srv.search(k, timeout=120)
+
+        def all_scenes():  # one request per scene, together: the server's typical batch
+            for r in [srv.submit(Request(k)) for k in range(len(scenes))]:
+                r.wait(120)
+
+        tuner = Autotuner(reps=2)
+        tuned = tuner.tune(all_scenes, key="served")
         srv.batches = srv.batched_requests = 0
         torch.cuda.synchronize()
         reqs = []
@@ -452,7 +460,7 @@ def bench_served(dev, seconds=1.0):
                            "batches": srv.batches, "mean_batch": srv.batched_requests / max(srv.batches, 1)}
 
     # ---- per call -----------------------------------------------------------------------
-    pos = [x.to(dev) for x, h in scenes]
+    pos = [x.to(dev) for x, h in scenes]  # (the same engine tuning as the server)
     sup = [torch.full((x.shape[0],), h, device=dev) for x, h in scenes]
     for k in range(len(scenes)):
         tcr.radiusSearch(tcr.PointCloud(pos[k], sup[k]), mode="gather", domain=dom, algorithm="compact")
@@ -474,6 +482,9 @@ def bench_served(dev, seconds=1.0):
                         f"50 neighbours, gather, COO; Poisson arrivals 2000/s for {seconds:g} s, each request "
                         f"jitters its scene by N(0, (0.05 h)^2); 40 GB admission budget, 2 worker streams",
             "points": int(sum(x.shape[0] for x, h in scenes)),
+            "tuning": {"chosen": {"queries_per_unit": tuned[0], "walk_blocks_per_sm": tuned[1]},
+                       "ms_per_batch_of_all_scenes": {f"{c[0]}q/{c[1]}b": round(v, 3)
+                                                      for c, v in tuner.timings["served"].items()}},
             "served": served, "served_capacity": served_capacity, "per_call": per_call,
             "speedup_vs_per_call": served_capacity["value"] / per_call["value"],
             "p99_ratio_per_call_over_served": per_call["p99_ms"] / served["p99_ms"]}

@@ -928,6 +928,8 @@ struct UnitCtx {
     int32_t qshift, rshift;  // subtracted from global query / reference indices (cloud-local numbering)
     float dmin[3], hcell[3], ext[3];
     float rmax, qmax;        // largest reference / query support (band of the fast test)
+    int32_t shift_ok;        // periodic dims all hold >= 6 cells: candidates across a seam are shifted
+    float shift_delta;       // bound on the error a shift adds to a difference
     int64_t map_base, map_cap;
 };
 
@@ -1000,6 +1002,21 @@ __device__ __forceinline__ void load_unit_ctx(UnitCtx& u, const WalkArgs& a, int
     u.rshift = a.local_index ? cp.ref_base : 0;
     u.rmax = key_float(g.ref_stats.max_key);
     u.qmax = q.qmax;
+    // Points of a stencil cell across the periodic seam can be moved by +-ext while staged, so
+    // the fast test needs no wrap: with >= 6 cells on every periodic dimension no candidate is near
+    // half the extent away, so the reference's moduloOp wraps exactly the shifted cells.  A shift
+    // changes a difference by at most one rounding of the shifted coordinate plus the reference's
+    // own rounding of q - c before its exact wrap: shift_delta bounds both.
+    bool ok = cp.periodic_mask != 0;
+    float delta = 0.0f;
+    for (int d = 0; d < cp.dim; ++d)
+        if ((cp.periodic_mask >> d) & 1) {
+            ok = ok && g.count[d] >= 6;
+            // two roundings of magnitude <= half an ulp of (|coordinate| + ext) each: <= 2^-23 of it
+            delta = fmaxf(delta, (fmaxf(fabsf(cp.dmin[d]), fabsf(cp.dmax[d])) + cp.ext[d]) * 1.1920928955078125e-7f);
+        }
+    u.shift_ok = ok && isfinite(delta);
+    u.shift_delta = delta;
     u.map_base = cp.map_base;
     u.map_cap = cp.map_cap;
 }
@@ -1147,6 +1164,7 @@ struct WalkSmem {
     int32_t beg[kWalkWarps][32];
     float4 q[kWalkWarps][32];
     float4 cand[kWalkWarps][36];                  // the chunk's candidates, stream-major, rows padded
+    float shift[kWalkWarps][3][32];               // per stencil cell: +-ext on dims it lies across a seam
     uint32_t mask[kWalkWarps][32 * kMaskStride];  // [query][chunk] hit masks
     int32_t sj[kWalkWarps][kSegChunks][32];       // output column of candidate (chunk, lane)
     UnitCtx u[kWalkWarps];
@@ -1177,6 +1195,15 @@ __device__ __forceinline__ float query_band(float hq, float rmax) {
     else if (MODE == kSymmetric) t = fmaf(hq, 0.5f, 0.5f * rmax);
     else t = fmaxf(hq, rmax);
     return kBandEps * t * t;
+}
+
+// The largest threshold lane q can meet (query_band is kBandEps times its square).
+template <int MODE>
+__device__ __forceinline__ float query_tmax(float hq, float rmax) {
+    if (MODE == kGather) return hq;
+    if (MODE == kScatter) return rmax;
+    if (MODE == kSymmetric) return fmaf(hq, 0.5f, 0.5f * rmax);
+    return fmaxf(hq, rmax);
 }
 
 // Float test of query q (lane) against candidate c; r < 0 means inside.
@@ -1250,6 +1277,23 @@ __device__ __forceinline__ void count_unit(const WalkArgs& a, WalkSmem& sm, int3
     const int32_t gc[3] = {a.group_coords[3 * grp], a.group_coords[3 * grp + 1], a.group_coords[3 * grp + 2]};
     int32_t beg = 0, cnt = 0;
     if (lane < S) stencil_lookup(a, u, gc, lane, beg, cnt);
+    const bool shift_mode = PERIODIC && u.shift_ok;
+    bool seam = false;  // some stencil cell of the unit lies across a seam
+    if (shift_mode) {  // the stencil cell's seam shift, in stencil_lookup's offset order
+        float sh[3] = {0.f, 0.f, 0.f};
+        int rem = lane;
+#pragma unroll
+        for (int d = DIM - 1; d >= 0; --d) {
+            const int32_t v = gc[d] + rem % 3 - 1;
+            rem /= 3;
+            if (lane < S && ((u.periodic_mask >> d) & 1))
+                sh[d] = v < 0 ? -u.ext[d] : (v >= u.count[d] ? u.ext[d] : 0.f);
+        }
+        sm.shift[w][0][lane] = sh[0];
+        sm.shift[w][1][lane] = sh[1];
+        sm.shift[w][2][lane] = sh[2];
+        seam = __any_sync(0xffffffffu, sh[0] != 0.f || sh[1] != 0.f || sh[2] != 0.f);
+    }
     const int32_t inc = warp_inclusive_scan(cnt);
     sm.pre[w][lane + 1] = inc;
     if (lane == 0) sm.pre[w][0] = 0;
@@ -1284,6 +1328,13 @@ __device__ __forceinline__ void count_unit(const WalkArgs& a, WalkSmem& sm, int3
     const float4 myq = sm.q[w][lq];
     const float qs = query_share<MODE>(myq.w);
     const float band = exact_all ? __int_as_float(0x7f800000) : query_band<MODE>(myq.w, rmax);
+    // a unit with shifted candidates: the band also covers the shift's rounding (|d2 error| <= 2 T
+    // delta + delta^2); units away from the seams keep the tight band
+    float band_s = band;
+    if (seam) {
+        const float t = query_tmax<MODE>(myq.w, rmax), dl = u.shift_delta;
+        band_s = band + fmaf(2.0f * t, dl, dl * dl);
+    }
     const float4* my_cand = &sm.cand[w][ls * (Q + 1)];
     // Lane k of chunk c holds candidate 32c + k.  Its stencil cell r only moves forward from
     // chunk to chunk, so it is tracked incrementally instead of searched.
@@ -1293,13 +1344,23 @@ __device__ __forceinline__ void count_unit(const WalkArgs& a, WalkSmem& sm, int3
     const float4* __restrict__ rs = a.rsorted;
     const int32_t* __restrict__ ri = a.rsidx;
     const int32_t* __restrict__ rid = a.ref_ids;
-    auto fetch = [&cr, pre, begs, rs, ri, rid, rshift, M, nan4](int32_t k, float4& v, int32_t& jo) {
+    const float* shx = sm.shift[w][0];
+    const float* shy = sm.shift[w][1];
+    const float* shz = sm.shift[w][2];
+    bool shifting = false;  // the fast pass stages shifted candidates, the exact pass the originals
+    auto fetch = [&cr, &shifting, pre, begs, rs, ri, rid, rshift, M, nan4, shx, shy, shz](int32_t k, float4& v,
+                                                                                         int32_t& jo) {
         v = nan4;
         jo = 0;
         if (k < M) {
             while (pre[cr + 1] <= k) ++cr;
             const int32_t j = begs[cr] + (k - pre[cr]);
             v = __ldg(&rs[j]);
+            if (PERIODIC && shifting) {
+                v.x += shx[cr];
+                if (DIM > 1) v.y += shy[cr];
+                if (DIM > 2) v.z += shz[cr];
+            }
             jo = __ldg(&ri[j]);
             jo = rid ? __ldg(&rid[jo]) : jo - rshift;
         }
@@ -1309,6 +1370,7 @@ __device__ __forceinline__ void count_unit(const WalkArgs& a, WalkSmem& sm, int3
     bool unc = false;
     for (int pass = 0; pass < 2; ++pass) {
         const bool exact = pass == 1;
+        shifting = shift_mode && !exact;
         cr = 0;
         qcount = 0;
         float4 nxt;
@@ -1324,6 +1386,10 @@ __device__ __forceinline__ void count_unit(const WalkArgs& a, WalkSmem& sm, int3
             if (exact) {
                 m = stream_mask_exact<DIM, PERIODIC, MODE>(unit_exact_ctx(u, MODE), my_cand, Q, myq, qs, band)
                     << (Q == 32 ? 0 : Q * ls);
+            } else if (shift_mode) {  // shifted candidates: the non-periodic test
+                if (Q == 32) m = stream_mask<DIM, false, MODE, 32>(wc, my_cand, myq, qs, band_s, unc);
+                else if (Q == 16) m = stream_mask<DIM, false, MODE, 16>(wc, my_cand, myq, qs, band_s, unc) << (16 * ls);
+                else m = stream_mask<DIM, false, MODE, 8>(wc, my_cand, myq, qs, band_s, unc) << (8 * ls);
             } else if (Q == 32) {
                 m = stream_mask<DIM, PERIODIC, MODE, 32>(wc, my_cand, myq, qs, band, unc);
             } else if (Q == 16) {
