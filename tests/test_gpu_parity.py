@@ -233,3 +233,38 @@ def test_multilevel_wide_support_and_tiny_periodic_box():
     for mode in cases.MODES:
         _mlm_vs_brute_force(x, h, None, None, np.zeros(2, np.float32), np.ones(2, np.float32),
                             np.array([True, True]), mode)
+
+
+def _ref_periodic_distance(a, b, ext):
+    """The reference's float/double distance (common.h:106-129) with every dimension periodic."""
+    s = np.float32(0.0)
+    for d in range(a.shape[-1]):
+        pq = np.float32(a[..., d] - b[..., d]).astype(np.float64)
+        h = np.float64(np.float32(ext[d]))
+        t = pq + h / 2.0
+        diff = (t - np.floor(t / h) * h) - h / 2.0
+        s = np.float32(np.float64(s) + diff * diff)
+    return np.sqrt(np.float32(s))
+
+
+def test_pairs_across_periodic_seams_at_the_threshold():
+    # clouds whose periodic dimensions hold >= 6 cells take the shifted-candidate walk: pairs across
+    # the seam whose support equals their reference distance (or its float successor) must be
+    # decided exactly as the reference decides them
+    rng = np.random.default_rng(23)
+    n = 20000
+    x = (rng.random((n, 3)) * 2 - 1).astype(np.float32)
+    h = np.full(n, 0.06, np.float32)
+    lo_x = np.nonzero(x[:, 0] < -0.96)[0]
+    hi_x = np.nonzero(x[:, 0] > 0.96)[0]
+    k = min(len(lo_x), len(hi_x), 400)
+    i, j = lo_x[:k], hi_x[:k]
+    x[j, 1:] = (x[i, 1:] + (rng.random((k, 2)) * 0.04 - 0.02)).astype(np.float32)  # neighbours across x
+    ext = np.array([2, 2, 2], np.float32)
+    d = _ref_periodic_distance(x[i], x[j], ext)
+    hi = np.clip(d, 0.01, 0.09).astype(np.float32)
+    hi[::2] = np.nextafter(hi[::2], np.float32(1))
+    h[i] = hi
+    for mode in ("gather", "symmetric", "superSymmetric"):
+        _check_vs_oracle(x, h, None, None, np.array([-1] * 3, np.float32), np.array([1] * 3, np.float32),
+                         np.array([True, True, True]), mode)
