@@ -558,6 +558,69 @@ def bench_graphs(dev, flush, steps=200):
                     "value": pairs / (statistics.mean(ms) / 1e3), "unit": "pairs/s"}}
 
 
+def make_adaptive_workload(seed=6, n=1 << 22, k_target=32.0):
+    """Adaptive resolution: 2^22 points, 70% from 8 Gaussian blobs (sigma 0.1, centres
+    U[-0.8, 0.8]^3) and 30% uniform in [-1, 1]^3; x periodic (wrapped), y and z clamped; supports
+    h_i = cbrt(3 K / (4 pi rho(x_i))) from the mixture's own density, clamped to [h_max/4, h_max]
+    with h_max the background's (K = 32 gives about 40 neighbours per point)."""
+    import numpy as np
+    import torch
+    g = torch.Generator().manual_seed(seed)
+    nb = int(0.7 * n)
+    centres = torch.rand(8, 3, generator=g) * 1.6 - 0.8
+    pick = torch.randint(0, 8, (nb,), generator=g)
+    x = torch.cat([centres[pick] + 0.1 * torch.randn(nb, 3, generator=g), torch.rand(n - nb, 3, generator=g) * 2 - 1])
+    x[:, 0] = torch.remainder(x[:, 0] + 1.0, 2.0) - 1.0
+    x[:, 1:] = x[:, 1:].clamp(-1.0, 0.999999)
+    sigma = 0.1
+    rho = torch.full((n,), 0.3 * n / 8.0)
+    norm = 0.7 * n / 8.0 / (2 * np.pi * sigma * sigma) ** 1.5
+    for c in centres:
+        d = x - c
+        d[:, 0] = torch.remainder(d[:, 0] + 1.0, 2.0) - 1.0  # periodic in x
+        rho += norm * torch.exp(-(d * d).sum(1) / (2 * sigma * sigma))
+    h = (3 * k_target / (4 * np.pi * rho)) ** (1.0 / 3.0)
+    hmax = float((3 * k_target / (4 * np.pi * 0.3 * n / 8.0)) ** (1.0 / 3.0))
+    h = h.clamp(hmax / 4, hmax)
+    return x.contiguous(), h.to(torch.float32).contiguous()
+
+
+def bench_adaptive(dev, flush, steps=3):
+    """The adaptive workload in scatter mode, COO: single-level compact cells (sized for the
+    largest support) against the exact multi-level search, same pair set checked."""
+    import torch
+
+    import torchcompactradius_b200 as tcr
+    x, h = make_adaptive_workload()
+    x, h = x.to(dev), h.to(dev)
+    dom = tcr.DomainDescription(torch.full((3,), -1.0), torch.full((3,), 1.0), torch.tensor([True, False, False]), 3)
+    stream = torch.cuda.current_stream(dev)
+    res = {}
+    keys = {}
+    for algo in ("mlm", "compact"):
+        adj = tcr.radiusSearch(tcr.PointCloud(x, h), mode="scatter", domain=dom, algorithm=algo, format="coo")
+        ms = []
+        for k in range(steps):
+            flush.fill_(k & 0xff)
+            s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            s.record(stream)
+            adj = tcr.radiusSearch(tcr.PointCloud(x, h), mode="scatter", domain=dom, algorithm=algo, format="coo")
+            e.record(stream)
+            e.synchronize()
+            ms.append(s.elapsed_time(e))
+        pairs = int(adj.row.numel())
+        keys[algo] = torch.sort(adj.row * x.shape[0] + adj.col)[0]
+        del adj
+        res[algo] = {"ms_per_search": statistics.mean(ms), "value": pairs / (statistics.mean(ms) / 1e3),
+                     "unit": "pairs/s", "pairs": pairs}
+    same = bool(torch.equal(keys["mlm"], keys["compact"]))
+    del keys
+    return {"workload": "2^22 points, 70% in 8 Gaussian blobs (sigma 0.1) + 30% uniform, periodic in x, supports "
+                        "from the mixture density (ratio up to 4), scatter, COO (seed 6)",
+            "mlm": res["mlm"], "compact": res["compact"], "same_pair_set": same,
+            "speedup_mlm_vs_compact": res["compact"]["ms_per_search"] / res["mlm"]["ms_per_search"]}
+
+
 def cpu_baseline_batched(clouds, budget_s=12.0):
     """The reference's own CPU search, one call per cloud (its batched radius() fails), over the
     first clouds of the workload until about budget_s seconds have passed."""
@@ -773,6 +836,7 @@ def run_b200(args):
                                         rank == 0 and not args.no_cpu_baseline)
         set_tuning(0, 0)  # the other forms run with the defaults
         line["graphs"] = bench_graphs(dev, flush)
+        line["adaptive"] = bench_adaptive(dev, flush)
         del flush
         line["served"] = bench_served(dev)
     if world > 1:

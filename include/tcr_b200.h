@@ -20,7 +20,7 @@
 extern "C" {
 #endif
 
-#define TCR_ABI_VERSION 6
+#define TCR_ABI_VERSION 7
 
 #define TCR_OK 0
 #define TCR_ERR_INVALID (-1) /* bad argument or workspace too small */
@@ -76,6 +76,9 @@ typedef struct tcr_cloud_desc {
     const float* query_sup;  /* device [n_query] or NULL (TCR_SCATTER) */
     const float* ref_pos;    /* device [n_ref*dim] */
     const float* ref_sup;    /* device [n_ref] or NULL (TCR_GATHER) */
+    float hcell[3];          /* > 0: caller-chosen cell sizes (as tcr_search_desc.hcell) */
+    int32_t clamped_grid;    /* 1: exact grid semantics for caller-chosen cells (as tcr_search_desc) */
+    int32_t reserved;
 } tcr_cloud_desc;
 
 /* A batch of independent searches run by one set of launches (the many scenes or timesteps of a

@@ -55,6 +55,9 @@ class CloudDesc(ctypes.Structure):
         ("query_sup", ctypes.c_void_p),
         ("ref_pos", ctypes.c_void_p),
         ("ref_sup", ctypes.c_void_p),
+        ("hcell", ctypes.c_float * 3),
+        ("clamped_grid", ctypes.c_int32),
+        ("reserved", ctypes.c_int32),
     ]
 
 

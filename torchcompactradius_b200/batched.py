@@ -25,7 +25,8 @@ from .util import DomainDescription, PointCloud, SparseCOO, SparseCSR
 CLOUD_DTYPE = np.dtype([("dim", "<i4"), ("periodic_mask", "<i4"), ("domain_min", "<f4", (3,)),
                         ("domain_max", "<f4", (3,)), ("hash_map_length", "<i8"), ("n_query", "<i8"),
                         ("n_ref", "<i8"), ("query_pos", "<u8"), ("query_sup", "<u8"), ("ref_pos", "<u8"),
-                        ("ref_sup", "<u8")], align=True)
+                        ("ref_sup", "<u8"), ("hcell", "<f4", (3,)), ("clamped_grid", "<i4"), ("reserved", "<i4")],
+                       align=True)
 
 # Pairs and staging words per query of the previous batch: they size the next one's buffers.
 _pairs_per_query = [64.0]

@@ -23,6 +23,7 @@
 #include <cstddef>
 #include <algorithm>
 #include <mutex>
+#include <type_traits>
 #include <vector>
 
 #include "tcr_common.cuh"
@@ -64,8 +65,9 @@ static inline int64_t hash_capacity(int64_t n_ref, int64_t min_cap) {
 constexpr int64_t kSingleMapMin = 1024;  // one search
 constexpr int64_t kBatchMapMin = 64;     // per cloud of a batch
 // Work counters: [0] count walk, [1] emit walk, [2 + cls] / [8 + cls] the count / emit walk of
-// one cloud class (cls = dim * 2 + periodic, 2..7) in a batch that mixes classes.
-constexpr int kWorkCounters = 16;
+// one cloud class (cls = dim * 2 + periodic, 2..7) in a batch that mixes classes, [16 + the same]
+// for the count walk of the units recorded window by window.
+constexpr int kWorkCounters = 32;
 
 // Run-time tuning (tcr_set_tuning): queries per work unit -- 32, 16 or 8, i.e. 1, 2 or 4 lanes of
 // the walk per query -- and resident walk blocks per SM.  Neither changes a result: a query's
@@ -136,6 +138,7 @@ struct Scratch {
     int32_t* exact_clouds;  // [1] clouds whose every pair takes the exact test
     int32_t* num_exact;     // [1] units the count walk re-tested with exact decisions
     int32_t* unit_cap;      // [1] queries per work unit of this search (set by the count phase)
+    int32_t* num_big;       // [1] units recorded window by window
     unsigned long long* cursor;  // [1] staging fill
     float4* pack;           // [max(nq,nr)] packed input points before sorting
     void* keys[2];          // [max(nq,nr)] 64-bit slots (32-bit keys use the first half)
@@ -155,6 +158,7 @@ struct Scratch {
     int32_t* stray;         // [nq]
     int32_t* rec;           // [nq] per unit: offset of its record in the staging list (-1: not staged)
     int32_t* flagged;       // [nq] units re-walked by the emit pass
+    int32_t* big;           // [nq] units of more than one record window
     // incremental re-sort (builds given the previous cell of every reference point), else null
     int32_t* stay;          // [nr] 1: the point is still in its previous cell
     void* stay_keys;        // [nr] keys of the unmoved points, input order (sorted when the hint holds)
@@ -184,6 +188,7 @@ static Scratch carve_scratch(void* buf, int64_t nq, int64_t nr, int64_t C, bool 
     s.exact_clouds = c.take<int32_t>(1);
     s.num_exact = c.take<int32_t>(1);
     s.unit_cap = c.take<int32_t>(1);
+    s.num_big = c.take<int32_t>(1);
     s.cursor = c.take<unsigned long long>(1);
     s.pack = c.take<float4>(nmax);
     s.keys[0] = c.take<unsigned long long>(nmax);
@@ -206,6 +211,7 @@ static Scratch carve_scratch(void* buf, int64_t nq, int64_t nr, int64_t C, bool 
     s.stray = c.take<int32_t>(q);
     s.rec = c.take<int32_t>(q);
     s.flagged = c.take<int32_t>(q);
+    s.big = c.take<int32_t>(q);
     const int64_t ni = incremental ? std::max<int64_t>(nr, 1) : 0;
     s.stay = incremental ? c.take<int32_t>(ni) : nullptr;
     s.stay_keys = incremental ? c.take<unsigned long long>(ni) : nullptr;
@@ -474,6 +480,7 @@ __global__ void count_init_kernel(Scratch W, int C, int unit_cap) {
         *W.exact_clouds = 0;
         *W.num_exact = 0;
         *W.unit_cap = unit_cap;
+        *W.num_big = 0;
         *W.cursor = 0ull;
     }
 }
@@ -969,6 +976,8 @@ struct WalkArgs {
     int32_t* flagged;             // [units] units to re-walk in the emit pass
     int32_t* num_flagged;
     int32_t* num_exact;           // units re-tested with exact decisions
+    int32_t* big;                 // units of more than kSegChunks chunks (for the windowed count walk)
+    int32_t* num_big;
     unsigned long long* cursor;   // staging list fill
     int32_t* stage;               // staging list
     int64_t stage_cap;
@@ -1165,6 +1174,8 @@ struct WalkSmem {
     float4 q[kWalkWarps][32];
     float4 cand[kWalkWarps][36];                  // the chunk's candidates, stream-major, rows padded
     float shift[kWalkWarps][3][32];               // per stencil cell: +-ext on dims it lies across a seam
+    int32_t qbefore[kWalkWarps][32];              // per query: hits before the current record window
+    int32_t* rec_ptr[kWalkWarps];                 // the unit's record (null: not staged)
     uint32_t mask[kWalkWarps][32 * kMaskStride];  // [query][chunk] hit masks
     int32_t sj[kWalkWarps][kSegChunks][32];       // output column of candidate (chunk, lane)
     UnitCtx u[kWalkWarps];
@@ -1256,13 +1267,29 @@ __device__ __noinline__ uint32_t stream_mask_exact(ExactCtx xc, const float4* ca
     return m;
 }
 
+// Writes the record window that ends with chunk c (its masks and candidate columns are in shared
+// memory): the queries' hits before the window, the masks, the columns.  Out of line: it runs once
+// per window and keeps its registers out of the candidate loop.
+__device__ __noinline__ void flush_window(WalkSmem& sm, int w, int lane, int32_t nb, int32_t c, int32_t qcount) {
+    const int32_t win = c / kSegChunks, nc = c - win * kSegChunks + 1;
+    int32_t* r = sm.rec_ptr[w] + 1 + (int64_t)win * (nb + (nb + 32) * kSegChunks);
+    if (lane < nb) r[lane] = sm.qbefore[w][lane];
+    for (int q = 0; q < nb; ++q)
+        if (lane < nc) r[nb + q * nc + lane] = sm.mask[w][q * kMaskStride + lane];
+    int32_t* rj = r + nb + nb * nc;
+    for (int32_t k = 0; k < nc; ++k) rj[k * 32 + lane] = sm.sj[w][k][lane];
+    __syncwarp();
+    sm.qbefore[w][lane] = qcount;
+    __syncwarp();
+}
+
 // Count walk of one unit: test every (query, candidate) once; count, stage the hits of small units.
 //
 // Each chunk's 32 candidates are staged in shared memory; lane (q, s) holds query q and tests it
 // against the Q candidates of stream s (Q = 8, 16 or 32 as the unit has <= 8, <= 16 or <= 32
 // queries, so 32/Q streams keep every lane busy).  Hits become bits of a per-lane mask, merged
 // across streams with shuffles into the 32-bit (query, chunk) mask.
-template <int DIM, bool PERIODIC, int MODE>
+template <int DIM, bool PERIODIC, int MODE, bool WIN>
 __device__ __forceinline__ void count_unit(const WalkArgs& a, WalkSmem& sm, int32_t unit, int32_t grp, int lane,
                                            int w) {
     constexpr int S = DIM == 1 ? 3 : (DIM == 2 ? 9 : 27);
@@ -1299,6 +1326,10 @@ __device__ __forceinline__ void count_unit(const WalkArgs& a, WalkSmem& sm, int3
     if (lane == 0) sm.pre[w][0] = 0;
     sm.beg[w][lane] = beg;
     const int32_t M = __shfl_sync(0xffffffffu, inc, 31);
+    if (!WIN && ((M + 31) >> 5) > kSegChunks) {  // more than one record window: the windowed launch
+        if (lane == 0) a.big[atomicAdd(a.num_big, 1)] = unit;
+        return;
+    }
     bool active = false;
     int32_t qorig = 0;
     float4 qv = nan4;
@@ -1318,9 +1349,24 @@ __device__ __forceinline__ void count_unit(const WalkArgs& a, WalkSmem& sm, int3
             qv = nan4;
         }
     }
-    sm.q[w][lane] = qv;  // rows >= nb hold NaN queries and never hit
     const int32_t nchunks = (M + 31) >> 5;
-    const bool stage = a.stage_cap > 0 && nchunks <= kSegChunks;
+    sm.q[w][lane] = qv;  // rows >= nb hold NaN queries and never hit
+    // The unit's record, reserved up front: [nchunks] then one window per kSegChunks chunks,
+    // [hits of each query before the window: nb][masks: nb x nc, query-major][candidates: nc x 32]
+    const int32_t nwin = (nchunks + kSegChunks - 1) / kSegChunks;
+    const int64_t words = 1 + (int64_t)nwin * nb + (int64_t)(nb + 32) * nchunks;
+    bool stage = false;
+    if (a.stage_cap > 0) {
+        unsigned long long base = 0;
+        if (lane == 0) base = atomicAdd(a.cursor, (unsigned long long)words);
+        base = __shfl_sync(0xffffffffu, base, 0);
+        stage = base + (unsigned long long)words <= (unsigned long long)a.stage_cap;
+        if (stage && lane == 0) {
+            a.stage[base] = nchunks;
+            a.rec[unit] = (int32_t)base;
+            sm.rec_ptr[w] = a.stage + base;
+        }
+    }
     const int Q = nb <= 8 ? 8 : (nb <= 16 ? 16 : 32);
     const int lq = lane & (Q - 1);      // this lane's query
     const int ls = lane / Q;            // this lane's stream
@@ -1365,7 +1411,9 @@ __device__ __forceinline__ void count_unit(const WalkArgs& a, WalkSmem& sm, int3
             jo = rid ? __ldg(&rid[jo]) : jo - rshift;
         }
     };
-    // the unit's chunk loop; `exact` redoes it deciding in-band pairs with the reference test
+    // the unit's chunk loop; `exact` redoes it deciding in-band pairs with the reference test.  A
+    // unit of more than kSegChunks chunks (the windowed launch, WIN) writes its record window by
+    // window; the others keep every mask in shared memory and write their one window after the loop.
     int32_t qcount = 0;
     bool unc = false;
     for (int pass = 0; pass < 2; ++pass) {
@@ -1373,13 +1421,15 @@ __device__ __forceinline__ void count_unit(const WalkArgs& a, WalkSmem& sm, int3
         shifting = shift_mode && !exact;
         cr = 0;
         qcount = 0;
+        if (WIN) sm.qbefore[w][lane] = 0;  // this query's hits before the current window
         float4 nxt;
         int32_t nxt_j;
         fetch(lane, nxt, nxt_j);
         for (int32_t c = 0; c < nchunks; ++c) {
+            const int32_t cw = WIN ? c % kSegChunks : c;
             // stage candidate `lane` of this chunk: stream lane / Q, slot lane % Q
             sm.cand[w][(lane / Q) * (Q + 1) + (lane & (Q - 1))] = nxt;
-            if (stage) sm.sj[w][c][lane] = nxt_j;
+            if (stage) sm.sj[w][cw][lane] = nxt_j;
             fetch(((c + 1) << 5) + lane, nxt, nxt_j);  // prefetch the next chunk's candidate
             __syncwarp();
             uint32_t m;
@@ -1401,36 +1451,25 @@ __device__ __forceinline__ void count_unit(const WalkArgs& a, WalkSmem& sm, int3
             if (Q == 8) m |= __shfl_xor_sync(0xffffffffu, m, 8);
             if (lane < nb) {
                 qcount += __popc(m);
-                if (stage) sm.mask[w][lane * kMaskStride + c] = m;
+                if (stage) sm.mask[w][lane * kMaskStride + cw] = m;
             }
             __syncwarp();
+            if (WIN && stage && (cw == kSegChunks - 1 || c == nchunks - 1))  // the window is complete
+                flush_window(sm, w, lane, nb, c, qcount);
         }
         if (exact || !__any_sync(0xffffffffu, unc)) break;
         if (lane == 0) atomicAdd(a.num_exact, 1);  // the unit is walked again with exact decisions
     }
-    if (active) a.counts[qorig] = qcount;
-    bool staged = false;
-    if (stage) {
-        // record: [nchunks] [masks: nb x nchunks, query-major] [candidates: nchunks x 32]
-        const int64_t words = 1 + (int64_t)nb * nchunks + 32 * (int64_t)nchunks;
-        unsigned long long base = 0;
-        if (lane == 0) base = atomicAdd(a.cursor, (unsigned long long)words);
-        base = __shfl_sync(0xffffffffu, base, 0);
-        staged = base + (unsigned long long)words <= (unsigned long long)a.stage_cap;
-        if (staged) {
-            int32_t* r = a.stage + base;
-            if (lane == 0) {
-                r[0] = nchunks;
-                a.rec[unit] = (int32_t)base;
-            }
-            __syncwarp();
-            for (int q = 0; q < nb; ++q)
-                if (lane < nchunks) r[1 + q * nchunks + lane] = sm.mask[w][q * kMaskStride + lane];
-            int32_t* rj = r + 1 + nb * nchunks;
-            for (int32_t c = 0; c < nchunks; ++c) rj[c * 32 + lane] = sm.sj[w][c][lane];
-        }
+    if (!WIN && stage && nchunks > 0) {  // the one window: [nchunks][zeros: nb][masks][candidates]
+        int32_t* r = sm.rec_ptr[w] + 1;
+        if (lane < nb) r[lane] = 0;
+        for (int q = 0; q < nb; ++q)
+            if (lane < nchunks) r[nb + q * nchunks + lane] = sm.mask[w][q * kMaskStride + lane];
+        int32_t* rj = r + nb + nb * nchunks;
+        for (int32_t c = 0; c < nchunks; ++c) rj[c * 32 + lane] = sm.sj[w][c][lane];
     }
-    if (!staged && lane == 0) {
+    if (active) a.counts[qorig] = qcount;
+    if (!stage && lane == 0) {
         a.rec[unit] = -1;
         int32_t f = atomicAdd(a.num_flagged, 1);
         a.flagged[f] = unit;
@@ -1461,21 +1500,23 @@ __device__ __forceinline__ uint32_t next_units(const WalkArgs& a, int32_t* count
     return __ballot_sync(0xffffffffu, mine);  // bit k: unit base + k belongs to this launch
 }
 
-template <int DIM, bool PERIODIC, int MODE>
+// WIN = false: every unit that fits one record window (the others go to the big-unit list);
+// WIN = true: the big-unit list, recorded window by window.
+template <int DIM, bool PERIODIC, int MODE, bool WIN>
 __global__ void __launch_bounds__(kWalkWarps * 32, PERIODIC ? kWalkMinBlocksPeriodic : kWalkMinBlocks)
     walk_count_kernel(WalkArgs a) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     WalkSmem& sm = *reinterpret_cast<WalkSmem*>(smem_raw);
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-    const int32_t nunits = *a.num_units;
-    int32_t* counter = a.class_filter >= 0 ? &a.work[2 + a.class_filter] : &a.work[0];
+    const int32_t nunits = WIN ? *a.num_big : *a.num_units;
+    int32_t* counter = &a.work[(WIN ? 16 : 0) + (a.class_filter >= 0 ? 2 + a.class_filter : 0)];
     int cur = -1;
     for (;;) {
         int32_t base;
-        uint32_t todo = next_units(a, counter, nullptr, nunits, lane, base);
+        uint32_t todo = next_units(a, counter, WIN ? a.big : nullptr, nunits, lane, base);
         if (base >= nunits) break;
         while (todo) {
-            const int32_t unit = base + (__ffs(todo) - 1);
+            const int32_t unit = WIN ? a.big[base + (__ffs(todo) - 1)] : base + (__ffs(todo) - 1);
             todo &= todo - 1;
             const int32_t grp = a.unit_group[unit];
             const int cloud = a.num_clouds == 1 ? 0 : a.group_cloud[grp];
@@ -1489,7 +1530,7 @@ __global__ void __launch_bounds__(kWalkWarps * 32, PERIODIC ? kWalkMinBlocksPeri
                 if (lane == 0) a.rec[unit] = -1;
                 continue;
             }
-            count_unit<DIM, PERIODIC, MODE>(a, sm, unit, grp, lane, w);
+            count_unit<DIM, PERIODIC, MODE, WIN>(a, sm, unit, grp, lane, w);
         }
     }
 }
@@ -1610,7 +1651,8 @@ constexpr int kExpandTab = 2048;
 struct ExpandSmem {
     uint16_t tab[kExpandWarps][kExpandTab];        // (query << 10) | (chunk << 5) | bit, in output order
     int32_t qpre[kExpandWarps][33];                // exclusive output prefix over queries
-    int64_t qoff[kExpandWarps][32];
+    int64_t qoff[kExpandWarps][32];                // output position of each query's first hit of the window
+    int64_t qbase[kExpandWarps][32];               // the query's row start
     int32_t qrow[kExpandWarps][32];
 };
 
@@ -1634,7 +1676,7 @@ struct ExpandArgs {
     int64_t out_cap;
 };
 
-__global__ void __launch_bounds__(kExpandWarps * 32) expand_records_kernel(ExpandArgs a) {
+__global__ void __launch_bounds__(kExpandWarps * 32, 5) expand_records_kernel(ExpandArgs a) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     ExpandSmem& sm = *reinterpret_cast<ExpandSmem*>(smem_raw);
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
@@ -1653,85 +1695,95 @@ __global__ void __launch_bounds__(kExpandWarps * 32) expand_records_kernel(Expan
             gn = a.unit_group[u + warps];
         }
         if (r0 < 0) continue;  // re-tested by the emit walk
-        const int32_t* r = a.stage + r0;
-        const int32_t nchunks = r[0];
-        if (nchunks <= 0) continue;  // no candidates, no outputs
+        const int32_t nchunks_all = a.stage[r0];
+        if (nchunks_all <= 0) continue;  // no candidates, no outputs
         const int32_t nb = min(*a.unit_cap, a.group_start[grp + 1] - t0);
-        const int32_t nm = nb * nchunks;
-        const uint32_t* mk = reinterpret_cast<const uint32_t*>(r + 1);  // [query][chunk]
-        const int32_t* cands = r + 1 + nm;                               // [chunk][32]
-        int32_t total = 0;
         if (lane < nb) {
             const int32_t row = a.qsidx[t0 + lane];
             int32_t qrow = row;
             if (a.query_ids) qrow = a.query_ids[row];
             else if (a.local_index) qrow -= a.table[a.num_clouds == 1 ? 0 : a.group_cloud[grp]].query_base;
             sm.qrow[w][lane] = qrow;
-            sm.qoff[w][lane] = a.offsets[row];
-            for (int c = 0; c < nchunks; ++c) total += __popc(mk[lane * nchunks + c]);
+            sm.qbase[w][lane] = a.offsets[row];
         }
-        const int32_t qinc = warp_inclusive_scan(total);
-        sm.qpre[w][lane + 1] = qinc;
-        if (lane == 0) sm.qpre[w][0] = 0;
-        const int32_t n = __shfl_sync(0xffffffffu, qinc, 31);
-        if (n <= kExpandTab) {
-            // lanes over (query, chunk) pairs in output order; each expands its few hit bits
-            int32_t carry = 0;
-            int pq = 0, pc = lane;  // pair (query, chunk) of p = base + lane, advanced without division
-            while (pc >= nchunks) { pc -= nchunks; ++pq; }
-            for (int32_t base = 0; base < nm; base += 32) {
-                const int32_t p = base + lane;
-                uint32_t m = p < nm ? mk[p] : 0u;
-                const int32_t cnt = __popc(m);
-                const int32_t inc = warp_inclusive_scan(cnt);
-                int32_t k = carry + inc - cnt;
-                carry += __shfl_sync(0xffffffffu, inc, 31);
-                const int32_t tag = (pq << 10) | (pc << 5);
-                while (m) {
-                    const int bit = __ffs(m) - 1;
-                    m &= m - 1;
-                    tab[k++] = (uint16_t)(tag | bit);
-                }
-                pc += 32;
+        // one window of at most kSegChunks chunks at a time; a window's hits of a query follow the
+        // query's hits of the earlier windows
+        for (int32_t c0 = 0; c0 < nchunks_all; c0 += kSegChunks) {
+            const int32_t win = c0 / kSegChunks;
+            const int32_t nchunks = min(kSegChunks, nchunks_all - c0);
+            const int32_t* r = a.stage + r0 + 1 + (int64_t)win * (nb + (nb + 32) * kSegChunks);
+            const int32_t nm = nb * nchunks;
+            const uint32_t* mk = reinterpret_cast<const uint32_t*>(r + nb);  // [query][chunk]
+            const int32_t* cands = r + nb + nm;                              // [chunk][32]
+            int32_t total = 0;
+            __syncwarp();
+            if (lane < nb) {
+                sm.qoff[w][lane] = sm.qbase[w][lane] + r[lane];
+                for (int c = 0; c < nchunks; ++c) total += __popc(mk[lane * nchunks + c]);
+            }
+            const int32_t qinc = warp_inclusive_scan(total);
+            sm.qpre[w][lane + 1] = qinc;
+            if (lane == 0) sm.qpre[w][0] = 0;
+            const int32_t n = __shfl_sync(0xffffffffu, qinc, 31);
+            if (n <= kExpandTab) {
+                // lanes over (query, chunk) pairs in output order; each expands its few hit bits
+                int32_t carry = 0;
+                int pq = 0, pc = lane;  // pair (query, chunk) of p = base + lane, advanced without division
                 while (pc >= nchunks) { pc -= nchunks; ++pq; }
-            }
-            __syncwarp();
+                for (int32_t base = 0; base < nm; base += 32) {
+                    const int32_t p = base + lane;
+                    uint32_t m = p < nm ? mk[p] : 0u;
+                    const int32_t cnt = __popc(m);
+                    const int32_t inc = warp_inclusive_scan(cnt);
+                    int32_t k = carry + inc - cnt;
+                    carry += __shfl_sync(0xffffffffu, inc, 31);
+                    const int32_t tag = (pq << 10) | (pc << 5);
+                    while (m) {
+                        const int bit = __ffs(m) - 1;
+                        m &= m - 1;
+                        tab[k++] = (uint16_t)(tag | bit);
+                    }
+                    pc += 32;
+                    while (pc >= nchunks) { pc -= nchunks; ++pq; }
+                }
+                __syncwarp();
 #pragma unroll 4
-            for (int32_t o = lane; o < n; o += 32) {
-                const int32_t v = tab[o];
-                const int q = v >> 10;
-                const int64_t pos = sm.qoff[w][q] + (o - sm.qpre[w][q]);
-                if (pos < a.out_cap) {
-                    a.col_out[pos] = (int64_t)cands[v & 0x3ff];
-                    if (a.row_out) a.row_out[pos] = (int64_t)sm.qrow[w][q];
+                for (int32_t o = lane; o < n; o += 32) {
+                    const int32_t v = tab[o];
+                    const int q = v >> 10;
+                    const int64_t pos = sm.qoff[w][q] + (o - sm.qpre[w][q]);
+                    if (pos < a.out_cap) {
+                        a.col_out[pos] = (int64_t)cands[v & 0x3ff];
+                        if (a.row_out) a.row_out[pos] = (int64_t)sm.qrow[w][q];
+                    }
+                }
+            } else {
+                __syncwarp();
+                for (int32_t o = lane; o < n; o += 32) {
+                    int lo = 0, hi = nb;  // query: qpre[lo] <= o < qpre[hi]
+                    while (hi - lo > 1) {
+                        const int mid = (lo + hi) >> 1;
+                        if (sm.qpre[w][mid] <= o) lo = mid; else hi = mid;
+                    }
+                    const int q = lo;
+                    int32_t tq = o - sm.qpre[w][q];
+                    int c = 0;  // chunk holding the query's tq-th hit (tq < hits of q, so c < nchunks)
+                    for (; c < nchunks; ++c) {
+                        const int32_t pcnt = __popc(mk[q * nchunks + c]);
+                        if (tq < pcnt) break;
+                        tq -= pcnt;
+                    }
+                    if (c >= nchunks) continue;
+                    const int bit = __fns(mk[q * nchunks + c], 0, tq + 1);
+                    const int64_t pos = sm.qoff[w][q] + (o - sm.qpre[w][q]);
+                    if (pos < a.out_cap) {
+                        a.col_out[pos] = (int64_t)cands[c * 32 + bit];
+                        if (a.row_out) a.row_out[pos] = (int64_t)sm.qrow[w][q];
+                    }
                 }
             }
-        } else {
             __syncwarp();
-            for (int32_t o = lane; o < n; o += 32) {
-                int lo = 0, hi = nb;  // query: qpre[lo] <= o < qpre[hi]
-                while (hi - lo > 1) {
-                    const int mid = (lo + hi) >> 1;
-                    if (sm.qpre[w][mid] <= o) lo = mid; else hi = mid;
-                }
-                const int q = lo;
-                int32_t tq = o - sm.qpre[w][q];
-                int c = 0;  // chunk holding the query's tq-th hit (tq < hits of q, so c < nchunks)
-                for (; c < nchunks; ++c) {
-                    const int32_t pcnt = __popc(mk[q * nchunks + c]);
-                    if (tq < pcnt) break;
-                    tq -= pcnt;
-                }
-                if (c >= nchunks) continue;
-                const int bit = __fns(mk[q * nchunks + c], 0, tq + 1);
-                const int64_t pos = sm.qoff[w][q] + (o - sm.qpre[w][q]);
-                if (pos < a.out_cap) {
-                    a.col_out[pos] = (int64_t)cands[c * 32 + bit];
-                    if (a.row_out) a.row_out[pos] = (int64_t)sm.qrow[w][q];
-                }
-            }
         }
-        __syncwarp();
     }
 }
 
@@ -1948,11 +2000,17 @@ static int batch_of(const tcr_batch_desc* bd, int level, HostBatch& b) {
         int rc = check_cloud(who, c.dim, bd->mode, c.hash_map_length, c.n_query, c.n_ref, c.query_pos, c.query_sup,
                              c.ref_pos, c.ref_sup, bd->self_search, level);
         if (rc) return rc;
+        if (level >= 1 && c.hcell[0] > 0.0f)
+            for (int d = 0; d < c.dim; ++d)
+                if (!(c.hcell[d] > 0.0f) || !(c.hcell[d] < 3.0e38f))
+                    return set_error(TCR_ERR_INVALID, "%scell size override must be positive and finite", who);
         CloudParams& cp = b.clouds[k];
         memset(&cp, 0, sizeof(cp));
         cp.dim = c.dim;
         cp.mode = bd->mode;
         cp.periodic_mask = c.periodic_mask & ((1 << c.dim) - 1);
+        for (int d = 0; d < 3; ++d) cp.hcell_override[d] = c.hcell[0] > 0.0f ? (d < c.dim ? c.hcell[d] : 1.0f) : 0.0f;
+        cp.dedupe = c.clamped_grid ? 1 : 0;
         cp.hash_len = (uint32_t)c.hash_map_length;
         fill_domain(cp, c.dim, c.domain_min, c.domain_max);
         cp.n_query = (int32_t)c.n_query;
@@ -2055,6 +2113,8 @@ static WalkArgs make_walk(const HostBatch& b, const Structure& S, const Scratch&
     a.flagged = W.flagged;
     a.num_flagged = W.num_flagged;
     a.num_exact = W.num_exact;
+    a.big = W.big;
+    a.num_big = W.num_big;
     a.cursor = W.cursor;
     a.query_ids = b.query_ids;
     a.ref_ids = b.ref_ids;
@@ -2101,9 +2161,19 @@ template <int D, bool P, int M>
 struct CountLaunch {
     static cudaError_t launch(const WalkArgs& a, dim3 g, dim3 b, size_t smem, cudaStream_t st) {
         static uint64_t done = 0;
-        cudaError_t e = ensure_smem(walk_count_kernel<D, P, M>, (int)smem, &done);
+        cudaError_t e = ensure_smem(walk_count_kernel<D, P, M, false>, (int)smem, &done);
         if (e != cudaSuccess) return e;
-        walk_count_kernel<D, P, M><<<g, b, smem, st>>>(a);
+        walk_count_kernel<D, P, M, false><<<g, b, smem, st>>>(a);
+        return cudaGetLastError();
+    }
+};
+template <int D, bool P, int M>
+struct CountWindowedLaunch {
+    static cudaError_t launch(const WalkArgs& a, dim3 g, dim3 b, size_t smem, cudaStream_t st) {
+        static uint64_t done = 0;
+        cudaError_t e = ensure_smem(walk_count_kernel<D, P, M, true>, (int)smem, &done);
+        if (e != cudaSuccess) return e;
+        walk_count_kernel<D, P, M, true><<<g, b, smem, st>>>(a);
         return cudaGetLastError();
     }
 };
@@ -2271,6 +2341,8 @@ static int count_impl(const HostBatch& b, const Structure& S, const Scratch& W, 
         a.stage_cap = stage_cap;
         prof_mark(TCR_PROFILE_COUNT_WALK, 0, st);
         TCR_CUDA(launch_walks<CountLaunch>(b, a, dim3(walk_blocks(nq)), dim3(kWalkWarps * 32), sizeof(WalkSmem), st));
+        TCR_CUDA(launch_walks<CountWindowedLaunch>(b, a, dim3(walk_blocks(nq)), dim3(kWalkWarps * 32),
+                                                   sizeof(WalkSmem), st));
         prof_mark(TCR_PROFILE_COUNT_WALK, 1, st);
         stray_kernel<false><<<grid_for(nq, 128, num_sms() * 4), 128, 0, st>>>(a);
         note_launches(1);
