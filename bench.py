@@ -17,7 +17,9 @@ result copied back every step.  `roofline` covers the dominant kernel (the count
 inside the replays), `search_roofline` the whole search, `cpu_baseline` the reference's own CPU
 operators on this host.  `batched`, `graphs` and `served` measure the other forms: 256 clouds per
 launch against the per-call loop, graph replay against the eager API, and a request trace served
-with continuous batching against per-call searches.
+with continuous batching against per-call searches.  `adaptive` compares the multi-level search
+with single-level cells on variable supports; `scatter` times the per-particle scatter_sum over
+the neighbour list against its HBM roofline.
 """
 import argparse
 import json
@@ -48,6 +50,8 @@ def parse():
     ap.add_argument("--no-batched", action="store_true", help="skip the batched-form measurement")
     ap.add_argument("--profile-searches", type=int, default=0,
                     help="only run this many eager searches of the workload (a small case for ncu captures)")
+    ap.add_argument("--profile-scatter", type=int, default=0,
+                    help="only search the workload once and run this many scatter_sum calls over its neighbour list")
     return ap.parse_args()
 
 
@@ -621,6 +625,78 @@ def bench_adaptive(dev, flush, steps=3):
             "speedup_mlm_vs_compact": res["compact"]["ms_per_search"] / res["mlm"]["ms_per_search"]}
 
 
+def bench_scatter(dev, flush, steps=10):
+    """scatter_sum of one float32 value per pair onto the rows of the 1M-point neighbour list (COO,
+    rows non-decreasing): the per-particle sum an SPH density or a GNN aggregation does next.
+    Device time per call (L2 flushed), against the HBM roofline of reading the index and the
+    values once and writing the sums; torch's atomic index_add_ and the reference's own CPU
+    operator on the same data beside it."""
+    import torch
+
+    import torchcompactradius_b200 as tcr
+    pos, sup = make_workload()
+    x, h = pos.to(dev), sup.to(dev)
+    dom = tcr.DomainDescription(torch.full((3,), -1.0), torch.full((3,), 1.0), torch.zeros(3, dtype=torch.bool), 3)
+    adj = tcr.radiusSearch(tcr.PointCloud(x, h), None, mode="symmetric", domain=dom, algorithm="compact", format="coo")
+    row = adj.row
+    del adj
+    n, P = x.shape[0], row.numel()
+    vals = torch.rand(P, device=dev, generator=torch.Generator(dev).manual_seed(9))
+    stream = torch.cuda.current_stream(dev)
+
+    def timed(fn):
+        for _ in range(3):
+            fn()
+        ms = []
+        for k in range(steps):
+            flush.fill_(k & 0xff)
+            s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            s.record(stream)
+            r = fn()
+            e.record(stream)
+            e.synchronize()
+            ms.append(s.elapsed_time(e))
+        return statistics.median(ms), r
+
+    l0 = tcr_launches()
+    ms, sums = timed(lambda: tcr.scatter_sum(vals, row, 0, None, n))
+    launches = (tcr_launches() - l0) // (steps + 3)
+    again = tcr.scatter_sum(vals, row, 0, None, n)
+    ms_ia, ref_ia = timed(lambda: torch.zeros(n, device=dev).index_add_(0, row, vals))
+    alg = 8 * P + 4 * P + 4 * n  # index and values read once, sums written once
+    peak, peak_kind = measured_peak()
+    res = {"workload": "scatter_sum of one float32 per pair onto the rows of the 3D 1M symmetric neighbour list "
+                       f"({P} pairs, {n} rows, COO rows non-decreasing)",
+           "ms_per_call": ms, "value": P / (ms / 1e3), "unit": "pairs/s", "launches_per_call": int(launches),
+           "roofline": {"bound": "hbm", "algorithmic_bytes": alg, "achieved": alg / (ms / 1e3) / 1e9, "peak": peak,
+                        "unit": "GB/s", "frac": alg / (ms / 1e3) / 1e9 / peak, "peak_kind": peak_kind},
+           "repeatable": bool(torch.equal(sums, again)),
+           "torch_index_add_ms": ms_ia,
+           "torch_index_add_max_abs_diff": float((ref_ia - sums).abs().max())}
+    try:
+        from oracle import ref_pipeline
+        if ref_pipeline.available():
+            ops = ref_pipeline.ops()
+            torch.set_num_threads(os.cpu_count() or 1)
+            v_h, r_h = vals.cpu(), row.cpu()
+            ops.scatter_sum(v_h, r_h, 0, None, n)
+            t0 = time.perf_counter()
+            ref = ops.scatter_sum(v_h, r_h, 0, None, n)
+            dt = time.perf_counter() - t0
+            res["cpu_baseline"] = {"value": P / dt, "unit": "pairs/s", "cores": 1, "kind": "reference",
+                                   "sample": "the full reduction, one call after a warm-up (the reference's CPU "
+                                             "scatter loop is serial)", "seconds": dt,
+                                   "bit_identical": bool(torch.equal(ref, sums.cpu()))}
+    except Exception as ex:  # the compiled reference is optional on the GPU box
+        res["cpu_baseline"] = {"unavailable": str(ex)}
+    return res
+
+
+def tcr_launches():
+    from torchcompactradius_b200 import _lib
+    return int(_lib.load().tcr_kernel_launches())
+
+
 def cpu_baseline_batched(clouds, budget_s=12.0):
     """The reference's own CPU search, one call per cloud (its batched radius() fails), over the
     first clouds of the workload until about budget_s seconds have passed."""
@@ -837,6 +913,7 @@ def run_b200(args):
         set_tuning(0, 0)  # the other forms run with the defaults
         line["graphs"] = bench_graphs(dev, flush)
         line["adaptive"] = bench_adaptive(dev, flush)
+        line["scatter"] = bench_scatter(dev, flush)
         del flush
         line["served"] = bench_served(dev)
     if world > 1:
@@ -867,10 +944,29 @@ def profile_searches(n):
     return 0
 
 
+def profile_scatter(n):
+    """One search of the 1M-point workload (COO) and n scatter_sum calls over its rows."""
+    import torch
+
+    import torchcompactradius_b200 as tcr
+    pos, sup = make_workload()
+    p, h = pos.cuda(), sup.cuda()
+    dom = tcr.DomainDescription(torch.full((3,), -1.0), torch.full((3,), 1.0), torch.zeros(3, dtype=torch.bool), 3)
+    adj = tcr.radiusSearch(tcr.PointCloud(p, h), None, mode="symmetric", domain=dom, algorithm="compact", format="coo")
+    vals = torch.rand(adj.row.numel(), device="cuda")
+    for _ in range(n):
+        s = tcr.scatter_sum(vals, adj.row, 0, None, p.shape[0])
+    torch.cuda.synchronize()
+    print(json.dumps({"profile_scatter": n, "pairs": int(adj.row.numel()), "checksum": float(s.double().sum())}))
+    return 0
+
+
 def main():
     args = parse()
     if args.profile_searches:
         return profile_searches(args.profile_searches)
+    if args.profile_scatter:
+        return profile_scatter(args.profile_scatter)
     if args.impl == "reference":
         return run_reference(args)
     return run_b200(args)

@@ -20,7 +20,7 @@
 extern "C" {
 #endif
 
-#define TCR_ABI_VERSION 7
+#define TCR_ABI_VERSION 8
 
 #define TCR_OK 0
 #define TCR_ERR_INVALID (-1) /* bad argument or workspace too small */
@@ -250,6 +250,73 @@ int tcr_batch_emit(const tcr_batch_desc* b, const void* structure, void* scratch
  * (other streams, other host threads) race and must be serialised by the caller. */
 int tcr_search_noalloc(const tcr_search_desc* d, int64_t* offsets, int32_t* indptr_out, int64_t* row_entries_out,
                        int64_t* row_out, int64_t* col_out, int64_t pair_capacity, int64_t* total_out, void* stream);
+
+/* ---------------------------------------------------------------------------------------------
+ * Reductions of values onto an index: the reference's scatter operators scatter_sum, scatter_mul,
+ * scatter_mean, scatter_min and scatter_max (src/torchCompactRadius/cppSrc/sparseOperations/
+ * scatter.h:10-36, registered in cppSrc/cppWrapper.cpp:54-58; forward scatter_cpu.cpp:7-85 and
+ * scatter_cuda.cu:52-128).  src is viewed as [B][E][K] (E along the scattered dimension), out and
+ * arg_out as [B][N][K].  Every output element is reduced in increasing e, one element after the
+ * other in the element type's own arithmetic, exactly as the reference's CPU loop does: the sums
+ * and products are bit-identical to it (its CUDA kernel adds with atomics in an arbitrary order),
+ * and min/max keep the first of equal values as the reference's CPU loop does.
+ * ------------------------------------------------------------------------------------------- */
+#define TCR_REDUCE_SUM 0
+#define TCR_REDUCE_MEAN 1
+#define TCR_REDUCE_MUL 2
+#define TCR_REDUCE_MIN 3
+#define TCR_REDUCE_MAX 4
+
+/* Element types of src and out (AT_DISPATCH_ALL_TYPES_AND2(Half, BFloat16) in the reference). */
+#define TCR_DTYPE_U8 0
+#define TCR_DTYPE_I8 1
+#define TCR_DTYPE_I16 2
+#define TCR_DTYPE_I32 3
+#define TCR_DTYPE_I64 4
+#define TCR_DTYPE_F16 5
+#define TCR_DTYPE_BF16 6
+#define TCR_DTYPE_F32 7
+#define TCR_DTYPE_F64 8
+
+typedef struct tcr_scatter_desc {
+    int32_t reduce;        /* TCR_REDUCE_* */
+    int32_t dtype;         /* TCR_DTYPE_* of src and out */
+    int32_t index_full;    /* 0: index[E], the same for every b and k (an index broadcast along the
+                              scattered dimension); 1: index[B][E][K] */
+    int32_t index_sorted;  /* index_full == 0: 1 when index is non-decreasing (stats[2] == 0 from
+                              tcr_index_stats); such an index needs no sort */
+    int32_t accumulate;    /* 1: out holds the starting values (the reference's optional_out);
+                              0: out is overwritten (0 where no element lands) */
+    int32_t reserved;
+    int64_t B, E, K, N;
+    const void* src;       /* device [B*E*K], contiguous */
+    const int64_t* index;  /* device [E] or [B*E*K] */
+    void* out;             /* device [B*N*K] */
+    int64_t* arg_out;      /* TCR_REDUCE_MIN / MAX: device [B*N*K], the e of the kept value or E when
+                              none (the reference's arg_out); otherwise NULL */
+} tcr_scatter_desc;
+
+/* sizeof(tcr_scatter_desc) as compiled into the library, for FFI layout checks. */
+int64_t tcr_scatter_desc_bytes(void);
+
+/* stats[0] = min, stats[1] = max (INT64_MAX / INT64_MIN for n == 0) and stats[2] = the number of
+ * positions i > 0 with index[i] < index[i - 1], over the n values of index.  stats is 3 int64 of
+ * device memory; when stats_host is not NULL (pinned host memory) they are also copied there, in
+ * stream order.  Replaces the host side of the reference's sizing (`index.max()`,
+ * scatter_cpu.cpp:29-35) and tells whether the index needs sorting. */
+int tcr_index_stats(const int64_t* index, int64_t n, int64_t* stats, int64_t* stats_host, void* stream);
+
+/* Scratch bytes tcr_scatter needs for this description. */
+int tcr_scatter_sizes(const tcr_scatter_desc* d, int64_t* scratch_bytes);
+
+/* One reduction (the reference's scatter_fw, scatterWrapper.cpp:29-42, with the reduce of
+ * Reducer<>::update, reducer.h:44-66).  Index values must lie in [0, N): others land nowhere (the
+ * reference writes outside out).  TCR_REDUCE_MEAN divides by the count of elements that landed,
+ * counted in the element type, below 1 taken as 1 (true division for floating types, floor
+ * division for integers), as the reference's scatter_mean does (scatterWrapper.cpp:121-146).
+ * Without accumulate, MIN / MAX outputs still at the type's max / lowest become 0.  With
+ * E == 0 (no elements) and no accumulate, out becomes 0 and arg_out E, for every reduce. */
+int tcr_scatter(const tcr_scatter_desc* d, void* scratch, int64_t scratch_bytes, void* stream);
 
 #ifdef __cplusplus
 }

@@ -35,7 +35,7 @@ def test_descriptor_layout_matches_library():
     assert ctypes.sizeof(_lib.SearchDesc) == _lib.load().tcr_desc_bytes()
     assert ctypes.sizeof(_lib.CloudDesc) == _lib.load().tcr_cloud_desc_bytes()
     assert ctypes.sizeof(_lib.BatchDesc) == _lib.load().tcr_batch_desc_bytes()
-    assert _lib.load().tcr_version() == 7
+    assert _lib.load().tcr_version() == 8
 
 
 def _batch(clouds, mode=0, self_search=1):
@@ -151,3 +151,41 @@ def test_tuning_is_validated():
     assert lib.tcr_set_tuning(0, 65) == -1
     assert lib.tcr_set_tuning(16, 8) == 0
     assert lib.tcr_set_tuning(0, 0) == 0  # back to the defaults
+
+
+def test_scatter_descriptor_and_validation_without_device_work():
+    """tcr_scatter_desc layout, scratch sizing per index layout, and argument checks that fail
+    before any device call."""
+    from torchcompactradius_b200 import _lib
+    lib = _lib.load()
+    assert ctypes.sizeof(_lib.ScatterDesc) == lib.tcr_scatter_desc_bytes()
+    d = _lib.ScatterDesc()
+    d.reduce, d.dtype, d.B, d.E, d.K, d.N = 0, 7, 1, 1000, 1, 50
+    d.index_sorted = 1
+    sorted_bytes = _lib.scatter_sizes(d)
+    d.index_sorted = 0
+    unsorted_bytes = _lib.scatter_sizes(d)
+    assert unsorted_bytes > sorted_bytes > 0  # only an unsorted index needs the sort buffers
+    d.index_full, d.B, d.K = 1, 2, 3
+    assert _lib.scatter_sizes(d) > unsorted_bytes
+    for field, bad in (("reduce", 5), ("dtype", 9), ("N", -1)):
+        e = _lib.ScatterDesc()
+        e.reduce, e.dtype, e.B, e.E, e.K, e.N = 0, 7, 1, 10, 1, 4
+        setattr(e, field, bad)
+        assert lib.tcr_scatter_sizes(ctypes.byref(e), None) == -1
+        assert lib.tcr_scatter(ctypes.byref(e), None, 0, None) == -1
+    e = _lib.ScatterDesc()
+    e.reduce, e.dtype, e.B, e.E, e.K, e.N = 3, 7, 1, 10, 1, 4  # min without arg_out / src / index
+    assert lib.tcr_scatter(ctypes.byref(e), None, 0, None) == -1
+    assert lib.tcr_index_stats(None, -1, None, None, None) == -1
+
+
+def test_scatter_index_broadcast_matches_reference_rule():
+    import torch
+    from torchcompactradius_b200.scatter import broadcast
+    src = torch.empty(3, 5, 4)
+    b = broadcast(torch.arange(5), src, 1)
+    assert b.shape == src.shape and b.stride(0) == 0 and b.stride(2) == 0
+    assert torch.equal(b[2, :, 3], torch.arange(5))
+    full = torch.zeros(3, 5, 4, dtype=torch.int64)
+    assert broadcast(full, src, 1).data_ptr() == full.data_ptr()

@@ -77,10 +77,33 @@ class BatchDesc(ctypes.Structure):
     ]
 
 
+class ScatterDesc(ctypes.Structure):
+    """tcr_scatter_desc (include/tcr_b200.h): one reduction of values onto an index."""
+    _fields_ = [
+        ("reduce", ctypes.c_int32),
+        ("dtype", ctypes.c_int32),
+        ("index_full", ctypes.c_int32),
+        ("index_sorted", ctypes.c_int32),
+        ("accumulate", ctypes.c_int32),
+        ("reserved", ctypes.c_int32),
+        ("B", ctypes.c_int64),
+        ("E", ctypes.c_int64),
+        ("K", ctypes.c_int64),
+        ("N", ctypes.c_int64),
+        ("src", ctypes.c_void_p),
+        ("index", ctypes.c_void_p),
+        ("out", ctypes.c_void_p),
+        ("arg_out", ctypes.c_void_p),
+    ]
+
+
+REDUCE = {"sum": 0, "mean": 1, "mul": 2, "min": 3, "max": 4}
+
 # name -> (restype, argtypes); every function declared in include/tcr_b200.h
 _vp, _i64, _i32 = ctypes.c_void_p, ctypes.c_int64, ctypes.c_int32
 _desc_p = ctypes.POINTER(SearchDesc)
 _batch_p = ctypes.POINTER(BatchDesc)
+_scatter_p = ctypes.POINTER(ScatterDesc)
 SIGNATURES = {
     "tcr_last_error": (ctypes.c_char_p, []),
     "tcr_version": (ctypes.c_int, []),
@@ -101,6 +124,10 @@ SIGNATURES = {
     "tcr_batch_count": (ctypes.c_int, [_batch_p, _vp, _vp, _i64, _vp, _i64, _vp, _vp, _vp, _vp, _vp]),
     "tcr_batch_emit": (ctypes.c_int, [_batch_p, _vp, _vp, _i64, _vp, _vp, _vp, _vp, _i64, _vp]),
     "tcr_search_noalloc": (ctypes.c_int, [_desc_p, _vp, _vp, _vp, _vp, _vp, _i64, ctypes.POINTER(_i64), _vp]),
+    "tcr_scatter_desc_bytes": (_i64, []),
+    "tcr_index_stats": (ctypes.c_int, [_vp, _i64, _vp, _vp, _vp]),
+    "tcr_scatter_sizes": (ctypes.c_int, [_scatter_p, ctypes.POINTER(_i64)]),
+    "tcr_scatter": (ctypes.c_int, [_scatter_p, _vp, _i64, _vp]),
 }
 
 
@@ -145,6 +172,12 @@ def search_sizes(n_query, n_ref, dim):
     s, w = _i64(0), _i64(0)
     check(load().tcr_search_sizes(n_query, n_ref, dim, ctypes.byref(s), ctypes.byref(w)), "tcr_search_sizes")
     return s.value, w.value
+
+
+def scatter_sizes(sdesc):
+    w = _i64(0)
+    check(load().tcr_scatter_sizes(ctypes.byref(sdesc), ctypes.byref(w)), "tcr_scatter_sizes")
+    return w.value
 
 
 def batch_sizes(bdesc):

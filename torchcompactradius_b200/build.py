@@ -7,10 +7,10 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 REPO = os.path.dirname(HERE)
 NVCC_FLAGS = ["-gencode", "arch=compute_100a,code=sm_100a", "-lineinfo", "-O3", "-std=c++17", "-Xcompiler", "-fPIC",
-              "-shared", "-I" + os.path.join(REPO, "include")]
+              "-shared", "-static-global-template-stub=true", "-I" + os.path.join(REPO, "include")]
 
 LIBS = {
-    "libtcr_b200.so": ["tcr_search.cu"],
+    "libtcr_b200.so": ["tcr_search.cu", "tcr_scatter.cu"],
 }
 
 

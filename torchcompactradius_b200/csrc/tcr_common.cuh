@@ -10,14 +10,27 @@
 // contract it into an FMA; the float fast test below is decided exactly by this path whenever
 // its result lies inside a narrow band around the threshold.
 #pragma once
+#include <cstdarg>
 #include <cstdint>
+#include <cstdio>
 #include <cuda_runtime.h>
 
 namespace tcr {
 
-// Number of kernels this library has launched (all threads), for launch accounting.
-static unsigned long long g_launches = 0;
+// Number of kernels this library has launched (all threads, every source file), for launch
+// accounting.
+inline unsigned long long g_launches = 0;
 static inline void note_launches(int k) { __atomic_fetch_add(&g_launches, (unsigned long long)k, __ATOMIC_RELAXED); }
+
+// The calling thread's last error message (tcr_last_error), shared by every source file.
+inline thread_local char g_err[512];
+static inline int set_error(int code, const char* fmt, ...) {
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(g_err, sizeof(g_err), fmt, ap);
+    va_end(ap);
+    return code;
+}
 
 enum Mode : int { kGather = 0, kScatter = 1, kSymmetric = 2, kSuperSymmetric = 3 };
 
@@ -141,7 +154,7 @@ struct ExactCtx {
     float ext[3];
 };
 // The reference's exact distance test (common.h:106-129 at scalar_t=float).
-__device__ __noinline__ bool exact_pair_test(ExactCtx sp, float4 xi, float hi, float4 xj, float hj) {
+static __device__ __noinline__ bool exact_pair_test(ExactCtx sp, float4 xi, float hi, float4 xj, float hj) {
     float sum = 0.0f;
     for (int d = 0; d < sp.dim; ++d) {
         float a = comp(xi, d), b = comp(xj, d);

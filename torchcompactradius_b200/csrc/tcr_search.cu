@@ -34,15 +34,7 @@
 namespace tcr {
 
 // ------------------------------------------------------------------------------------------
-// error reporting
-static thread_local char g_err[512];
-static int set_error(int code, const char* fmt, ...) {
-    va_list ap;
-    va_start(ap, fmt);
-    vsnprintf(g_err, sizeof(g_err), fmt, ap);
-    va_end(ap);
-    return code;
-}
+// error reporting (set_error / g_err: tcr_common.cuh)
 #define TCR_CUDA(call)                                                                         \
     do {                                                                                       \
         cudaError_t e_ = (call);                                                               \
