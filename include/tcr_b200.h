@@ -310,13 +310,18 @@ int tcr_index_stats(const int64_t* index, int64_t n, int64_t* stats, int64_t* st
 int tcr_scatter_sizes(const tcr_scatter_desc* d, int64_t* scratch_bytes);
 
 /* One reduction (the reference's scatter_fw, scatterWrapper.cpp:29-42, with the reduce of
- * Reducer<>::update, reducer.h:44-66).  Index values must lie in [0, N): others land nowhere (the
- * reference writes outside out).  TCR_REDUCE_MEAN divides by the count of elements that landed,
- * counted in the element type, below 1 taken as 1 (true division for floating types, floor
- * division for integers), as the reference's scatter_mean does (scatterWrapper.cpp:121-146).
- * Without accumulate, MIN / MAX outputs still at the type's max / lowest become 0.  With
- * E == 0 (no elements) and no accumulate, out becomes 0 and arg_out E, for every reduce. */
-int tcr_scatter(const tcr_scatter_desc* d, void* scratch, int64_t scratch_bytes, void* stream);
+ * Reducer<>::update, reducer.h:44-66).  TCR_REDUCE_MEAN divides by the count of elements that
+ * landed, counted in the element type, below 1 taken as 1 (true division for floating types,
+ * floor division for integers), as the reference's scatter_mean does (scatterWrapper.cpp:121-146).
+ * Without accumulate, MIN / MAX outputs still at the type's max / lowest become 0.  With E == 0
+ * (no elements) and no accumulate, out becomes 0 and arg_out E, for every reduce.
+ * The index is checked on the device while it is read: when some value lies outside [0, N), or
+ * index_sorted is 1 and the index descends somewhere, nothing is written (out and arg_out keep
+ * their contents).  stats_host (pinned host memory, 3 int64, may be NULL) receives the index's
+ * min, max and (with index_sorted = 1) number of descents, in stream order, so that a caller who
+ * guessed "sorted" learns whether the call ran and otherwise calls again with index_sorted = 0
+ * (the reference writes outside out for such indices). */
+int tcr_scatter(const tcr_scatter_desc* d, void* scratch, int64_t scratch_bytes, int64_t* stats_host, void* stream);
 
 #ifdef __cplusplus
 }

@@ -173,10 +173,10 @@ def test_scatter_descriptor_and_validation_without_device_work():
         e.reduce, e.dtype, e.B, e.E, e.K, e.N = 0, 7, 1, 10, 1, 4
         setattr(e, field, bad)
         assert lib.tcr_scatter_sizes(ctypes.byref(e), None) == -1
-        assert lib.tcr_scatter(ctypes.byref(e), None, 0, None) == -1
+        assert lib.tcr_scatter(ctypes.byref(e), None, 0, None, None) == -1
     e = _lib.ScatterDesc()
     e.reduce, e.dtype, e.B, e.E, e.K, e.N = 3, 7, 1, 10, 1, 4  # min without arg_out / src / index
-    assert lib.tcr_scatter(ctypes.byref(e), None, 0, None) == -1
+    assert lib.tcr_scatter(ctypes.byref(e), None, 0, None, None) == -1
     assert lib.tcr_index_stats(None, -1, None, None, None) == -1
 
 

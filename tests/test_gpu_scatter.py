@@ -187,3 +187,40 @@ def test_neighbour_list_reduction_at_full_size():
         assert b - a == indptr[r + 1] - indptr[r]
         acc = np.cumsum(v[a:b], dtype=np.float32)[-1] if b > a else np.float32(0)
         assert np.float32(sums[r].item()) == acc
+
+
+def test_known_size_paths_fall_back_for_unsorted_and_reject_out_of_range():
+    """With the output size known the index is first taken in its own order; an index that
+    descends (here one alternating between the ends, whose runs would overlap) falls back to the
+    sorted path, and an index outside [0, N) leaves a given out untouched."""
+    g = torch.Generator().manual_seed(8)
+    N = 100000
+    index = torch.zeros(20000, dtype=torch.int64)
+    index[1::2] = N - 1
+    src = torch.randn(20000, generator=g)
+    for reduce in REDUCES:
+        res, arg = run(src.cuda(), index.cuda(), 0, reduce, dim_size=N)
+        want, warg = oracle(src, index, 0, reduce, dim_size=N)
+        check_bits(res, want, torch.float32)
+        if warg is not None:
+            assert np.array_equal(arg.cpu().numpy(), warg)
+    out = torch.full((10,), 7.0, device="cuda")
+    bad = torch.tensor([0, 3, 10], device="cuda")
+    with pytest.raises(IndexError):
+        tcr().scatter_sum(torch.ones(3, device="cuda"), bad, 0, out)
+    assert torch.equal(out, torch.full((10,), 7.0, device="cuda"))
+
+
+@pytest.mark.parametrize("shape,dim", [((3, 5000), 1), ((5000, 6), 0), ((2, 5000, 40), 1)])
+def test_sorted_index_with_known_size_and_batches_or_features(shape, dim):
+    g = torch.Generator().manual_seed(12)
+    E = shape[dim]
+    index = torch.sort(torch.randint(0, 300, (E,), generator=g))[0]
+    for dtype in (torch.float32, torch.bfloat16, torch.int64):
+        for reduce in REDUCES:
+            src = _values(g, dtype, reduce, shape)
+            res, arg = run(src.cuda(), index.cuda(), dim, reduce, dim_size=310)
+            want, warg = oracle(src, index, dim, reduce, dim_size=310)
+            check_bits(res, want, dtype)
+            if warg is not None:
+                assert np.array_equal(arg.cpu().numpy(), warg)

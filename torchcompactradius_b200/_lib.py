@@ -127,7 +127,7 @@ SIGNATURES = {
     "tcr_scatter_desc_bytes": (_i64, []),
     "tcr_index_stats": (ctypes.c_int, [_vp, _i64, _vp, _vp, _vp]),
     "tcr_scatter_sizes": (ctypes.c_int, [_scatter_p, ctypes.POINTER(_i64)]),
-    "tcr_scatter": (ctypes.c_int, [_scatter_p, _vp, _i64, _vp]),
+    "tcr_scatter": (ctypes.c_int, [_scatter_p, _vp, _i64, _vp, _vp]),
 }
 
 

@@ -18,7 +18,9 @@
 #include <cfloat>
 #include <climits>
 #include <cstdint>
+#include <mutex>
 #include <type_traits>
+#include <unordered_map>
 #include <cuda_bf16.h>
 #include <cuda_fp16.h>
 #include <cuda_runtime.h>
@@ -55,8 +57,7 @@ struct Carve {
     }
 };
 
-// Grid of a grid-stride kernel over n items: enough blocks to fill every SM, no more than needed.
-inline unsigned grid_for(int64_t n) {
+inline int sm_count() {
     static int sms[64] = {0};
     int dev = 0;
     cudaGetDevice(&dev);
@@ -64,8 +65,36 @@ inline unsigned grid_for(int64_t n) {
     if (s == 0) {
         if (cudaDeviceGetAttribute(&s, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || s <= 0) s = 148;
     }
+    return s;
+}
+
+// Grid of a grid-stride kernel over n items: enough blocks to fill every SM, no more than needed.
+inline unsigned grid_for(int64_t n) {
     const int64_t want = (n + kThreads - 1) / kThreads;
-    const int64_t cap = (int64_t)s * 8;
+    const int64_t cap = (int64_t)sm_count() * 8;
+    return (unsigned)(want < 1 ? 1 : (want < cap ? want : cap));
+}
+
+// The same for a streaming kernel whose blocks all carry equal shares of the work: exactly the
+// blocks that are resident at once (one wave), so no SM idles through a partial second wave.
+template <typename Kern>
+unsigned grid_resident(Kern kernel, int64_t n) {
+    static std::mutex mu;
+    static std::unordered_map<const void*, int> per_sm;
+    int nb = 0;
+    {
+        std::lock_guard<std::mutex> lk(mu);
+        auto it = per_sm.find(reinterpret_cast<const void*>(kernel));
+        if (it != per_sm.end()) {
+            nb = it->second;
+        } else {
+            if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, kernel, kThreads, 0) != cudaSuccess || nb <= 0)
+                nb = 4;
+            per_sm[reinterpret_cast<const void*>(kernel)] = nb;
+        }
+    }
+    const int64_t want = (n + kThreads - 1) / kThreads;
+    const int64_t cap = (int64_t)sm_count() * nb;
     return (unsigned)(want < 1 ? 1 : (want < cap ? want : cap));
 }
 
@@ -183,17 +212,8 @@ __global__ void stats_init_kernel(int64_t* stats) {
     stats[2] = 0;
 }
 
-__global__ void __launch_bounds__(kThreads) index_stats_kernel(const int64_t* __restrict__ idx, int64_t n,
-                                                               int64_t* stats) {
-    long long lo = LLONG_MAX, hi = LLONG_MIN;
-    unsigned long long desc = 0;
-    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
-    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
-        const long long v = idx[i];
-        lo = v < lo ? v : lo;
-        hi = v > hi ? v : hi;
-        if (i > 0 && v < idx[i - 1]) ++desc;
-    }
+// One warp's contribution to stats (min, max, descents); every lane of the warp calls it.
+__device__ __forceinline__ void stats_add(int64_t* stats, long long lo, long long hi, unsigned long long desc) {
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) {
         const long long l2 = __shfl_down_sync(0xffffffffu, lo, o);
@@ -209,6 +229,27 @@ __global__ void __launch_bounds__(kThreads) index_stats_kernel(const int64_t* __
     }
 }
 
+__global__ void __launch_bounds__(kThreads) index_stats_kernel(const int64_t* __restrict__ idx, int64_t n,
+                                                               int64_t* stats) {
+    long long lo = LLONG_MAX, hi = LLONG_MIN;
+    unsigned long long desc = 0;
+    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
+        const long long v = idx[i];
+        lo = v < lo ? v : lo;
+        hi = v > hi ? v : hi;
+        if (i > 0 && v < idx[i - 1]) ++desc;
+    }
+    stats_add(stats, lo, hi, desc);
+}
+
+// The fold may run: every index value lies in [0, N) and, when the index is used in its own
+// order, it never descends.  Otherwise the folds write nothing and the caller, who reads the
+// statistics back, reports the index or sorts it.
+__device__ __forceinline__ bool stats_allow(const int64_t* stats, int64_t N, bool need_sorted) {
+    return stats[0] >= 0 && stats[1] < N && (!need_sorted || stats[2] == 0);
+}
+
 // ------------------------------------------------------------------------------------------
 // sort keys: the output slot of every element (slot = index for an index over e, (b*K + k)*N +
 // index for a full index), with all ones for an index outside [0, N) so that it sorts past every
@@ -219,11 +260,14 @@ __global__ void sort_init_kernel(SortStateT<K>* st) { sort_state_reset(st); }
 template <typename K, bool FULL>
 __global__ void __launch_bounds__(kThreads) pack_keys_kernel(const int64_t* __restrict__ idx, int64_t M, int64_t E,
                                                              int64_t Kdim, int64_t N, K* keys, int32_t* vals,
-                                                             SortStateT<K>* st) {
+                                                             SortStateT<K>* st, int64_t* stats) {
     K kmin = ~(K)0, kmax = 0;
+    long long lo = LLONG_MAX, hi = LLONG_MIN;
     const int64_t stride = (int64_t)gridDim.x * blockDim.x;
     for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < M; i += stride) {
         const int64_t v = idx[i];
+        lo = v < lo ? v : lo;
+        hi = v > hi ? v : hi;
         K key = ~(K)0;
         if (v >= 0 && v < N) {
             if (FULL) {
@@ -250,6 +294,7 @@ __global__ void __launch_bounds__(kThreads) pack_keys_kernel(const int64_t* __re
         if (kmin != ~(K)0) atomicMin(&st->key_min, kmin);
         if (kmax != 0) atomicMax(&st->key_max, kmax);
     }
+    stats_add(stats, lo, hi, 0ull);
 }
 
 // ------------------------------------------------------------------------------------------
@@ -268,38 +313,142 @@ __device__ __forceinline__ int64_t key_slot(unsigned long long k, int64_t nslots
 }
 
 __device__ __forceinline__ void mark_range(int64_t lo, int64_t hi, int64_t value, int64_t* off, int64_t* gaps,
-                                           unsigned long long* ngaps, int64_t gap_cap) {
+                                           unsigned long long* ngaps, int64_t gap_cap, unsigned long long* descents) {
     if (hi < lo) return;
     if (hi - lo + 1 > kInlineGap) {
-        // Disjoint runs longer than kInlineGap number at most gap_cap; an index that was declared
-        // sorted but is not can overlap runs, and then the thread writes its run itself.
+        // The runs of a non-decreasing index are disjoint, so at most gap_cap of them are longer
+        // than kInlineGap; more means the index descends (its fold will not run): count a descent
+        // and drop the run, so that an unsorted index costs bounded work here.
         const unsigned long long g = atomicAdd(ngaps, 1ull);
         if (g < (unsigned long long)gap_cap) {
             gaps[3 * g] = lo;
             gaps[3 * g + 1] = hi;
             gaps[3 * g + 2] = value;
-            return;
+        } else {
+            atomicAdd(descents, 1ull);
         }
+        return;
     }
     for (int64_t s = lo; s <= hi; ++s) off[s] = value;
 }
 
+// Eight consecutive keys from base (fewer at the end of the array): loaded before any of them is
+// used, with 16-byte vector loads when the keys are 16-byte aligned, so each thread keeps eight
+// loads in flight.
+constexpr int kMarkKeys = 8;
+
 template <typename KT>
-__global__ void __launch_bounds__(kThreads) mark_runs_kernel(const KT* k0, const KT* k1, const int32_t* sel, int64_t M,
-                                                             int64_t nslots, int64_t* off, int64_t* gaps,
-                                                             unsigned long long* ngaps, int64_t gap_cap) {
-    const KT* keys = (sel && *sel) ? k1 : k0;
-    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
-    for (int64_t j = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; j < M; j += stride) {
-        const int64_t cur = key_slot(keys[j], nslots);
-        const int64_t prev = j == 0 ? -1 : key_slot(keys[j - 1], nslots);
-        mark_range(prev + 1 < 0 ? 0 : prev + 1, cur, j, off, gaps, ngaps, gap_cap);
-        if (j == M - 1) mark_range(cur + 1 < 0 ? 0 : cur + 1, nslots, M, off, gaps, ngaps, gap_cap);
+__device__ __forceinline__ void load_keys(const KT* keys, int64_t base, int64_t M, bool aligned, KT (&v)[kMarkKeys]) {
+    if (base + kMarkKeys <= M) {
+        if constexpr (sizeof(KT) == 8) {
+            if (aligned) {
+                const longlong2* p = reinterpret_cast<const longlong2*>(keys + base);
+#pragma unroll
+                for (int k = 0; k < kMarkKeys / 2; ++k) {
+                    const longlong2 q = p[k];
+                    v[2 * k] = (KT)q.x;
+                    v[2 * k + 1] = (KT)q.y;
+                }
+                return;
+            }
+        } else {
+            if (aligned) {
+                const uint4* p = reinterpret_cast<const uint4*>(keys + base);
+#pragma unroll
+                for (int k = 0; k < kMarkKeys / 4; ++k) {
+                    const uint4 q = p[k];
+                    v[4 * k] = (KT)q.x;
+                    v[4 * k + 1] = (KT)q.y;
+                    v[4 * k + 2] = (KT)q.z;
+                    v[4 * k + 3] = (KT)q.w;
+                }
+                return;
+            }
+        }
+#pragma unroll
+        for (int k = 0; k < kMarkKeys; ++k) v[k] = keys[base + k];
+    } else {
+#pragma unroll
+        for (int k = 0; k < kMarkKeys; ++k) v[k] = base + k < M ? keys[base + k] : (KT)0;
     }
 }
 
+// RAW: the keys are the caller's index in its own order (min, max and descents go to stats).
+// Each thread takes kMarkKeys consecutive positions.  Most such chunks lie inside one run (a run
+// of a neighbour list's rows is ~50 long): a chunk that never descends and ends on the key before
+// it marks nothing, so it costs a few compares; only chunks where the key changes mark run starts.
+template <typename KT, bool RAW>
+__global__ void __launch_bounds__(kThreads) mark_runs_kernel(const KT* k0, const KT* k1, const int32_t* sel, int64_t M,
+                                                             int64_t nslots, int64_t* off, int64_t* gaps,
+                                                             unsigned long long* ngaps, int64_t gap_cap,
+                                                             int64_t* stats) {
+    const KT* keys = (sel && *sel) ? k1 : k0;
+    const bool aligned = (reinterpret_cast<uintptr_t>(keys) & 15) == 0;
+    unsigned long long* dsc = reinterpret_cast<unsigned long long*>(&stats[2]);
+    long long lo = LLONG_MAX, hi = LLONG_MIN;
+    unsigned long long desc = 0;
+    const int64_t nchunks = (M + kMarkKeys - 1) / kMarkKeys;
+    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    for (int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; c < nchunks; c += stride) {
+        const int64_t base = c * kMarkKeys;
+        const int nk = M - base < kMarkKeys ? (int)(M - base) : kMarkKeys;
+        KT v[kMarkKeys];
+        load_keys(keys, base, M, aligned, v);
+        const KT pk = base == 0 ? v[0] : keys[base - 1];
+        bool mono = true;
+        KT last = v[0];
+#pragma unroll
+        for (int k = 0; k < kMarkKeys; ++k) {
+            if (k < nk) {
+                const KT before = k == 0 ? pk : v[k - 1];
+                if (v[k] < before) {
+                    mono = false;
+                    if (RAW) ++desc;
+                }
+                last = v[k];
+            }
+        }
+        if (RAW) {
+            if (mono) {
+                const long long a = (long long)v[0], b = (long long)last;
+                lo = a < lo ? a : lo;
+                hi = b > hi ? b : hi;
+            } else {
+#pragma unroll
+                for (int k = 0; k < kMarkKeys; ++k) {
+                    if (k < nk) {
+                        const long long x = (long long)v[k];
+                        lo = x < lo ? x : lo;
+                        hi = x > hi ? x : hi;
+                    }
+                }
+            }
+        }
+        if (!(mono && base > 0 && last == pk)) {  // some run starts in this chunk
+            int64_t prev = base == 0 ? -1 : key_slot(pk, nslots);
+#pragma unroll
+            for (int k = 0; k < kMarkKeys; ++k) {
+                if (k < nk) {
+                    const int64_t cur = key_slot(v[k], nslots);
+                    mark_range(prev + 1 < 0 ? 0 : prev + 1, cur, base + k, off, gaps, ngaps, gap_cap, dsc);
+                    prev = cur;
+                }
+            }
+        }
+        if (base + nk == M) {  // after the last key: the remaining slots start at M
+            const int64_t cur = key_slot(last, nslots);
+            mark_range(cur + 1 < 0 ? 0 : cur + 1, nslots, M, off, gaps, ngaps, gap_cap, dsc);
+        }
+    }
+    if (RAW) stats_add(stats, lo, hi, desc);
+}
+
+// need_sorted: the runs come from the caller's index in its own order, which holds only when it
+// never descends (otherwise the runs may overlap and the fold will not run: nothing to fill).
 __global__ void __launch_bounds__(kThreads) fill_gaps_kernel(const int64_t* gaps, const unsigned long long* ngaps,
-                                                             int64_t gap_cap, int64_t* off) {
+                                                             int64_t gap_cap, int64_t* off, const int64_t* stats,
+                                                             int need_sorted) {
+    if (need_sorted && stats[2] != 0) return;
     unsigned long long n = *ngaps;
     if (n > (unsigned long long)gap_cap) n = (unsigned long long)gap_cap;
     for (unsigned long long g = blockIdx.x; g < n; g += gridDim.x) {
@@ -320,6 +469,7 @@ struct FoldArgs {
     const int32_t* perm0;
     const int32_t* perm1;
     const int32_t* sel;   // which perm buffer holds the sorted order (null: perm0)
+    const int64_t* stats; // index statistics of this call (stats_allow)
     int64_t B, E, K, N;
     int32_t accumulate;
 };
@@ -345,9 +495,77 @@ struct Fold {
     }
 };
 
+template <typename T, int R>
+__device__ __forceinline__ void fold_write(const FoldArgs& a, T* out, int64_t t, const Fold<T, R>& f) {
+    using Nm = Num<T>;
+    if (R == TCR_REDUCE_MEAN) {
+        T c = f.cnt;
+        if (Nm::lt(c, Nm::one())) c = Nm::one();
+        out[t] = Nm::div(f.acc, c);
+    } else if (R == TCR_REDUCE_MIN || R == TCR_REDUCE_MAX) {
+        T v = f.acc;
+        if (!a.accumulate && Nm::eq(v, reduce_init<T, R>())) v = Nm::zero();
+        out[t] = v;
+        a.arg[t] = f.arg;
+    } else {
+        out[t] = f.acc;
+    }
+}
+
+// Index over e, non-decreasing, one value per (b, e) (K == 1): a block owns kThreads consecutive
+// rows of one b, whose elements are one contiguous range of src.  The range streams through
+// shared memory in tiles with coalesced loads; each thread folds its own row from the tile in
+// order.
+constexpr int kFoldTileBytes = 16384;
+
+template <typename T, int R>
+__global__ void __launch_bounds__(kThreads) fold_rows_kernel(FoldArgs a) {
+    using Nm = Num<T>;
+    constexpr int TILE = kFoldTileBytes / (int)sizeof(T);
+    __shared__ __align__(16) unsigned char tile_raw[kFoldTileBytes];
+    T* tile = reinterpret_cast<T*>(tile_raw);
+    if (!stats_allow(a.stats, a.N, true)) return;
+    const T* __restrict__ src = static_cast<const T*>(a.src);
+    T* __restrict__ out = static_cast<T*>(a.out);
+    const int64_t M = a.E;
+    const int64_t rb = (a.N + kThreads - 1) / kThreads;
+    for (int64_t blk = blockIdx.x; blk < a.B * rb; blk += gridDim.x) {
+        const int64_t b = blk / rb, n0 = (blk % rb) * kThreads;
+        const int64_t n = n0 + threadIdx.x;
+        const int64_t nend = n0 + kThreads < a.N ? n0 + kThreads : a.N;
+        int64_t E0 = a.off[n0], E1 = a.off[nend];
+        E0 = E0 < 0 ? 0 : (E0 > M ? M : E0);
+        E1 = E1 < E0 ? E0 : (E1 > M ? M : E1);
+        int64_t lo = E1, hi = E1;
+        if (n < a.N) {
+            lo = a.off[n];
+            hi = a.off[n + 1];
+            lo = lo < E0 ? E0 : (lo > E1 ? E1 : lo);
+            hi = hi < lo ? lo : (hi > E1 ? E1 : hi);
+        }
+        Fold<T, R> f;
+        f.acc = (a.accumulate && n < a.N) ? out[b * a.N + n] : reduce_init<T, R>();
+        f.cnt = Nm::zero();
+        f.arg = a.E;
+        const T* s = src + b * a.E;
+        for (int64_t t0 = E0; t0 < E1; t0 += TILE) {
+            const int len = (int)(E1 - t0 < TILE ? E1 - t0 : TILE);
+            __syncthreads();  // the previous tile is consumed
+#pragma unroll 8
+            for (int i = threadIdx.x; i < len; i += kThreads) tile[i] = s[t0 + i];
+            __syncthreads();
+            const int64_t j0 = lo > t0 ? lo : t0;
+            const int64_t j1 = hi < t0 + len ? hi : t0 + len;
+            for (int64_t j = j0; j < j1; ++j) f.take(tile[j - t0], j);
+        }
+        if (n < a.N) fold_write<T, R>(a, out, b * a.N + n, f);
+    }
+}
+
 template <typename T, int R, int P>
 __global__ void __launch_bounds__(kThreads) fold_kernel(FoldArgs a) {
     using Nm = Num<T>;
+    if (!stats_allow(a.stats, a.N, P == 0)) return;
     const T* __restrict__ src = static_cast<const T*>(a.src);
     T* __restrict__ out = static_cast<T*>(a.out);
     const int32_t* __restrict__ perm = (a.sel && *a.sel) ? a.perm1 : a.perm0;
@@ -396,29 +614,27 @@ __global__ void __launch_bounds__(kThreads) fold_kernel(FoldArgs a) {
                 f.take(src[pos], (pos / a.K) % a.E);
             }
         }
-        if (R == TCR_REDUCE_MEAN) {
-            T c = f.cnt;
-            if (Nm::lt(c, Nm::one())) c = Nm::one();
-            out[t] = Nm::div(f.acc, c);
-        } else if (R == TCR_REDUCE_MIN || R == TCR_REDUCE_MAX) {
-            T v = f.acc;
-            if (!a.accumulate && Nm::eq(v, reduce_init<T, R>())) v = Nm::zero();
-            out[t] = v;
-            a.arg[t] = f.arg;
-        } else {
-            out[t] = f.acc;
-        }
+        fold_write<T, R>(a, out, t, f);
     }
 }
 
+template <typename T, int R, int P>
+void launch_one(const FoldArgs& fa, unsigned grid, cudaStream_t st) {
+    if constexpr (P == 3)
+        fold_rows_kernel<T, R><<<grid, kThreads, 0, st>>>(fa);
+    else
+        fold_kernel<T, R, P><<<grid, kThreads, 0, st>>>(fa);
+}
+
+// P = 0, 1, 2: fold_kernel paths; P = 3: fold_rows_kernel (index over e, non-decreasing, K == 1).
 template <typename T, int P>
 cudaError_t launch_fold_r(int reduce, const FoldArgs& fa, unsigned grid, cudaStream_t st) {
     switch (reduce) {
-        case TCR_REDUCE_SUM: fold_kernel<T, TCR_REDUCE_SUM, P><<<grid, kThreads, 0, st>>>(fa); break;
-        case TCR_REDUCE_MEAN: fold_kernel<T, TCR_REDUCE_MEAN, P><<<grid, kThreads, 0, st>>>(fa); break;
-        case TCR_REDUCE_MUL: fold_kernel<T, TCR_REDUCE_MUL, P><<<grid, kThreads, 0, st>>>(fa); break;
-        case TCR_REDUCE_MIN: fold_kernel<T, TCR_REDUCE_MIN, P><<<grid, kThreads, 0, st>>>(fa); break;
-        default: fold_kernel<T, TCR_REDUCE_MAX, P><<<grid, kThreads, 0, st>>>(fa); break;
+        case TCR_REDUCE_SUM: launch_one<T, TCR_REDUCE_SUM, P>(fa, grid, st); break;
+        case TCR_REDUCE_MEAN: launch_one<T, TCR_REDUCE_MEAN, P>(fa, grid, st); break;
+        case TCR_REDUCE_MUL: launch_one<T, TCR_REDUCE_MUL, P>(fa, grid, st); break;
+        case TCR_REDUCE_MIN: launch_one<T, TCR_REDUCE_MIN, P>(fa, grid, st); break;
+        default: launch_one<T, TCR_REDUCE_MAX, P>(fa, grid, st); break;
     }
     return cudaGetLastError();
 }
@@ -462,6 +678,7 @@ struct Plan {
 };
 
 struct Work {
+    int64_t* stats;
     int64_t* off;
     int64_t* gaps;
     unsigned long long* ngaps;
@@ -474,6 +691,7 @@ struct Work {
 
 int64_t carve_work(const Plan& p, char* base, Work& w) {
     Carve c{base, 0};
+    w.stats = c.take<int64_t>(4);
     w.off = c.take<int64_t>(p.nslots + 1);
     w.gaps = c.take<int64_t>(3 * p.gap_cap);
     w.ngaps = c.take<unsigned long long>(1);
@@ -532,10 +750,10 @@ cudaError_t sort_path(const tcr_scatter_desc* d, const Plan& p, const Work& w, c
     sort_init_kernel<K><<<1, 1, 0, st>>>(state);
     if (p.path == 2)
         pack_keys_kernel<K, true><<<grid_for(p.M), kThreads, 0, st>>>(d->index, p.M, d->E, d->K, d->N, k0, w.vals[0],
-                                                                       state);
+                                                                       state, w.stats);
     else
         pack_keys_kernel<K, false><<<grid_for(p.M), kThreads, 0, st>>>(d->index, p.M, d->E, d->K, d->N, k0, w.vals[0],
-                                                                        state);
+                                                                        state, w.stats);
     note_launches(2);
     SortWorkspaceT<K> ws;
     ws.keys[0] = k0;
@@ -548,8 +766,9 @@ cudaError_t sort_path(const tcr_scatter_desc* d, const Plan& p, const Work& w, c
     cudaError_t e = radix_sort_pairs<K>(ws, p.M, st);
     if (e != cudaSuccess) return e;
     const int32_t* sel = &state->sel[key_passes<K>()];
-    mark_runs_kernel<K><<<grid_for(p.M), kThreads, 0, st>>>(k0, k1, sel, p.M, p.nslots, w.off, w.gaps, w.ngaps,
-                                                            p.gap_cap);
+    const unsigned mgrid = grid_resident(mark_runs_kernel<K, false>, (p.M + kMarkKeys - 1) / kMarkKeys);
+    mark_runs_kernel<K, false><<<mgrid, kThreads, 0, st>>>(k0, k1, sel, p.M, p.nslots, w.off, w.gaps, w.ngaps, p.gap_cap,
+                                                           w.stats);
     note_launches(1);
     return cudaGetLastError();
 }
@@ -587,7 +806,7 @@ int tcr_scatter_sizes(const tcr_scatter_desc* d, int64_t* scratch_bytes) {
     return TCR_OK;
 }
 
-int tcr_scatter(const tcr_scatter_desc* d, void* scratch, int64_t scratch_bytes, void* stream) {
+int tcr_scatter(const tcr_scatter_desc* d, void* scratch, int64_t scratch_bytes, int64_t* stats_host, void* stream) {
     Plan p;
     int rc = check_desc(d, p, true);
     if (rc) return rc;
@@ -606,10 +825,13 @@ int tcr_scatter(const tcr_scatter_desc* d, void* scratch, int64_t scratch_bytes,
         return set_error(TCR_ERR_INVALID, "tcr_scatter: scratch of %lld bytes, %lld needed", (long long)scratch_bytes,
                          (long long)need);
     carve_work(p, static_cast<char*>(scratch), w);
+    stats_init_kernel<<<1, 1, 0, st>>>(w.stats);
+    note_launches(1);
     TCR_SCATTER_CUDA(cudaMemsetAsync(w.ngaps, 0, sizeof(unsigned long long), st));
     if (p.path == 0) {
-        mark_runs_kernel<int64_t><<<grid_for(p.M), kThreads, 0, st>>>(d->index, nullptr, nullptr, p.M, p.nslots, w.off,
-                                                                      w.gaps, w.ngaps, p.gap_cap);
+        const unsigned mgrid = grid_resident(mark_runs_kernel<int64_t, true>, (p.M + kMarkKeys - 1) / kMarkKeys);
+        mark_runs_kernel<int64_t, true><<<mgrid, kThreads, 0, st>>>(d->index, nullptr, nullptr, p.M, p.nslots, w.off,
+                                                                    w.gaps, w.ngaps, p.gap_cap, w.stats);
         note_launches(1);
         TCR_SCATTER_CUDA(cudaGetLastError());
     } else if (p.wide) {
@@ -617,7 +839,8 @@ int tcr_scatter(const tcr_scatter_desc* d, void* scratch, int64_t scratch_bytes,
     } else {
         TCR_SCATTER_CUDA(sort_path<uint32_t>(d, p, w, st));
     }
-    fill_gaps_kernel<<<grid_for((p.nslots + 1) / 4), kThreads, 0, st>>>(w.gaps, w.ngaps, p.gap_cap, w.off);
+    fill_gaps_kernel<<<grid_for((p.nslots + 1) / 4), kThreads, 0, st>>>(w.gaps, w.ngaps, p.gap_cap, w.off, w.stats,
+                                                                         p.path == 0 ? 1 : 0);
     note_launches(1);
     TCR_SCATTER_CUDA(cudaGetLastError());
 
@@ -632,17 +855,26 @@ int tcr_scatter(const tcr_scatter_desc* d, void* scratch, int64_t scratch_bytes,
     if (p.path != 0)
         fa.sel = p.wide ? &static_cast<SortState64*>(w.state)->sel[key_passes<unsigned long long>()]
                         : &static_cast<SortState32*>(w.state)->sel[key_passes<uint32_t>()];
+    fa.stats = w.stats;
     fa.B = d->B;
     fa.E = d->E;
     fa.K = d->K;
     fa.N = d->N;
     fa.accumulate = d->accumulate;
-    const unsigned grid = grid_for(nout);
-    cudaError_t e = p.path == 0   ? launch_fold<0>(d->dtype, d->reduce, fa, grid, st)
-                    : p.path == 1 ? launch_fold<1>(d->dtype, d->reduce, fa, grid, st)
-                                  : launch_fold<2>(d->dtype, d->reduce, fa, grid, st);
+    cudaError_t e;
+    if (p.path == 0 && d->K == 1) {
+        const int64_t rows = d->B * ((d->N + kThreads - 1) / kThreads);
+        e = launch_fold<3>(d->dtype, d->reduce, fa, grid_for(rows * kThreads), st);
+    } else {
+        const unsigned grid = grid_for(nout);
+        e = p.path == 0   ? launch_fold<0>(d->dtype, d->reduce, fa, grid, st)
+            : p.path == 1 ? launch_fold<1>(d->dtype, d->reduce, fa, grid, st)
+                          : launch_fold<2>(d->dtype, d->reduce, fa, grid, st);
+    }
     note_launches(1);
     TCR_SCATTER_CUDA(e);
+    if (stats_host)
+        TCR_SCATTER_CUDA(cudaMemcpyAsync(stats_host, w.stats, 3 * sizeof(int64_t), cudaMemcpyDeviceToHost, st));
     return TCR_OK;
 }
 

@@ -93,19 +93,21 @@ def _scatter(src: torch.Tensor, index: torch.Tensor, dim: int, out: Optional[tor
         idx_d = idx_d[sel].contiguous()
     else:
         idx_d = idx_d.contiguous().reshape(-1)
+    nel = B * E * K
     with torch.cuda.device(device):
         stream = torch.cuda.current_stream(device)
-        lo, hi, descents = index_stats(idx_d, stream) if idx_d.numel() > 0 else (0, -1, 0)
+        known = out is not None or dim_size is not None
         if out is not None:
             N = out.size(dim)
         elif dim_size is not None:
             N = int(dim_size)
-        else:
+        else:  # the size comes from the index: read its statistics first (the reference's index.max())
+            lo, hi, descents = index_stats(idx_d, stream) if idx_d.numel() > 0 else (0, -1, 0)
             N = 0 if index_b.numel() == 0 else hi + 1
         if N < 0:
             raise RuntimeError(f"dim_size {N} is negative")
-        if idx_d.numel() > 0 and (lo < 0 or hi >= N) and B * E * K > 0:
-            raise IndexError(f"index values must lie in [0, {N}) (found {lo} .. {hi})")
+        if nel > 0 and N == 0:
+            raise IndexError("index values must lie in [0, 0): the output is empty")
         shape[dim] = N
         if out is not None:
             out_d = out.detach()
@@ -119,16 +121,38 @@ def _scatter(src: torch.Tensor, index: torch.Tensor, dim: int, out: Optional[tor
         d.reduce = _lib.REDUCE[reduce]
         d.dtype = DTYPES[src.dtype]
         d.index_full = 0 if one_d else 1
-        d.index_sorted = 1 if (one_d and descents == 0) else 0
         d.accumulate = 1 if out is not None else 0
         d.B, d.E, d.K, d.N = B, E, K, N
         d.src = src_d.data_ptr() if src_d.numel() else None
         d.index = idx_d.data_ptr() if idx_d.numel() else None
         d.out = out_d.data_ptr() if out_d.numel() else None
         d.arg_out = arg_d.data_ptr() if (arg_d is not None and arg_d.numel()) else None
-        scratch = torch.empty(max(_lib.scatter_sizes(d), 1), dtype=torch.uint8, device=device)
-        _lib.check(_lib.load().tcr_scatter(ctypes.byref(d), _ptr(scratch), scratch.numel(),
-                                           ctypes.c_void_p(stream.cuda_stream)), "tcr_scatter")
+        lib = _lib.load()
+        sp = ctypes.c_void_p(stream.cuda_stream)
+
+        def call(index_sorted, stats_host):
+            d.index_sorted = index_sorted
+            scratch = torch.empty(max(_lib.scatter_sizes(d), 1), dtype=torch.uint8, device=device)
+            _lib.check(lib.tcr_scatter(ctypes.byref(d), _ptr(scratch), scratch.numel(), stats_host, sp),
+                       "tcr_scatter")
+
+        if nel == 0:
+            call(0, None)
+        elif known:
+            # One pass when the index is in order (the rows of a neighbour list): the kernels check
+            # it while reading it and write nothing when it descends or leaves [0, N).
+            host = torch.empty(3, dtype=torch.int64, pin_memory=True)
+            call(1 if one_d else 0, ctypes.c_void_p(host.data_ptr()))
+            stream.synchronize()
+            lo, hi, descents = int(host[0]), int(host[1]), int(host[2])
+            if lo < 0 or hi >= N:
+                raise IndexError(f"index values must lie in [0, {N}) (found {lo} .. {hi})")
+            if one_d and descents > 0:
+                call(0, None)
+        else:
+            if lo < 0:
+                raise IndexError(f"index values must lie in [0, {N}) (found {lo} .. {hi})")
+            call(1 if (one_d and descents == 0) else 0, None)
     if out is not None:
         if out_d.data_ptr() != out.data_ptr():
             out.copy_(out_d)
