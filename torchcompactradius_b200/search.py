@@ -8,6 +8,7 @@ only the emit when the estimate was short.  Device memory comes from torch's cac
 """
 import ctypes
 import threading
+import warnings
 from typing import Optional
 
 import torch
@@ -38,8 +39,21 @@ def _require_cuda(device):
     return device
 
 
+_warned_f64 = False
+
+
 def _as_f32(t, device, shape=None):
+    """Positions and supports as contiguous float32 on the device.  The search computes in float32
+    (the reference's float path); a float64 input is rounded to float32 first, with one warning per
+    process, since the reference searches float64 inputs in double and pairs whose distance lies
+    within float32 rounding of the threshold can then differ."""
+    global _warned_f64
     t = torch.as_tensor(t)
+    if t.dtype == torch.float64 and not _warned_f64:
+        _warned_f64 = True
+        warnings.warn("torchcompactradius_b200 searches in float32: float64 positions / supports are rounded to "
+                      "float32 (pairs within float32 rounding of the threshold may differ from a float64 search)",
+                      stacklevel=3)
     t = t.to(device=device, dtype=torch.float32)
     return t.contiguous()
 
