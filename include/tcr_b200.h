@@ -252,6 +252,38 @@ int tcr_search_noalloc(const tcr_search_desc* d, int64_t* offsets, int32_t* indp
                        int64_t* row_out, int64_t* col_out, int64_t pair_capacity, int64_t* total_out, void* stream);
 
 /* ---------------------------------------------------------------------------------------------
+ * Float64 inputs.  The reference's operators dispatch on float and double
+ * (cppSrc/neighborhoodDynamic_cpu.cpp:504,531); for double positions it computes cell indices,
+ * moduloOp, the squared sum, sqrt and the threshold in double.  These two calls replace tcr_count /
+ * tcr_emit for such inputs.  The structure is built by tcr_build_structure from float32 copies of
+ * the wrapped positions and supports, with hcell set to a cell size no smaller than the reference's
+ * double hCell (so every pair within the double support lies in a query's 3^d stencil); each
+ * candidate is then decided on the double arrays below by the reference's double expression.
+ * ------------------------------------------------------------------------------------------- */
+typedef struct tcr_f64_inputs {
+    const double* query_pos;  /* device [n_query*dim], wrapped as the reference wraps queries
+                                 (util.py:375-387) */
+    const double* query_sup;  /* device [n_query]; may be NULL for TCR_SCATTER */
+    const double* ref_pos;    /* device [n_ref*dim], wrapped as the reference wraps references
+                                 (util.py:375-387, then compactHashing/cppSearch.py:221) */
+    const double* ref_sup;    /* device [n_ref]; may be NULL for TCR_GATHER */
+    double domain_min[3];     /* the domain in double: periodic differences use max - min */
+    double domain_max[3];
+} tcr_f64_inputs;
+
+/* countNeighbors at scalar_t = double (neighborhoodDynamic.h:37-74) + the offsets scan; d describes
+ * the float32 copies the structure was built from (hcell > 0, clamped_grid 0). */
+int tcr_count_f64(const tcr_search_desc* d, const tcr_f64_inputs* in, const void* structure, void* scratch,
+                  int64_t scratch_bytes, int64_t* offsets, int32_t* indptr_out, int64_t* row_entries_out,
+                  int64_t* info_out, void* stream);
+
+/* buildNeighborList at scalar_t = double (neighborhoodDynamic.h:76-115): writes each query's pairs
+ * from offsets[q] in stencil order. */
+int tcr_emit_f64(const tcr_search_desc* d, const tcr_f64_inputs* in, const void* structure, void* scratch,
+                 int64_t scratch_bytes, const int64_t* offsets, int64_t* row_out, int64_t* col_out,
+                 int64_t out_capacity, void* stream);
+
+/* ---------------------------------------------------------------------------------------------
  * Reductions of values onto an index: the reference's scatter operators scatter_sum, scatter_mul,
  * scatter_mean, scatter_min and scatter_max (src/torchCompactRadius/cppSrc/sparseOperations/
  * scatter.h:10-36, registered in cppSrc/cppWrapper.cpp:54-58; forward scatter_cpu.cpp:7-85 and

@@ -77,6 +77,18 @@ class BatchDesc(ctypes.Structure):
     ]
 
 
+class F64Inputs(ctypes.Structure):
+    """tcr_f64_inputs (include/tcr_b200.h): the double arrays of a float64 search."""
+    _fields_ = [
+        ("query_pos", ctypes.c_void_p),
+        ("query_sup", ctypes.c_void_p),
+        ("ref_pos", ctypes.c_void_p),
+        ("ref_sup", ctypes.c_void_p),
+        ("domain_min", ctypes.c_double * 3),
+        ("domain_max", ctypes.c_double * 3),
+    ]
+
+
 class ScatterDesc(ctypes.Structure):
     """tcr_scatter_desc (include/tcr_b200.h): one reduction of values onto an index."""
     _fields_ = [
@@ -124,6 +136,8 @@ SIGNATURES = {
     "tcr_batch_count": (ctypes.c_int, [_batch_p, _vp, _vp, _i64, _vp, _i64, _vp, _vp, _vp, _vp, _vp]),
     "tcr_batch_emit": (ctypes.c_int, [_batch_p, _vp, _vp, _i64, _vp, _vp, _vp, _vp, _i64, _vp]),
     "tcr_search_noalloc": (ctypes.c_int, [_desc_p, _vp, _vp, _vp, _vp, _vp, _i64, ctypes.POINTER(_i64), _vp]),
+    "tcr_count_f64": (ctypes.c_int, [_desc_p, ctypes.POINTER(F64Inputs), _vp, _vp, _i64, _vp, _vp, _vp, _vp, _vp]),
+    "tcr_emit_f64": (ctypes.c_int, [_desc_p, ctypes.POINTER(F64Inputs), _vp, _vp, _i64, _vp, _vp, _vp, _i64, _vp]),
     "tcr_scatter_desc_bytes": (_i64, []),
     "tcr_index_stats": (ctypes.c_int, [_vp, _i64, _vp, _vp, _vp]),
     "tcr_scatter_sizes": (ctypes.c_int, [_scatter_p, ctypes.POINTER(_i64)]),

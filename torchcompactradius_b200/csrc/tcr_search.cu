@@ -1819,6 +1819,100 @@ __global__ void stray_kernel(WalkArgs a) {
     }
 }
 
+// ------------------------------------------------------------------------------------------
+// float64 inputs (the reference dispatches its operators on float and double,
+// neighborhoodDynamic_cpu.cpp:504,531).  The structure is built from float32 copies with a cell
+// size no smaller than the reference's double one, so every pair within the double support lies
+// in the query's 3^d stencil; each candidate is then decided on the caller's double positions and
+// supports by the reference's double expression.
+struct F64Args {
+    const double* qpos;  // [nq * dim], wrapped as the reference wraps queries
+    const double* qsup;  // [nq] or null
+    const double* rpos;  // [nr * dim], reference j at row j, wrapped as the reference wraps references
+    const double* rsup;  // [nr] or null
+    double ext[3];       // max - min of the domain, in double
+    int64_t nq;
+};
+
+// common.h:106-129 and neighborhoodDynamic.h:59-70 at scalar_t = double: per dimension
+// diff = moduloOp(x_i, x_j, max - min) = ((x_i - x_j + h/2) - floor((x_i - x_j + h/2) / h) * h) - h/2
+// on periodic dimensions, x_i - x_j otherwise; sum += diff * diff; sqrt(sum) < the mode's
+// threshold.  Explicit intrinsics keep every operation rounded on its own (no FMA).
+__device__ __noinline__ bool f64_pair_test(int dim, int mask, int mode, const double* ext, const double* xi,
+                                           double hi, const double* xj, double hj) {
+    double sum = 0.0;
+    for (int d = 0; d < dim; ++d) {
+        double diff;
+        if ((mask >> d) & 1) {
+            const double h = ext[d];
+            const double half = __ddiv_rn(h, 2.0);
+            const double t = __dadd_rn(__dsub_rn(xi[d], xj[d]), half);
+            diff = __dsub_rn(__dsub_rn(t, __dmul_rn(floor(__ddiv_rn(t, h)), h)), half);
+        } else {
+            diff = __dsub_rn(xi[d], xj[d]);
+        }
+        sum = __dadd_rn(sum, __dmul_rn(diff, diff));
+    }
+    const double dist = __dsqrt_rn(sum);
+    double thr;
+    switch (mode) {
+        case kGather: thr = hi; break;
+        case kScatter: thr = hj; break;
+        case kSymmetric: thr = __ddiv_rn(__dadd_rn(hi, hj), 2.0); break;
+        default: thr = hi < hj ? hj : hi; break;  // std::max
+    }
+    return dist < thr;
+}
+
+// One thread per query, in the caller's query order: the query's cell from its float32 copy, the
+// 3^d stencil of the structure, every candidate tested in double.  Count pass (EMIT = false)
+// writes counts[q]; emit pass writes the row's pairs from offsets[q] in stencil order.
+template <bool EMIT>
+__global__ void __launch_bounds__(128) f64_walk_kernel(WalkArgs a, F64Args f) {
+    UnitCtx u;
+    load_unit_ctx(u, a, 0);
+    const CloudParams& cp = a.table[0];
+    const int S = u.dim == 1 ? 3 : (u.dim == 2 ? 9 : 27);
+    const int dim = u.dim;
+    for (int64_t q = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; q < f.nq; q += (int64_t)gridDim.x * blockDim.x) {
+        if (u.error) {
+            if (!EMIT) a.counts[q] = 0;
+            continue;
+        }
+        const float4 qf = wrap_point(cp.dim, cp.periodic_mask, cp.dmin, cp.ext,
+                                     load_point(cp.query_pos, cp.query_sup, q, cp.dim), 1);
+        int32_t qc[3];
+        cell_of(u.dim, u.dedupe, u.dmin, u.hcell, u.count, qf, qc);
+        double xi[3] = {0.0, 0.0, 0.0};
+        for (int d = 0; d < dim; ++d) xi[d] = f.qpos[q * dim + d];
+        const double hi = f.qsup ? f.qsup[q] : 0.0;
+        int64_t pos = EMIT ? a.offsets[q] : 0;
+        int32_t n = 0;
+        for (int o = 0; o < S; ++o) {
+            int32_t beg, cnt;
+            stencil_lookup(a, u, qc, o, beg, cnt);
+            for (int32_t j = beg; j < beg + cnt; ++j) {
+                const int32_t jl = a.rsidx[j];
+                double xj[3] = {0.0, 0.0, 0.0};
+                for (int d = 0; d < dim; ++d) xj[d] = f.rpos[(int64_t)jl * dim + d];
+                const double hj = f.rsup ? f.rsup[jl] : 0.0;
+                if (f64_pair_test(dim, u.periodic_mask, a.mode, f.ext, xi, hi, xj, hj)) {
+                    if (EMIT) {
+                        if (pos < a.out_cap) {
+                            a.col_out[pos] = (int64_t)(a.ref_ids ? a.ref_ids[jl] : jl - u.rshift);
+                            if (a.row_out) a.row_out[pos] = a.query_ids ? a.query_ids[q] : q - u.qshift;
+                        }
+                        ++pos;
+                    } else {
+                        ++n;
+                    }
+                }
+            }
+        }
+        if (!EMIT) a.counts[q] = n;
+    }
+}
+
 // counts -> offsets (int64, nq+1), optional CSR indptr (int32) and rowEntries (int64).
 struct CountIn {
     const int32_t* counts;
@@ -2549,6 +2643,95 @@ int tcr_emit(const tcr_search_desc* d, const void* structure, void* scratch, int
     int rc = batch_of_desc(d, 1, b);
     if (rc) return rc;
     return run_emit(b, structure, scratch, scratch_bytes, stage, offsets, row_out, col_out, out_capacity, stream);
+}
+
+static int f64_args(const tcr_search_desc* d, const tcr_f64_inputs* in, F64Args& f) {
+    if (!in) return set_error(TCR_ERR_INVALID, "missing float64 inputs");
+    if ((d->n_query > 0 && !in->query_pos) || (d->n_ref > 0 && !in->ref_pos))
+        return set_error(TCR_ERR_INVALID, "missing float64 positions");
+    if (d->mode != TCR_SCATTER && d->n_query > 0 && !in->query_sup)
+        return set_error(TCR_ERR_INVALID, "this mode needs float64 query supports");
+    if (d->mode != TCR_GATHER && d->n_ref > 0 && !in->ref_sup)
+        return set_error(TCR_ERR_INVALID, "this mode needs float64 reference supports");
+    if (d->hcell[0] <= 0.0f) return set_error(TCR_ERR_INVALID, "float64 searches need the cell size in hcell");
+    if (d->clamped_grid) return set_error(TCR_ERR_INVALID, "float64 searches use the reference's unclamped grid");
+    f.qpos = in->query_pos;
+    f.qsup = in->query_sup;
+    f.rpos = in->ref_pos;
+    f.rsup = in->ref_sup;
+    for (int k = 0; k < 3; ++k) f.ext[k] = in->domain_max[k] - in->domain_min[k];
+    f.nq = d->n_query;
+    return TCR_OK;
+}
+
+int tcr_count_f64(const tcr_search_desc* d, const tcr_f64_inputs* in, const void* structure, void* scratch,
+                  int64_t scratch_bytes, int64_t* offsets, int32_t* indptr_out, int64_t* row_entries_out,
+                  int64_t* info_out, void* stream) {
+    HostBatch b;
+    int rc = batch_of_desc(d, 1, b);
+    if (rc) return rc;
+    F64Args f;
+    rc = f64_args(d, in, f);
+    if (rc) return rc;
+    int64_t need_w = 0;
+    batch_sizes(b, nullptr, &need_w);
+    if (!structure || !scratch || scratch_bytes < need_w || !offsets)
+        return set_error(TCR_ERR_INVALID, "workspace too small or offsets missing");
+    const Structure S = carve_structure(const_cast<void*>(structure), b.nr, b.C, b.map_total, nullptr);
+    const Scratch W = carve_scratch(scratch, b.nq, b.nr, b.C, false, nullptr);
+    cudaStream_t st = (cudaStream_t)stream;
+    rc = upload_table(b, W, st);
+    if (rc) return rc;
+    count_init_kernel<<<1, 128, 0, st>>>(W, b.C, g_unit_cap);
+    query_params_kernel<<<1, 128, 0, st>>>(W.table, S.grid, b.C, W.qparams, W.exact_clouds);
+    note_launches(2);
+    const int64_t nq = b.nq;
+    if (nq > 0) {
+        WalkArgs a = make_walk(b, S, W);
+        f64_walk_kernel<false><<<grid_for(nq, 128, num_sms() * 8), 128, 0, st>>>(a, f);
+        note_launches(1);
+    }
+    CountIn ci{W.counts, nq};
+    OffsetOut oo{nq, offsets, indptr_out, row_entries_out};
+    TCR_CUDA(device_exclusive_scan<int64_t>(ci, oo, nq + 1, W.scan_tiles64, W.total, st));
+    info_kernel<<<1, 1, 0, st>>>(S.bad_grids, W.total, W.num_stray, W.exact_clouds, W.cursor, W.num_flagged,
+                                 W.num_exact, nullptr, b.nr, W.info);
+    note_launches(1);
+    if (info_out) TCR_CUDA(cudaMemcpyAsync(info_out, W.info, 8 * sizeof(int64_t), cudaMemcpyDeviceToHost, st));
+    TCR_CUDA(cudaGetLastError());
+    return TCR_OK;
+}
+
+int tcr_emit_f64(const tcr_search_desc* d, const tcr_f64_inputs* in, const void* structure, void* scratch,
+                 int64_t scratch_bytes, const int64_t* offsets, int64_t* row_out, int64_t* col_out,
+                 int64_t out_capacity, void* stream) {
+    HostBatch b;
+    int rc = batch_of_desc(d, 1, b);
+    if (rc) return rc;
+    F64Args f;
+    rc = f64_args(d, in, f);
+    if (rc) return rc;
+    int64_t need_w = 0;
+    batch_sizes(b, nullptr, &need_w);
+    if (!structure || !scratch || scratch_bytes < need_w || !offsets)
+        return set_error(TCR_ERR_INVALID, "workspace too small or offsets missing");
+    if (out_capacity < 0 || (out_capacity > 0 && !col_out)) return set_error(TCR_ERR_INVALID, "bad output buffer");
+    const Structure S = carve_structure(const_cast<void*>(structure), b.nr, b.C, b.map_total, nullptr);
+    const Scratch W = carve_scratch(scratch, b.nq, b.nr, b.C, false, nullptr);
+    cudaStream_t st = (cudaStream_t)stream;
+    rc = upload_table(b, W, st);
+    if (rc) return rc;
+    const int64_t nq = b.nq;
+    if (nq <= 0) return TCR_OK;
+    WalkArgs a = make_walk(b, S, W);
+    a.offsets = offsets;
+    a.row_out = row_out;
+    a.col_out = col_out;
+    a.out_cap = out_capacity;
+    f64_walk_kernel<true><<<grid_for(nq, 128, num_sms() * 8), 128, 0, st>>>(a, f);
+    note_launches(1);
+    TCR_CUDA(cudaGetLastError());
+    return TCR_OK;
 }
 
 int tcr_batch_sizes(const tcr_batch_desc* bd, int64_t* structure_bytes, int64_t* scratch_bytes) {

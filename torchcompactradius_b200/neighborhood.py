@@ -75,6 +75,14 @@ def radiusSearch(queryPointCloud: PointCloud, referencePointCloud: Optional[Poin
             print(f"radiusSearch: {qpos.shape[0]} queries, {rpos.shape[0]} references, dim {dim}, mode {mode}, "
                   f"periodic mask {mask}, hashMapLength {hashMapLength}, format {format}")
         nq, nr = qpos.shape[0], rpos.shape[0]
+        if (qpos.dtype == torch.float64 or rpos.dtype == torch.float64) and algorithm != "mlm":
+            out = _radius_search_f64(queryPointCloud, referencePointCloud, supportOverride, mode, domain, lo, hi, mask,
+                                     hashMapLength, format, self_cloud, returnStructure, device)
+            if in_device.type != "cuda":
+                out = tuple(None if t is None else t.to(in_device) for t in out)
+            if format == "coo":
+                return SparseCOO(out[0], out[1], nq, nr)
+            return SparseCSR(out[0], out[1], out[2], nq, nr)
         xq = _as_f32(qpos, device)
         same = self_cloud or (rpos.data_ptr() == qpos.data_ptr() and rpos.shape == qpos.shape
                               and rpos.stride() == qpos.stride() and rpos.dtype == qpos.dtype)
@@ -107,6 +115,42 @@ def radiusSearch(queryPointCloud: PointCloud, referencePointCloud: Optional[Poin
         if returnStructure:
             return adj, ds
         return adj
+
+
+def _radius_search_f64(q: PointCloud, r: PointCloud, supportOverride, mode, domain, lo, hi, mask, L, fmt, self_cloud,
+                       returnStructure, device):
+    """Float64 positions: the reference's double search (search64.py).  Positions, supports and the
+    domain must all be float64, as the reference's double operators require (their accessors raise
+    otherwise)."""
+    from .search64 import compact_search_f64
+    if returnStructure:
+        raise ValueError("returnStructure is not available for float64 inputs")
+    need = [("positions", q.positions), ("positions", r.positions), ("domain.min", domain.min),
+            ("domain.max", domain.max)]
+    if supportOverride is None:
+        if mode != "scatter":
+            need.append(("supports", q.supports))
+        if mode != "gather":
+            need.append(("supports", r.supports))
+    for name, t in need:
+        if t is None:
+            continue
+        if torch.as_tensor(t).dtype != torch.float64:
+            raise RuntimeError(f"expected scalar type Double but found Float ({name} of a float64 search)")
+    xq = q.positions.to(device=device, dtype=torch.float64).contiguous()
+    xr = xq if self_cloud else r.positions.to(device=device, dtype=torch.float64).contiguous()
+    if supportOverride is not None:
+        hq = torch.full((xq.shape[0],), supportOverride, dtype=torch.float64, device=device)
+        hr = hq if self_cloud else torch.full((xr.shape[0],), supportOverride, dtype=torch.float64, device=device)
+    else:
+        hq = None if q.supports is None else q.supports.to(device=device, dtype=torch.float64).contiguous()
+        hr = None if r.supports is None else (hq if self_cloud else
+                                              r.supports.to(device=device, dtype=torch.float64).contiguous())
+    if mode in ("gather", "symmetric", "superSymmetric"):
+        assert hq is not None, f"queryParticleSupports must be provided for {mode} mode"
+    if mode in ("scatter", "symmetric", "superSymmetric"):
+        assert hr is not None, f"referenceSupports must be provided for {mode} mode"
+    return compact_search_f64(xq, hq, xr, hr, lo, hi, mask, mode, L, fmt, self_cloud)
 
 
 def neighborSearchExisting(queryPointCloud: PointCloud, hashMap: CompactHashMap, mode: str = "symmetric",
