@@ -698,6 +698,53 @@ def tcr_launches():
     return int(_lib.load().tcr_kernel_launches())
 
 
+def bench_f64(dev, flush, steps=3, cpu=True):
+    """The 1M-point workload in float64 (positions, supports and domain): the reference's double
+    search, symmetric CSR, timed per search with events (L2 flushed), and the reference's own double
+    operators on the host beside it."""
+    import torch
+
+    import torchcompactradius_b200 as tcr
+    pos, sup = make_workload()
+    x, h = pos.double().to(dev), sup.double().to(dev)
+    dom = tcr.DomainDescription(torch.full((3,), -1.0, dtype=torch.float64), torch.full((3,), 1.0, dtype=torch.float64),
+                                torch.zeros(3, dtype=torch.bool), 3)
+    stream = torch.cuda.current_stream(dev)
+    adj = tcr.radiusSearch(tcr.PointCloud(x, h), None, mode="symmetric", domain=dom, algorithm="compact", format="csr")
+    ms = []
+    for k in range(steps):
+        flush.fill_(k & 0xff)
+        s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        s.record(stream)
+        adj = tcr.radiusSearch(tcr.PointCloud(x, h), None, mode="symmetric", domain=dom, algorithm="compact",
+                               format="csr")
+        e.record(stream)
+        e.synchronize()
+        ms.append(s.elapsed_time(e))
+    pairs = int(adj.indices.numel())
+    res = {"workload": "3d_1m_uniform_symmetric_csr in float64 (positions, supports, domain)", "pairs": pairs,
+           "ms_per_search": statistics.median(ms), "value": pairs / (statistics.median(ms) / 1e3), "unit": "pairs/s",
+           "note": "one thread per query, every stencil candidate tested in double"}
+    if cpu:
+        try:
+            from oracle import ref_pipeline
+            if ref_pipeline.available():
+                torch.set_num_threads(os.cpu_count() or 1)
+                t0 = time.perf_counter()
+                ref = ref_pipeline.radius_search(pos.double(), sup.double(), None, None, [-1.0] * 3, [1.0] * 3,
+                                                 [False] * 3, "symmetric", 4096, "csr", dtype=torch.float64)
+                dt = time.perf_counter() - t0
+                res["cpu_baseline"] = {"value": int(ref[0].numel()) / dt, "unit": "pairs/s",
+                                       "cores": torch.get_num_threads(), "kind": "reference",
+                                       "sample": "the full workload in float64, one run", "seconds": dt,
+                                       "pairs_match": int(ref[0].numel()) == pairs,
+                                       "indptr_match": bool(torch.equal(ref[1].to(torch.int64),
+                                                                        adj.indptr.cpu().to(torch.int64)))}
+        except Exception as ex:
+            res["cpu_baseline"] = {"unavailable": str(ex)}
+    return res
+
+
 def cpu_baseline_batched(clouds, budget_s=12.0):
     """The reference's own CPU search, one call per cloud (its batched radius() fails), over the
     first clouds of the workload until about budget_s seconds have passed."""
@@ -915,6 +962,7 @@ def run_b200(args):
         line["graphs"] = bench_graphs(dev, flush)
         line["adaptive"] = bench_adaptive(dev, flush)
         line["scatter"] = bench_scatter(dev, flush)
+        line["f64"] = bench_f64(dev, flush, cpu=rank == 0 and not args.no_cpu_baseline)
         del flush
         line["served"] = bench_served(dev)
     if world > 1:

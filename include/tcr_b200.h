@@ -267,6 +267,8 @@ typedef struct tcr_f64_inputs {
     const double* ref_pos;    /* device [n_ref*dim], wrapped as the reference wraps references
                                  (util.py:375-387, then compactHashing/cppSearch.py:221) */
     const double* ref_sup;    /* device [n_ref]; may be NULL for TCR_GATHER */
+    double* ref_sorted;       /* device workspace [n_ref*4] (32-byte aligned): tcr_count_f64 writes the
+                                 references in cell order there, tcr_emit_f64 reads them */
     double domain_min[3];     /* the domain in double: periodic differences use max - min */
     double domain_max[3];
 } tcr_f64_inputs;

@@ -108,22 +108,24 @@ def build_structure(x, hMax, minD, maxD, hashMapLength):
     return sortedPositions, hashTable, sortedCellTable.contiguous(), hCell, cellCount, sortIndex
 
 
-def radius_search(xq, hq, xr, hr, dmin, dmax, periodic, mode="gather", hashMapLength=4096, fmt="coo"):
+def radius_search(xq, hq, xr, hr, dmin, dmax, periodic, mode="gather", hashMapLength=4096, fmt="coo",
+                  dtype=torch.float32):
     """radiusSearch(PointCloud(xq,hq), PointCloud(xr,hr), mode=mode, domain=(dmin,dmax,periodic),
-    hashMapLength=..., algorithm='compact', format=fmt) on CPU tensors.
+    hashMapLength=..., algorithm='compact', format=fmt) on CPU tensors of ``dtype`` (the reference's
+    operators run at float or double).
 
     Returns ``(row, col)`` for COO or ``(indices, indptr, rowEntries)`` for CSR, exactly as the
     reference's SparseCOO / SparseCSR fields.
     """
     with torch.no_grad():
-        xq = torch.as_tensor(xq, dtype=torch.float32)
-        hq = None if hq is None else torch.as_tensor(hq, dtype=torch.float32)
+        xq = torch.as_tensor(xq, dtype=dtype)
+        hq = None if hq is None else torch.as_tensor(hq, dtype=dtype)
         if xr is None:  # neighborhood.py:187-188: the query cloud doubles as the reference cloud
             xr, hr = xq, hq
-        xr = torch.as_tensor(xr, dtype=torch.float32)
-        hr = None if hr is None else torch.as_tensor(hr, dtype=torch.float32)
-        dmin = torch.as_tensor(dmin, dtype=torch.float32)
-        dmax = torch.as_tensor(dmax, dtype=torch.float32)
+        xr = torch.as_tensor(xr, dtype=dtype)
+        hr = None if hr is None else torch.as_tensor(hr, dtype=dtype)
+        dmin = torch.as_tensor(dmin, dtype=dtype)
+        dmax = torch.as_tensor(dmax, dtype=dtype)
         periodic = torch.as_tensor(periodic, dtype=torch.bool)
         nq, nr = xq.shape[0], xr.shape[0]
         x = _wrap(xq, dmin, dmax, periodic)                  # neighborhood.py:202

@@ -84,6 +84,7 @@ class F64Inputs(ctypes.Structure):
         ("query_sup", ctypes.c_void_p),
         ("ref_pos", ctypes.c_void_p),
         ("ref_sup", ctypes.c_void_p),
+        ("ref_sorted", ctypes.c_void_p),
         ("domain_min", ctypes.c_double * 3),
         ("domain_max", ctypes.c_double * 3),
     ]

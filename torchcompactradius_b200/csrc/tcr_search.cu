@@ -1830,9 +1830,23 @@ struct F64Args {
     const double* qsup;  // [nq] or null
     const double* rpos;  // [nr * dim], reference j at row j, wrapped as the reference wraps references
     const double* rsup;  // [nr] or null
+    double4* rsorted;    // [nr] the references in the structure's cell order, .w = support
     double ext[3];       // max - min of the domain, in double
-    int64_t nq;
+    int64_t nq, nr;
+    int32_t self_order;  // queries are the references: walk them in cell order (rsidx)
 };
+
+// The double references in cell order, so that a stencil cell's candidates are one contiguous run.
+__global__ void f64_sort_refs_kernel(const int32_t* __restrict__ rsidx, F64Args f, int dim) {
+    for (int64_t j = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; j < f.nr; j += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t jl = rsidx[j];
+        double4 v = make_double4(0.0, 0.0, 0.0, f.rsup ? f.rsup[jl] : 0.0);
+        v.x = f.rpos[jl * dim];
+        if (dim > 1) v.y = f.rpos[jl * dim + 1];
+        if (dim > 2) v.z = f.rpos[jl * dim + 2];
+        f.rsorted[j] = v;
+    }
+}
 
 // common.h:106-129 and neighborhoodDynamic.h:59-70 at scalar_t = double: per dimension
 // diff = moduloOp(x_i, x_j, max - min) = ((x_i - x_j + h/2) - floor((x_i - x_j + h/2) / h) * h) - h/2
@@ -1864,9 +1878,10 @@ __device__ __noinline__ bool f64_pair_test(int dim, int mask, int mode, const do
     return dist < thr;
 }
 
-// One thread per query, in the caller's query order: the query's cell from its float32 copy, the
-// 3^d stencil of the structure, every candidate tested in double.  Count pass (EMIT = false)
-// writes counts[q]; emit pass writes the row's pairs from offsets[q] in stencil order.
+// One thread per query: the query's cell from its float32 copy, the 3^d stencil of the structure,
+// every candidate tested in double.  A self search walks the queries in cell order, so the threads
+// of a warp share stencils and read the same candidate runs.  Count pass (EMIT = false) writes
+// counts[q]; emit pass writes the row's pairs from offsets[q] in stencil order.
 template <bool EMIT>
 __global__ void __launch_bounds__(128) f64_walk_kernel(WalkArgs a, F64Args f) {
     UnitCtx u;
@@ -1874,7 +1889,8 @@ __global__ void __launch_bounds__(128) f64_walk_kernel(WalkArgs a, F64Args f) {
     const CloudParams& cp = a.table[0];
     const int S = u.dim == 1 ? 3 : (u.dim == 2 ? 9 : 27);
     const int dim = u.dim;
-    for (int64_t q = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; q < f.nq; q += (int64_t)gridDim.x * blockDim.x) {
+    for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < f.nq; t += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t q = f.self_order ? (int64_t)a.rsidx[t] : t;
         if (u.error) {
             if (!EMIT) a.counts[q] = 0;
             continue;
@@ -1892,11 +1908,10 @@ __global__ void __launch_bounds__(128) f64_walk_kernel(WalkArgs a, F64Args f) {
             int32_t beg, cnt;
             stencil_lookup(a, u, qc, o, beg, cnt);
             for (int32_t j = beg; j < beg + cnt; ++j) {
-                const int32_t jl = a.rsidx[j];
-                double xj[3] = {0.0, 0.0, 0.0};
-                for (int d = 0; d < dim; ++d) xj[d] = f.rpos[(int64_t)jl * dim + d];
-                const double hj = f.rsup ? f.rsup[jl] : 0.0;
-                if (f64_pair_test(dim, u.periodic_mask, a.mode, f.ext, xi, hi, xj, hj)) {
+                const double4 c = f.rsorted[j];
+                const double xj[3] = {c.x, c.y, c.z};
+                if (f64_pair_test(dim, u.periodic_mask, a.mode, f.ext, xi, hi, xj, c.w)) {
+                    const int32_t jl = a.rsidx[j];
                     if (EMIT) {
                         if (pos < a.out_cap) {
                             a.col_out[pos] = (int64_t)(a.ref_ids ? a.ref_ids[jl] : jl - u.rshift);
@@ -2647,8 +2662,8 @@ int tcr_emit(const tcr_search_desc* d, const void* structure, void* scratch, int
 
 static int f64_args(const tcr_search_desc* d, const tcr_f64_inputs* in, F64Args& f) {
     if (!in) return set_error(TCR_ERR_INVALID, "missing float64 inputs");
-    if ((d->n_query > 0 && !in->query_pos) || (d->n_ref > 0 && !in->ref_pos))
-        return set_error(TCR_ERR_INVALID, "missing float64 positions");
+    if ((d->n_query > 0 && !in->query_pos) || (d->n_ref > 0 && (!in->ref_pos || !in->ref_sorted)))
+        return set_error(TCR_ERR_INVALID, "missing float64 positions or the sorted-reference workspace");
     if (d->mode != TCR_SCATTER && d->n_query > 0 && !in->query_sup)
         return set_error(TCR_ERR_INVALID, "this mode needs float64 query supports");
     if (d->mode != TCR_GATHER && d->n_ref > 0 && !in->ref_sup)
@@ -2659,8 +2674,11 @@ static int f64_args(const tcr_search_desc* d, const tcr_f64_inputs* in, F64Args&
     f.qsup = in->query_sup;
     f.rpos = in->ref_pos;
     f.rsup = in->ref_sup;
+    f.rsorted = reinterpret_cast<double4*>(in->ref_sorted);
     for (int k = 0; k < 3; ++k) f.ext[k] = in->domain_max[k] - in->domain_min[k];
     f.nq = d->n_query;
+    f.nr = d->n_ref;
+    f.self_order = d->self_search ? 1 : 0;
     return TCR_OK;
 }
 
@@ -2686,6 +2704,10 @@ int tcr_count_f64(const tcr_search_desc* d, const tcr_f64_inputs* in, const void
     query_params_kernel<<<1, 128, 0, st>>>(W.table, S.grid, b.C, W.qparams, W.exact_clouds);
     note_launches(2);
     const int64_t nq = b.nq;
+    if (b.nr > 0) {
+        f64_sort_refs_kernel<<<grid_for(b.nr, 256), 256, 0, st>>>(S.rsidx, f, d->dim);
+        note_launches(1);
+    }
     if (nq > 0) {
         WalkArgs a = make_walk(b, S, W);
         f64_walk_kernel<false><<<grid_for(nq, 128, num_sms() * 8), 128, 0, st>>>(a, f);

@@ -12,8 +12,9 @@ keeps that arithmetic where it decides pairs and uses float32 only to find candi
   few float32 ulps of the largest coordinate, so that the float32 cell of every point is at least
   as wide as the double one: every pair within the double support lies in a query's 3^d stencil;
 * the float32 structure is built by ``tcr_build_structure`` with that cell size, and
-  ``tcr_count_f64`` / ``tcr_emit_f64`` decide every stencil candidate on the double arrays with the
-  reference's double expression (common.h:106-129 at scalar_t = double).
+  ``tcr_count_f64`` / ``tcr_emit_f64`` decide every stencil candidate on the double arrays (the
+  references gathered once into cell order) with the reference's double expression
+  (common.h:106-129 at scalar_t = double).
 
 The pair set is the reference's wherever the two grids have the same number of cells per periodic
 dimension (they differ only for a domain extent within a few ulps of a whole number of cells).
@@ -100,6 +101,8 @@ def compact_search_f64(xq, hq, xr, hr, lo, hi, mask, mode, L, fmt, self_search):
     inputs.query_sup = None if hq is None or not nq else hq.data_ptr()
     inputs.ref_pos = xr_w.data_ptr() if nr else None
     inputs.ref_sup = None if hr is None or not nr else hr.data_ptr()
+    ref_sorted = torch.empty((max(nr, 1), 4), dtype=torch.float64, device=device)
+    inputs.ref_sorted = ref_sorted.data_ptr()
     for k in range(3):
         inputs.domain_min[k] = lo[k] if k < dim else 0.0
         inputs.domain_max[k] = hi[k] if k < dim else 1.0
