@@ -55,7 +55,26 @@ def test_cpu_inputs_and_mismatched_dtypes():
     with pytest.raises(RuntimeError):  # the reference's double operators reject a float32 domain
         tcr.radiusSearch(tcr.PointCloud(torch.tensor(x).cuda(), torch.tensor(hx).cuda()), None, mode=c["mode"],
                          domain=dom32, algorithm="compact")
-    dom = tcr.DomainDescription(torch.tensor(lo), torch.tensor(hi), torch.as_tensor(per), len(lo))
-    with pytest.raises(ValueError):
-        tcr.radiusSearch(tcr.PointCloud(torch.tensor(x).cuda(), torch.tensor(hx).cuda()), None, mode=c["mode"],
-                         domain=dom, algorithm="compact", returnStructure=True)
+
+
+
+@pytest.mark.parametrize("mode", ["gather", "symmetric"])
+def test_returned_structure_serves_new_float64_queries(mode):
+    """returnStructure with float64 inputs, then neighborSearchExisting with other float64 queries:
+    the same pairs as radiusSearch of those queries against the structure's references."""
+    import f64_cases
+    import torchcompactradius_b200 as tcr
+    x, hx, y, hy, lo, hi, per = f64_cases.f64_case(21, 3, 3000, 2000, 40, [True, False, True])
+    hy = hy * 0.9  # the structure's cells were sized for the references' supports
+    t = lambda a: torch.as_tensor(a).cuda()
+    dom = tcr.DomainDescription(t(lo), t(hi), torch.as_tensor(per), 3)
+    adj, ds = tcr.radiusSearch(tcr.PointCloud(t(x), t(hx)), None, mode=mode, domain=dom, algorithm="compact",
+                               returnStructure=True)
+    again = tcr.neighborSearchExisting(tcr.PointCloud(t(y), t(hy)), ds, mode=mode)
+    direct = tcr.radiusSearch(tcr.PointCloud(t(y), t(hy)), tcr.PointCloud(t(x), t(hx)), mode=mode, domain=dom,
+                              algorithm="compact")
+    assert again.row.numel() == direct.row.numel()
+    assert cases.pair_sha(again.row.cpu().numpy(), again.col.cpu().numpy()) == \
+        cases.pair_sha(direct.row.cpu().numpy(), direct.col.cpu().numpy())
+    row, col = search64.radius_search(y, hy, x, hx, lo, hi, per, mode)
+    assert cases.pair_sha(row, col) == cases.pair_sha(direct.row.cpu().numpy(), direct.col.cpu().numpy())

@@ -76,13 +76,12 @@ def radiusSearch(queryPointCloud: PointCloud, referencePointCloud: Optional[Poin
                   f"periodic mask {mask}, hashMapLength {hashMapLength}, format {format}")
         nq, nr = qpos.shape[0], rpos.shape[0]
         if (qpos.dtype == torch.float64 or rpos.dtype == torch.float64) and algorithm != "mlm":
-            out = _radius_search_f64(queryPointCloud, referencePointCloud, supportOverride, mode, domain, lo, hi, mask,
-                                     hashMapLength, format, self_cloud, returnStructure, device)
+            out, ds = _radius_search_f64(queryPointCloud, referencePointCloud, supportOverride, mode, domain, lo, hi,
+                                         mask, hashMapLength, format, self_cloud, returnStructure, device)
             if in_device.type != "cuda":
                 out = tuple(None if t is None else t.to(in_device) for t in out)
-            if format == "coo":
-                return SparseCOO(out[0], out[1], nq, nr)
-            return SparseCSR(out[0], out[1], out[2], nq, nr)
+            adj = SparseCOO(out[0], out[1], nq, nr) if format == "coo" else SparseCSR(out[0], out[1], out[2], nq, nr)
+            return (adj, ds) if returnStructure else adj
         xq = _as_f32(qpos, device)
         same = self_cloud or (rpos.data_ptr() == qpos.data_ptr() and rpos.shape == qpos.shape
                               and rpos.stride() == qpos.stride() and rpos.dtype == qpos.dtype)
@@ -123,8 +122,6 @@ def _radius_search_f64(q: PointCloud, r: PointCloud, supportOverride, mode, doma
     domain must all be float64, as the reference's double operators require (their accessors raise
     otherwise)."""
     from .search64 import compact_search_f64
-    if returnStructure:
-        raise ValueError("returnStructure is not available for float64 inputs")
     need = [("positions", q.positions), ("positions", r.positions), ("domain.min", domain.min),
             ("domain.max", domain.max)]
     if supportOverride is None:
@@ -150,7 +147,8 @@ def _radius_search_f64(q: PointCloud, r: PointCloud, supportOverride, mode, doma
         assert hq is not None, f"queryParticleSupports must be provided for {mode} mode"
     if mode in ("scatter", "symmetric", "superSymmetric"):
         assert hr is not None, f"referenceSupports must be provided for {mode} mode"
-    return compact_search_f64(xq, hq, xr, hr, lo, hi, mask, mode, L, fmt, self_cloud)
+    return compact_search_f64(xq, hq, xr, hr, lo, hi, mask, mode, L, fmt, self_cloud, return_structure=returnStructure,
+                              ref_pos_user=r.positions, fixed_support=supportOverride)
 
 
 def neighborSearchExisting(queryPointCloud: PointCloud, hashMap: CompactHashMap, mode: str = "symmetric",
@@ -171,6 +169,8 @@ def neighborSearchExisting(queryPointCloud: PointCloud, hashMap: CompactHashMap,
         qpos = queryPointCloud.positions
         if qpos.shape[1] != hashMap._dim:
             raise ValueError("query dimensionality does not match the structure")
+        if getattr(hashMap, "_f64", None) is not None:  # a structure of float64 references
+            return _existing_f64(queryPointCloud, hashMap, mode, format, dev)
         xq = _as_f32(qpos, dev)
         sup = queryPointCloud.supports
         if sup is None and hashMap.fixedSupport is not None:
@@ -193,6 +193,32 @@ def neighborSearchExisting(queryPointCloud: PointCloud, hashMap: CompactHashMap,
         if format == "coo":
             return SparseCOO(out[0], out[1], nq, nr)
         return SparseCSR(out[0], out[1], out[2], nq, nr)
+
+
+def _existing_f64(q: PointCloud, hashMap: CompactHashMap, mode, fmt, dev):
+    """neighborSearchExisting against a float64 structure: float64 queries (and supports), searched
+    with the reference's double arithmetic against the structure's references."""
+    from .search64 import compact_search_f64
+    qpos = q.positions
+    if qpos.dtype != torch.float64 or (q.supports is not None and q.supports.dtype != torch.float64):
+        raise RuntimeError("expected scalar type Double but found Float (queries of a float64 structure)")
+    xq = qpos.to(device=dev).contiguous()
+    if q.supports is None and hashMap.fixedSupport is not None:
+        hq = torch.full((xq.shape[0],), float(hashMap.fixedSupport), dtype=torch.float64, device=dev)
+    else:
+        hq = None if q.supports is None else q.supports.to(device=dev).contiguous()
+    if mode in ("gather", "symmetric", "superSymmetric") and hq is None:
+        raise ValueError(f"query supports are required for {mode} mode")
+    if mode in ("scatter", "symmetric", "superSymmetric") and hashMap._f64["hr"] is None:
+        raise ValueError(f"the structure has no reference supports for {mode} mode")
+    out, _ = compact_search_f64(xq, hq, None, None, hashMap._lo, hashMap._hi, hashMap._mask, mode,
+                                hashMap.hashMapLength, fmt, False, structure=hashMap)
+    nq, nr = qpos.shape[0], hashMap._n
+    if qpos.device.type != "cuda":
+        out = tuple(None if t is None else t.to(qpos.device) for t in out)
+    if fmt == "coo":
+        return SparseCOO(out[0], out[1], nq, nr)
+    return SparseCSR(out[0], out[1], out[2], nq, nr)
 
 
 def radius(queryPositions: torch.Tensor, referencePositions: Optional[torch.Tensor],

@@ -122,6 +122,7 @@ class CompactHashMap:
         self.fixedSupport = fixedSupport
         self.searchRadius = searchRadius
         self._cache = {}
+        self._f64 = None  # float64 references: their wrapped copies and cell size (search64.py)
 
     # -- raw device views -------------------------------------------------------------------
     def _view(self, field, dtype, count):

@@ -67,32 +67,44 @@ def grid_support64(hq, hr, mode: str) -> float:
     return max(float(hr.max()), float(hq.max()))
 
 
-def compact_search_f64(xq, hq, xr, hr, lo, hi, mask, mode, L, fmt, self_search):
+def compact_search_f64(xq, hq, xr, hr, lo, hi, mask, mode, L, fmt, self_search, return_structure=False,
+                       structure=None, ref_pos_user=None, fixed_support=None):
     """One float64 search on the current CUDA stream.  xq / xr are float64 device tensors (the
-    caller's positions, unwrapped), hq / hr float64 or None.  Returns (i, j) for COO or
-    (indices, indptr, rowEntries) for CSR."""
+    caller's positions, unwrapped), hq / hr float64 or None.  Returns ((i, j) for COO or
+    (indices, indptr, rowEntries) for CSR, structure): with ``return_structure`` a
+    ``CompactHashMap`` that ``structure=`` (and ``neighborSearchExisting``) reuses for new
+    float64 queries against the same references (then xr / hr are ignored)."""
+    from .search import CompactHashMap
     lib = _lib.load()
     device = xq.device
     dim = xq.shape[1]
-    nq, nr = xq.shape[0], xr.shape[0]
+    nq = xq.shape[0]
     stream = torch.cuda.current_stream(device)
     sptr = ctypes.c_void_p(stream.cuda_stream)
     xq_w = wrap64(xq, lo, hi, mask)
-    xr_w = wrap64(wrap64(xr, lo, hi, mask), lo, hi, mask)
-    hc = compute_h64(lo, hi, grid_support64(hq, hr, mode)) if nq and nr else 1.0
-    if not (math.isfinite(hc) and hc > 0.0):
-        raise ValueError("no valid cell grid for this domain and support (the support is not smaller than the "
-                         "domain extent, or a support/domain value is not finite)")
-    big = max([abs(v) for v in lo] + [abs(v) for v in hi] +
-              [float(t.abs().max()) for t in (xq_w, xr_w) if t.numel()])
-    padded = hc + 8.0 * 2.0 ** -24 * big
-    hcell = np.float32(padded)
-    if float(hcell) < padded:
-        hcell = np.nextafter(hcell, np.float32(np.inf))
+    if structure is not None:  # references, cell size and float32 copies of an earlier build
+        f = structure._f64
+        xr_w, hr, xr_f, hr_f, hcell = f["xr_w"], f["hr"], f["xr_f"], f["hr_f"], f["hcell"]
+        self_search = False
+    else:
+        xr_w = wrap64(wrap64(xr, lo, hi, mask), lo, hi, mask)
+    nr = xr_w.shape[0]
+    if structure is None:
+        hc = compute_h64(lo, hi, grid_support64(hq, hr, mode)) if nq and nr else 1.0
+        if not (math.isfinite(hc) and hc > 0.0):
+            raise ValueError("no valid cell grid for this domain and support (the support is not smaller than the "
+                             "domain extent, or a support/domain value is not finite)")
+        big = max([abs(v) for v in lo] + [abs(v) for v in hi] +
+                  [float(t.abs().max()) for t in (xq_w, xr_w) if t.numel()])
+        padded = hc + 8.0 * 2.0 ** -24 * big
+        hcell = np.float32(padded)
+        if float(hcell) < padded:
+            hcell = np.nextafter(hcell, np.float32(np.inf))
     xq_f = xq_w.float().contiguous()
-    xr_f = xq_f if self_search else xr_w.float().contiguous()
     hq_f = None if hq is None else hq.float().contiguous()
-    hr_f = None if hr is None else (hq_f if (self_search and hq is hr) else hr.float().contiguous())
+    if structure is None:
+        xr_f = xq_f if self_search else xr_w.float().contiguous()
+        hr_f = None if hr is None else (hq_f if (self_search and hq is hr) else hr.float().contiguous())
     desc = make_desc(dim, mode, mask, lo, hi, L, xq_f, hq_f, xr_f, hr_f, self_search)
     for k in range(dim):
         desc.hcell[k] = float(hcell)
@@ -107,10 +119,17 @@ def compact_search_f64(xq, hq, xr, hr, lo, hi, mask, mode, L, fmt, self_search):
         inputs.domain_min[k] = lo[k] if k < dim else 0.0
         inputs.domain_max[k] = hi[k] if k < dim else 1.0
     s_bytes, w_bytes = _lib.search_sizes(nq, nr, dim)
-    sbuf = torch.empty(s_bytes, dtype=torch.uint8, device=device)
     scratch = torch.empty(w_bytes, dtype=torch.uint8, device=device)
-    _lib.check(lib.tcr_build_structure(ctypes.byref(desc), _ptr(sbuf), s_bytes, _ptr(scratch), w_bytes, sptr),
-               "tcr_build_structure")
+    if structure is None:
+        sbuf = torch.empty(s_bytes, dtype=torch.uint8, device=device)
+        _lib.check(lib.tcr_build_structure(ctypes.byref(desc), _ptr(sbuf), s_bytes, _ptr(scratch), w_bytes, sptr),
+                   "tcr_build_structure")
+        if return_structure:
+            structure = CompactHashMap(sbuf, nr, dim, lo, hi, mask, L, device,
+                                       ref_pos_user if ref_pos_user is not None else xr, hr, fixed_support)
+            structure._f64 = dict(xr_w=xr_w, hr=hr, xr_f=xr_f, hr_f=hr_f, hcell=hcell)
+    else:
+        sbuf = structure._buf
     offsets = torch.empty(nq + 1, dtype=torch.int64, device=device)
     indptr = rowEntries = None
     if fmt == "csr":
@@ -131,4 +150,4 @@ def compact_search_f64(xq, hq, xr, hr, lo, hi, mask, mode, L, fmt, self_search):
                                 _ptr(offsets), _ptr(row), _ptr(col), total, sptr), "tcr_emit_f64")
     col = col[:total]
     row = row[:total] if row is not None else None
-    return (row, col) if fmt == "coo" else (col, indptr, rowEntries)
+    return ((row, col) if fmt == "coo" else (col, indptr, rowEntries)), structure
