@@ -393,7 +393,7 @@ def make_served_workload(seed=5, n_scenes=64, rate=2000.0, seconds=1.0):
     return scenes, arrivals
 
 
-def bench_served(dev, seconds=1.0):
+def bench_served(dev, seconds=1.0, slots=2):
     """The served form: requests arrive on a Poisson trace; each jitters its scene by
     N(0, (0.05 h)^2) per coordinate and searches it (gather, COO).  The search server (resident
     scenes, incremental re-sort, HBM-budget admission, continuous batching on two streams) and the
@@ -413,7 +413,7 @@ def bench_served(dev, seconds=1.0):
         return v[min(len(v) - 1, int(q * len(v)))]
 
     # ---- served -------------------------------------------------------------------------
-    srv = SearchServer(dev, mode="gather", hbm_budget=40e9, slots=2)
+    srv = SearchServer(dev, mode="gather", hbm_budget=40e9, slots=slots)
     for x, h in scenes:
         srv.add_scene(Scene(x.to(dev), torch.full((x.shape[0],), h, device=dev), dom, expected_neighbours=50))
     with srv:
@@ -484,11 +484,11 @@ def bench_served(dev, seconds=1.0):
                 "note": "falls behind the arrivals, so value is its capacity"}
     return {"workload": f"64 persistent 3D scenes, sizes log-uniform [1e3, 1e6] (seed 5), periodic [-1,1]^3, "
                         f"50 neighbours, gather, COO; Poisson arrivals 2000/s for {seconds:g} s, each request "
-                        f"jitters its scene by N(0, (0.05 h)^2); 40 GB admission budget, 2 worker streams",
+                        f"jitters its scene by N(0, (0.05 h)^2); 40 GB admission budget, {slots} worker streams",
             "points": int(sum(x.shape[0] for x, h in scenes)),
             "tuning": {"chosen": {"queries_per_unit": tuned[0], "walk_blocks_per_sm": tuned[1]},
                        "ms_per_batch_of_all_scenes": {f"{c[0]}q/{c[1]}b": round(v, 3)
-                                                      for c, v in tuner.timings["served"].items()}},
+                                                      for c, v in tuner.timings.get("served", {}).items()}},
             "served": served, "served_capacity": served_capacity, "per_call": per_call,
             "speedup_vs_per_call": served_capacity["value"] / per_call["value"],
             "p99_ratio_per_call_over_served": per_call["p99_ms"] / served["p99_ms"]}
