@@ -52,6 +52,8 @@ def parse():
                     help="only run this many eager searches of the workload (a small case for ncu captures)")
     ap.add_argument("--profile-scatter", type=int, default=0,
                     help="only search the workload once and run this many scatter_sum calls over its neighbour list")
+    ap.add_argument("--profile-f64", type=int, default=0,
+                    help="only run this many float64 searches of the workload (a small case for ncu captures)")
     return ap.parse_args()
 
 
@@ -1010,12 +1012,31 @@ def profile_scatter(n):
     return 0
 
 
+def profile_f64(n):
+    """n float64 searches of the 1M-point workload through the public API, nothing else."""
+    import torch
+
+    import torchcompactradius_b200 as tcr
+    pos, sup = make_workload()
+    x, h = pos.double().cuda(), sup.double().cuda()
+    dom = tcr.DomainDescription(torch.full((3,), -1.0, dtype=torch.float64), torch.full((3,), 1.0, dtype=torch.float64),
+                                torch.zeros(3, dtype=torch.bool), 3)
+    for _ in range(n):
+        adj = tcr.radiusSearch(tcr.PointCloud(x, h), None, mode="symmetric", domain=dom, algorithm="compact",
+                               format="csr")
+    torch.cuda.synchronize()
+    print(json.dumps({"profile_f64": n, "pairs": int(adj.indices.numel())}))
+    return 0
+
+
 def main():
     args = parse()
     if args.profile_searches:
         return profile_searches(args.profile_searches)
     if args.profile_scatter:
         return profile_scatter(args.profile_scatter)
+    if args.profile_f64:
+        return profile_f64(args.profile_f64)
     if args.impl == "reference":
         return run_reference(args)
     return run_b200(args)
