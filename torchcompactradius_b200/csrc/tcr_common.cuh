@@ -14,6 +14,7 @@
 #include <cstdint>
 #include <cstdio>
 #include <cuda_runtime.h>
+#include <nvtx3/nvToolsExt.h>
 
 namespace tcr {
 
@@ -21,6 +22,15 @@ namespace tcr {
 // accounting.
 inline unsigned long long g_launches = 0;
 static inline void note_launches(int k) { __atomic_fetch_add(&g_launches, (unsigned long long)k, __ATOMIC_RELAXED); }
+
+// A named NVTX range around one C-ABI call (the host-side enqueue of a build, count, emit or scatter
+// stage), for timeline profilers; without a profiler attached a push or pop is one pointer check.
+struct NvtxRange {
+    explicit NvtxRange(const char* name) { nvtxRangePushA(name); }
+    ~NvtxRange() { nvtxRangePop(); }
+    NvtxRange(const NvtxRange&) = delete;
+    NvtxRange& operator=(const NvtxRange&) = delete;
+};
 
 // The calling thread's last error message (tcr_last_error), shared by every source file.
 inline thread_local char g_err[512];

@@ -783,6 +783,7 @@ extern "C" {
 int64_t tcr_scatter_desc_bytes(void) { return (int64_t)sizeof(tcr_scatter_desc); }
 
 int tcr_index_stats(const int64_t* index, int64_t n, int64_t* stats, int64_t* stats_host, void* stream) {
+    NvtxRange nvtx_("tcr_index_stats");
     if (n < 0 || !stats || (n > 0 && !index)) return set_error(TCR_ERR_INVALID, "tcr_index_stats: bad arguments");
     cudaStream_t st = static_cast<cudaStream_t>(stream);
     stats_init_kernel<<<1, 1, 0, st>>>(stats);
@@ -807,6 +808,7 @@ int tcr_scatter_sizes(const tcr_scatter_desc* d, int64_t* scratch_bytes) {
 }
 
 int tcr_scatter(const tcr_scatter_desc* d, void* scratch, int64_t scratch_bytes, int64_t* stats_host, void* stream) {
+    NvtxRange nvtx_("tcr_scatter");
     Plan p;
     int rc = check_desc(d, p, true);
     if (rc) return rc;

@@ -2635,6 +2635,7 @@ int tcr_structure_offsets(int64_t n_ref, int64_t* offsets, int32_t n) {
 
 int tcr_build_structure(const tcr_search_desc* d, void* structure, int64_t structure_bytes, void* scratch,
                         int64_t scratch_bytes, void* stream) {
+    NvtxRange nvtx_("tcr_build_structure");
     HostBatch b;
     int rc = batch_of_desc(d, 2, b);
     if (rc) return rc;
@@ -2644,6 +2645,7 @@ int tcr_build_structure(const tcr_search_desc* d, void* structure, int64_t struc
 int tcr_count(const tcr_search_desc* d, const void* structure, void* scratch, int64_t scratch_bytes, int32_t* stage,
               int64_t stage_capacity, int64_t* offsets, int32_t* indptr_out, int64_t* row_entries_out, int64_t* info_out,
               void* stream) {
+    NvtxRange nvtx_("tcr_count");
     HostBatch b;
     int rc = batch_of_desc(d, 1, b);
     if (rc) return rc;
@@ -2654,6 +2656,7 @@ int tcr_count(const tcr_search_desc* d, const void* structure, void* scratch, in
 int tcr_emit(const tcr_search_desc* d, const void* structure, void* scratch, int64_t scratch_bytes,
              const int32_t* stage, const int64_t* offsets, int64_t* row_out, int64_t* col_out, int64_t out_capacity,
              void* stream) {
+    NvtxRange nvtx_("tcr_emit");
     HostBatch b;
     int rc = batch_of_desc(d, 1, b);
     if (rc) return rc;
@@ -2685,6 +2688,7 @@ static int f64_args(const tcr_search_desc* d, const tcr_f64_inputs* in, F64Args&
 int tcr_count_f64(const tcr_search_desc* d, const tcr_f64_inputs* in, const void* structure, void* scratch,
                   int64_t scratch_bytes, int64_t* offsets, int32_t* indptr_out, int64_t* row_entries_out,
                   int64_t* info_out, void* stream) {
+    NvtxRange nvtx_("tcr_count_f64");
     HostBatch b;
     int rc = batch_of_desc(d, 1, b);
     if (rc) return rc;
@@ -2727,6 +2731,7 @@ int tcr_count_f64(const tcr_search_desc* d, const tcr_f64_inputs* in, const void
 int tcr_emit_f64(const tcr_search_desc* d, const tcr_f64_inputs* in, const void* structure, void* scratch,
                  int64_t scratch_bytes, const int64_t* offsets, int64_t* row_out, int64_t* col_out,
                  int64_t out_capacity, void* stream) {
+    NvtxRange nvtx_("tcr_emit_f64");
     HostBatch b;
     int rc = batch_of_desc(d, 1, b);
     if (rc) return rc;
@@ -2766,6 +2771,7 @@ int tcr_batch_sizes(const tcr_batch_desc* bd, int64_t* structure_bytes, int64_t*
 
 int tcr_batch_build_structure(const tcr_batch_desc* bd, void* structure, int64_t structure_bytes, void* scratch,
                               int64_t scratch_bytes, void* stream) {
+    NvtxRange nvtx_("tcr_batch_build_structure");
     HostBatch b;
     int rc = batch_of(bd, 2, b);
     if (rc) return rc;
@@ -2775,6 +2781,7 @@ int tcr_batch_build_structure(const tcr_batch_desc* bd, void* structure, int64_t
 int tcr_batch_count(const tcr_batch_desc* bd, const void* structure, void* scratch, int64_t scratch_bytes,
                     int32_t* stage, int64_t stage_capacity, int64_t* offsets, int32_t* indptr_out,
                     int64_t* row_entries_out, int64_t* info_out, void* stream) {
+    NvtxRange nvtx_("tcr_batch_count");
     HostBatch b;
     int rc = batch_of(bd, 1, b);
     if (rc) return rc;
@@ -2785,6 +2792,7 @@ int tcr_batch_count(const tcr_batch_desc* bd, const void* structure, void* scrat
 int tcr_batch_emit(const tcr_batch_desc* bd, const void* structure, void* scratch, int64_t scratch_bytes,
                    const int32_t* stage, const int64_t* offsets, int64_t* row_out, int64_t* col_out,
                    int64_t out_capacity, void* stream) {
+    NvtxRange nvtx_("tcr_batch_emit");
     HostBatch b;
     int rc = batch_of(bd, 1, b);
     if (rc) return rc;
