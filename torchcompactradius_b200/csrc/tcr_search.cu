@@ -130,7 +130,6 @@ struct Scratch {
     int32_t* exact_clouds;  // [1] clouds whose every pair takes the exact test
     int32_t* num_exact;     // [1] units the count walk re-tested with exact decisions
     int32_t* unit_cap;      // [1] queries per work unit of this search (set by the count phase)
-    int32_t* num_big;       // [1] units recorded window by window
     unsigned long long* cursor;  // [1] staging fill
     float4* pack;           // [max(nq,nr)] packed input points before sorting
     void* keys[2];          // [max(nq,nr)] 64-bit slots (32-bit keys use the first half)
@@ -150,7 +149,6 @@ struct Scratch {
     int32_t* stray;         // [nq]
     int32_t* rec;           // [nq] per unit: offset of its record in the staging list (-1: not staged)
     int32_t* flagged;       // [nq] units re-walked by the emit pass
-    int32_t* big;           // [nq] units of more than one record window
     // incremental re-sort (builds given the previous cell of every reference point), else null
     int32_t* stay;          // [nr] 1: the point is still in its previous cell
     void* stay_keys;        // [nr] keys of the unmoved points, input order (sorted when the hint holds)
@@ -180,7 +178,6 @@ static Scratch carve_scratch(void* buf, int64_t nq, int64_t nr, int64_t C, bool 
     s.exact_clouds = c.take<int32_t>(1);
     s.num_exact = c.take<int32_t>(1);
     s.unit_cap = c.take<int32_t>(1);
-    s.num_big = c.take<int32_t>(1);
     s.cursor = c.take<unsigned long long>(1);
     s.pack = c.take<float4>(nmax);
     s.keys[0] = c.take<unsigned long long>(nmax);
@@ -203,7 +200,6 @@ static Scratch carve_scratch(void* buf, int64_t nq, int64_t nr, int64_t C, bool 
     s.stray = c.take<int32_t>(q);
     s.rec = c.take<int32_t>(q);
     s.flagged = c.take<int32_t>(q);
-    s.big = c.take<int32_t>(q);
     const int64_t ni = incremental ? std::max<int64_t>(nr, 1) : 0;
     s.stay = incremental ? c.take<int32_t>(ni) : nullptr;
     s.stay_keys = incremental ? c.take<unsigned long long>(ni) : nullptr;
@@ -472,7 +468,6 @@ __global__ void count_init_kernel(Scratch W, int C, int unit_cap) {
         *W.exact_clouds = 0;
         *W.num_exact = 0;
         *W.unit_cap = unit_cap;
-        *W.num_big = 0;
         *W.cursor = 0ull;
     }
 }
@@ -912,11 +907,10 @@ struct BoundedUnitOut {
 // Work unit: <= 32 queries of one query group (cell).  One warp takes a unit, looks up its
 // cloud (one copy of the cloud's parameters in shared memory, refreshed when the warp moves to
 // another cloud), finds the unit's 3^d stencil cells and walks their candidates in chunks of 32.
-// The count walk tests every (query, candidate) pair once, keeps the 32-bit hit masks of a unit
-// with <= kSegChunks chunks in shared memory and writes them with the chunk's candidate indices
-// as one record to a staging list; the emit pass expands the records into CSR/COO slots.  A unit
-// with more chunks, or one that finds the staging list full, is only counted and is walked again
-// by the emit walk, which writes its pairs directly.
+// The count walk tests every (query, candidate) pair once and writes the unit's record -- its
+// candidate runs and the 32-bit hit mask of every (query, chunk) -- to a staging list; the emit
+// pass expands the records into CSR/COO slots.  A unit that finds the staging list full is only
+// counted and is walked again by the emit walk, which writes its pairs directly.
 
 // The unit's cloud, as the walk kernels read it (shared memory, warp-uniform).
 struct UnitCtx {
@@ -968,8 +962,6 @@ struct WalkArgs {
     int32_t* flagged;             // [units] units to re-walk in the emit pass
     int32_t* num_flagged;
     int32_t* num_exact;           // units re-tested with exact decisions
-    int32_t* big;                 // units of more than kSegChunks chunks (for the windowed count walk)
-    int32_t* num_big;
     unsigned long long* cursor;   // staging list fill
     int32_t* stage;               // staging list
     int64_t stage_cap;
@@ -1147,8 +1139,8 @@ __device__ __forceinline__ void lean_test(const WrapCtx& wc, const float4& q, co
 
 constexpr int kWalkWarps = 4;
 // Resident blocks per SM the count walk is compiled for (registers <= 65536 / (128 * blocks)):
-// five (20 warps) measured fastest on non-periodic clouds, four (128 registers, no spills) on
-// periodic ones, whose wrap tests need more registers.
+// five (96 registers, no spills) on non-periodic clouds, four on periodic ones, whose wrap tests
+// need more registers.
 #ifndef TCR_WALK_MIN_BLOCKS
 #define TCR_WALK_MIN_BLOCKS 5
 #endif
@@ -1157,19 +1149,26 @@ constexpr int kWalkWarps = 4;
 #endif
 constexpr int kWalkMinBlocks = TCR_WALK_MIN_BLOCKS;
 constexpr int kWalkMinBlocksPeriodic = TCR_WALK_MIN_BLOCKS_PERIODIC;
-constexpr int kSegChunks = 24;  // staged units: at most 24 chunks (768 candidates)
-constexpr int kMaskStride = kSegChunks + 1;  // padded rows: conflict-free per-lane reads
+
+// Record of a staged unit in the staging list (int32 words):
+//   [0] chunks of 32 candidates   [1] R, candidate runs   [2] nb, queries   [3] 0
+//   [4, 4 + R)          first sorted index of each run
+//   [4 + R, 5 + 2R)     candidate prefix of each run; entry R is the unit's candidate count M
+//   [5 + 2R, ...)       hit masks, chunk-major: word c * nb + q, bit j set when query q meets
+//                       candidate 32 c + j
+// A run is a stretch of consecutive sorted points: stencil cells whose ranges continue each other
+// (the row neighbours of a linear-order grid) merge into one.
+constexpr int kRecHeader = 4;
+__host__ __device__ __forceinline__ int64_t record_words(int32_t runs, int32_t nchunks, int32_t nb) {
+    return kRecHeader + 2 * (int64_t)runs + 1 + (int64_t)nchunks * nb;
+}
 
 struct WalkSmem {
-    int32_t pre[kWalkWarps][33];
-    int32_t beg[kWalkWarps][32];
-    float4 q[kWalkWarps][32];
-    float4 cand[kWalkWarps][36];                  // the chunk's candidates, stream-major, rows padded
-    float shift[kWalkWarps][3][32];               // per stencil cell: +-ext on dims it lies across a seam
-    int32_t qbefore[kWalkWarps][32];              // per query: hits before the current record window
-    int32_t* rec_ptr[kWalkWarps];                 // the unit's record (null: not staged)
-    uint32_t mask[kWalkWarps][32 * kMaskStride];  // [query][chunk] hit masks
-    int32_t sj[kWalkWarps][kSegChunks][32];       // output column of candidate (chunk, lane)
+    float4 q[kWalkWarps][32];        // the unit's queries: x, y, z and the query's share of the test
+    float qh[kWalkWarps][32];        // the queries' supports (for the exact re-test)
+    int32_t run_beg[kWalkWarps][32];
+    int32_t run_pre[kWalkWarps][33];
+    float shift[kWalkWarps][3][32];  // per run: +-ext on the dimensions its cells lie across a seam
     UnitCtx u[kWalkWarps];
 };
 
@@ -1183,35 +1182,26 @@ __device__ __forceinline__ int32_t cand_index(const int32_t* pre, const int32_t*
     return beg[lo] + (k - pre[lo]);
 }
 
-// Lane-side constants of the lean test for query q (support hq): the query's share of the
-// threshold and the half width of the band, conservative over every candidate (rmax is the
-// largest reference support).
+// The query's share of the test, kept in the .w of its shared-memory copy: gather hq^2 (the test is
+// d2 - hq^2), symmetric hq / 2 (thr = hq / 2 + hc / 2 == fl(hq + hc) / 2), superSymmetric hq.
 template <int MODE>
 __device__ __forceinline__ float query_share(float hq) {
     return MODE == kSymmetric ? 0.5f * hq : (MODE == kGather ? hq * hq : hq);
 }
+
+// The largest threshold candidate c (share cw) can meet over every query (qmax: the largest query
+// support); the band of the fast test is kBandEps times its square.
 template <int MODE>
-__device__ __forceinline__ float query_band(float hq, float rmax) {
-    float t;
-    if (MODE == kGather) t = hq;
-    else if (MODE == kScatter) t = rmax;
-    else if (MODE == kSymmetric) t = fmaf(hq, 0.5f, 0.5f * rmax);
-    else t = fmaxf(hq, rmax);
-    return kBandEps * t * t;
+__device__ __forceinline__ float cand_tmax(float cw, float qmax) {
+    if (MODE == kGather) return qmax;
+    if (MODE == kScatter) return cw;
+    if (MODE == kSymmetric) return fmaf(qmax, 0.5f, cw);
+    return fmaxf(qmax, cw);
 }
 
-// The largest threshold lane q can meet (query_band is kBandEps times its square).
-template <int MODE>
-__device__ __forceinline__ float query_tmax(float hq, float rmax) {
-    if (MODE == kGather) return hq;
-    if (MODE == kScatter) return rmax;
-    if (MODE == kSymmetric) return fmaf(hq, 0.5f, 0.5f * rmax);
-    return fmaxf(hq, rmax);
-}
-
-// Float test of query q (lane) against candidate c; r < 0 means inside.
+// Float test of query q (share in q.w) against candidate c (share cw): r < 0 means inside.
 template <int DIM, bool PERIODIC, int MODE>
-__device__ __forceinline__ float lane_residual(const WrapCtx& wc, const float4& q, float qs, const float4& c,
+__device__ __forceinline__ float pair_residual(const WrapCtx& wc, const float4& q, const float4& c, float cw,
                                                bool& wrap_unc) {
     float dd[3];
 #pragma unroll
@@ -1219,77 +1209,76 @@ __device__ __forceinline__ float lane_residual(const WrapCtx& wc, const float4& 
     float d2 = dd[0] * dd[0];
     if (DIM > 1) d2 = fmaf(dd[1], dd[1], d2);
     if (DIM > 2) d2 = fmaf(dd[2], dd[2], d2);
-    if (MODE == kGather) return d2 - qs;                 // qs = hq^2 (same sign as d2 - hq*hq)
+    if (MODE == kGather) return d2 - q.w;  // same sign as d2 - hq * hq up to the band
     if (MODE == kScatter) return fmaf(-c.w, c.w, d2);
-    const float thr = (MODE == kSymmetric) ? fmaf(c.w, 0.5f, qs) : fmaxf(q.w, c.w);
+    const float thr = MODE == kSymmetric ? q.w + cw : fmaxf(q.w, c.w);
     return fmaf(-thr, thr, d2);
 }
 
-// Tests the lane's query against the Q candidates of its stream; returns the Q-bit hit mask and
-// ORs into `unc` whether any pair lies in the band (those units are redone with exact decisions).
-template <int DIM, bool PERIODIC, int MODE, int Q>
-__device__ __forceinline__ uint32_t stream_mask(const WrapCtx& wc, const float4* cand, const float4& q, float qs,
-                                                float band, bool& unc) {
-    uint32_t m = 0;
+// Warp-wide 32 x 32 bit transpose: lane j holds row j (bit k = entry (j, k)); lane k receives
+// column k (bit j = entry (j, k)).  Five butterfly stages swap ever smaller off-diagonal blocks.
+__device__ __forceinline__ uint32_t warp_transpose32(uint32_t x, int lane) {
 #pragma unroll
-    for (int k = 0; k < Q; ++k) {
-        const float4 c = cand[k];
-        bool wrap_unc = false;
-        const float r = lane_residual<DIM, PERIODIC, MODE>(wc, q, qs, c, wrap_unc);
-        if (r < 0.0f) m |= 1u << k;
-        unc |= (fabsf(r) <= band) || wrap_unc;
+    for (int s = 16; s >= 1; s >>= 1) {
+        const uint32_t m = s == 16 ? 0x0000ffffu : (s == 8 ? 0x00ff00ffu : (s == 4 ? 0x0f0f0f0fu
+                                                                                 : (s == 2 ? 0x33333333u : 0x55555555u)));
+        const uint32_t y = __shfl_xor_sync(0xffffffffu, x, s);
+        x = (lane & s) ? ((x & ~m) | ((y & ~m) >> s)) : ((x & m) | ((y & m) << s));
     }
-    return m;
+    return x;
 }
 
-// The same with every in-band pair decided by the exact reference test (rare units only).
-template <int DIM, bool PERIODIC, int MODE>
-__device__ __noinline__ uint32_t stream_mask_exact(ExactCtx xc, const float4* cand, int n, float4 q, float qs,
-                                                   float band) {
+// The lane's candidate against queries K4-1 .. 0 of the unit (K4 a multiple of 4; rows past the
+// unit's queries are NaN and never hit): bit k of the result is query k's hit, taken from the sign
+// of the residual (an arithmetic NaN is positive).  `unc` collects pairs inside the band.
+template <int DIM, bool P, int MODE>
+__device__ __forceinline__ uint32_t chunk_hits(const WrapCtx& wc, const float4* __restrict__ qsm, int K4,
+                                               const float4& cv, float cw, float band, bool& unc) {
+    uint32_t hit = 0;
+    for (int k = K4 - 4; k >= 0; k -= 4) {
+#pragma unroll
+        for (int i = 3; i >= 0; --i) {
+            const float4 q = qsm[k + i];
+            bool wu = false;
+            const float r = pair_residual<DIM, P, MODE>(wc, q, cv, cw, wu);
+            hit = __funnelshift_l(__float_as_uint(r), hit, 1);
+            unc |= (fabsf(r) <= band) || wu;
+        }
+    }
+    return hit;
+}
+
+// The same with every pair inside the band decided by the reference's exact test, on the original
+// (unshifted) candidate; rare units only, so out of line.
+template <int DIM, int MODE>
+__device__ __noinline__ uint32_t chunk_hits_exact(ExactCtx xc, const float4* qsm, const float* qh, int K4, float4 cv,
+                                                  float band) {
     const WrapCtx wc = wrap_ctx(xc.periodic_mask, xc.ext);
-    uint32_t m = 0;
-    for (int k = 0; k < n; ++k) {
-        const float4 c = cand[k];
-        bool wrap_unc = false;
-        const float r = lane_residual<DIM, PERIODIC, MODE>(wc, q, qs, c, wrap_unc);
+    const float cw = cand_share<MODE>(cv.w);
+    uint32_t hit = 0;
+    for (int k = K4 - 1; k >= 0; --k) {
+        const float4 q = qsm[k];
+        bool wu = false;
+        const float r = pair_residual<DIM, true, MODE>(wc, q, cv, cw, wu);
         bool in = r < 0.0f;
-        if ((fabsf(r) <= band) || wrap_unc) in = exact_pair_test(xc, q, q.w, c, c.w);
-        if (in) m |= 1u << k;
+        if ((fabsf(r) <= band) || wu) in = exact_pair_test(xc, q, qh[k], cv, cv.w);
+        hit = (hit << 1) | (in ? 1u : 0u);
     }
-    return m;
+    return hit;
 }
 
-// Writes the record window that ends with chunk c (its masks and candidate columns are in shared
-// memory): the queries' hits before the window, the masks, the columns.  Out of line: it runs once
-// per window and keeps its registers out of the candidate loop.
-__device__ __noinline__ void flush_window(WalkSmem& sm, int w, int lane, int32_t nb, int32_t c, int32_t qcount) {
-    const int32_t win = c / kSegChunks, nc = c - win * kSegChunks + 1;
-    int32_t* r = sm.rec_ptr[w] + 1 + (int64_t)win * (nb + (nb + 32) * kSegChunks);
-    if (lane < nb) r[lane] = sm.qbefore[w][lane];
-    for (int q = 0; q < nb; ++q)
-        if (lane < nc) r[nb + q * nc + lane] = sm.mask[w][q * kMaskStride + lane];
-    int32_t* rj = r + nb + nb * nc;
-    for (int32_t k = 0; k < nc; ++k) rj[k * 32 + lane] = sm.sj[w][k][lane];
-    __syncwarp();
-    sm.qbefore[w][lane] = qcount;
-    __syncwarp();
-}
-
-// Count walk of one unit: test every (query, candidate) once; count, stage the hits of small units.
+// Count walk of one unit: test every (query, candidate) once, count, and stage the unit's record.
 //
-// Each chunk's 32 candidates are staged in shared memory; lane (q, s) holds query q and tests it
-// against the Q candidates of stream s (Q = 8, 16 or 32 as the unit has <= 8, <= 16 or <= 32
-// queries, so 32/Q streams keep every lane busy).  Hits become bits of a per-lane mask, merged
-// across streams with shuffles into the 32-bit (query, chunk) mask.
-template <int DIM, bool PERIODIC, int MODE, bool WIN>
+// The unit's candidates stream in chunks of 32, one per lane (a coalesced load of consecutive
+// sorted points); the unit's queries sit in shared memory and are broadcast to every lane, so each
+// lane tests its candidate against every query with no lane left idle but the last chunk's.  A
+// lane's hit bits over the queries are transposed across the warp into the (query, chunk) masks.
+template <int DIM, bool PERIODIC, int MODE>
 __device__ __forceinline__ void count_unit(const WalkArgs& a, WalkSmem& sm, int32_t unit, int32_t grp, int lane,
                                            int w) {
     constexpr int S = DIM == 1 ? 3 : (DIM == 2 ? 9 : 27);
     const UnitCtx& u = sm.u[w];
-    const WrapCtx wc = wrap_ctx(u.periodic_mask, u.ext);
-    const float rmax = u.rmax;
-    const bool exact_all = u.exact_all != 0;
-    const int32_t rshift = u.rshift;
+    const float inf = __int_as_float(0x7f800000);
     const float4 nan4 = make_float4(__int_as_float(0x7fc00000), 0.f, 0.f, 0.f);
     const int32_t t0 = a.unit_t0[unit];
     const int32_t nb = min(*a.unit_cap, a.group_start[grp + 1] - t0);
@@ -1297,9 +1286,8 @@ __device__ __forceinline__ void count_unit(const WalkArgs& a, WalkSmem& sm, int3
     int32_t beg = 0, cnt = 0;
     if (lane < S) stencil_lookup(a, u, gc, lane, beg, cnt);
     const bool shift_mode = PERIODIC && u.shift_ok;
-    bool seam = false;  // some stencil cell of the unit lies across a seam
-    if (shift_mode) {  // the stencil cell's seam shift, in stencil_lookup's offset order
-        float sh[3] = {0.f, 0.f, 0.f};
+    float sh[3] = {0.f, 0.f, 0.f};  // the stencil cell's seam shift, in stencil_lookup's offset order
+    if (shift_mode) {
         int rem = lane;
 #pragma unroll
         for (int d = DIM - 1; d >= 0; --d) {
@@ -1308,20 +1296,31 @@ __device__ __forceinline__ void count_unit(const WalkArgs& a, WalkSmem& sm, int3
             if (lane < S && ((u.periodic_mask >> d) & 1))
                 sh[d] = v < 0 ? -u.ext[d] : (v >= u.count[d] ? u.ext[d] : 0.f);
         }
-        sm.shift[w][0][lane] = sh[0];
-        sm.shift[w][1][lane] = sh[1];
-        sm.shift[w][2][lane] = sh[2];
-        seam = __any_sync(0xffffffffu, sh[0] != 0.f || sh[1] != 0.f || sh[2] != 0.f);
     }
+    const bool seam = shift_mode && __any_sync(0xffffffffu, sh[0] != 0.f || sh[1] != 0.f || sh[2] != 0.f);
+    // runs: a stencil cell whose range continues the previous cell's (same shift) extends its run
     const int32_t inc = warp_inclusive_scan(cnt);
-    sm.pre[w][lane + 1] = inc;
-    if (lane == 0) sm.pre[w][0] = 0;
-    sm.beg[w][lane] = beg;
     const int32_t M = __shfl_sync(0xffffffffu, inc, 31);
-    if (!WIN && ((M + 31) >> 5) > kSegChunks) {  // more than one record window: the windowed launch
-        if (lane == 0) a.big[atomicAdd(a.num_big, 1)] = unit;
-        return;
+    const int32_t pbeg = __shfl_up_sync(0xffffffffu, beg, 1);
+    const int32_t pcnt = __shfl_up_sync(0xffffffffu, cnt, 1);
+    bool cont = lane > 0 && pcnt > 0 && pbeg + pcnt == beg;
+    if (shift_mode) {
+#pragma unroll
+        for (int d = 0; d < DIM; ++d) cont = cont && __shfl_up_sync(0xffffffffu, sh[d], 1) == sh[d];
     }
+    const bool starts = cnt > 0 && !cont;
+    const uint32_t smask = __ballot_sync(0xffffffffu, starts);
+    const int32_t R = __popc(smask);
+    const int rid = __popc(smask & ((1u << lane) - 1u));
+    if (starts) {
+        sm.run_beg[w][rid] = beg;
+        sm.run_pre[w][rid] = inc - cnt;
+        sm.shift[w][0][rid] = sh[0];
+        sm.shift[w][1][rid] = sh[1];
+        sm.shift[w][2][rid] = sh[2];
+    }
+    if (lane == 0) sm.run_pre[w][R] = M;
+    // the unit's queries
     bool active = false;
     int32_t qorig = 0;
     float4 qv = nan4;
@@ -1336,135 +1335,112 @@ __device__ __forceinline__ void count_unit(const WalkArgs& a, WalkSmem& sm, int3
             active = same_cell<DIM>(qc, gc);
         }
         if (!active) {  // own cell differs from the group's (aliasing or wrap rounding): serial path
-            int32_t k = atomicAdd(a.num_stray, 1);
+            const int32_t k = atomicAdd(a.num_stray, 1);
             a.stray[k] = t;
             qv = nan4;
         }
     }
+    sm.qh[w][lane] = qv.w;
+    sm.q[w][lane] = make_float4(qv.x, qv.y, qv.z, query_share<MODE>(qv.w));  // rows >= nb: NaN, never hit
+    // the unit's record, reserved up front
     const int32_t nchunks = (M + 31) >> 5;
-    sm.q[w][lane] = qv;  // rows >= nb hold NaN queries and never hit
-    // The unit's record, reserved up front: [nchunks] then one window per kSegChunks chunks,
-    // [hits of each query before the window: nb][masks: nb x nc, query-major][candidates: nc x 32]
-    const int32_t nwin = (nchunks + kSegChunks - 1) / kSegChunks;
-    const int64_t words = 1 + (int64_t)nwin * nb + (int64_t)(nb + 32) * nchunks;
     bool stage = false;
-    if (a.stage_cap > 0) {
+    uint32_t* msk = nullptr;
+    if (a.stage_cap > 0 && nchunks > 0) {
+        const int64_t words = record_words(R, nchunks, nb);
         unsigned long long base = 0;
         if (lane == 0) base = atomicAdd(a.cursor, (unsigned long long)words);
         base = __shfl_sync(0xffffffffu, base, 0);
         stage = base + (unsigned long long)words <= (unsigned long long)a.stage_cap;
-        if (stage && lane == 0) {
-            a.stage[base] = nchunks;
-            a.rec[unit] = (int32_t)base;
-            sm.rec_ptr[w] = a.stage + base;
+        if (stage) {
+            int32_t* rec = a.stage + base;
+            if (lane == 0) {
+                rec[0] = nchunks;
+                rec[1] = R;
+                rec[2] = nb;
+                rec[3] = 0;
+                rec[kRecHeader + 2 * R] = M;
+                a.rec[unit] = (int32_t)base;
+            }
+            if (starts) {
+                rec[kRecHeader + rid] = beg;
+                rec[kRecHeader + R + rid] = inc - cnt;
+            }
+            msk = reinterpret_cast<uint32_t*>(rec + kRecHeader + 2 * R + 1);
         }
     }
-    const int Q = nb <= 8 ? 8 : (nb <= 16 ? 16 : 32);
-    const int lq = lane & (Q - 1);      // this lane's query
-    const int ls = lane / Q;            // this lane's stream
     __syncwarp();
-    const float4 myq = sm.q[w][lq];
-    const float qs = query_share<MODE>(myq.w);
-    const float band = exact_all ? __int_as_float(0x7f800000) : query_band<MODE>(myq.w, rmax);
-    // a unit with shifted candidates: the band also covers the shift's rounding (|d2 error| <= 2 T
-    // delta + delta^2); units away from the seams keep the tight band
-    float band_s = band;
-    if (seam) {
-        const float t = query_tmax<MODE>(myq.w, rmax), dl = u.shift_delta;
-        band_s = band + fmaf(2.0f * t, dl, dl * dl);
-    }
-    const float4* my_cand = &sm.cand[w][ls * (Q + 1)];
-    // Lane k of chunk c holds candidate 32c + k.  Its stencil cell r only moves forward from
-    // chunk to chunk, so it is tracked incrementally instead of searched.
-    int32_t cr = 0;
-    const int32_t* pre = sm.pre[w];
-    const int32_t* begs = sm.beg[w];
+    // lane k of chunk c holds candidate 32c + k; its run only moves forward from chunk to chunk
+    const int32_t* rpre = sm.run_pre[w];
+    const int32_t* rbeg = sm.run_beg[w];
     const float4* __restrict__ rs = a.rsorted;
-    const int32_t* __restrict__ ri = a.rsidx;
-    const int32_t* __restrict__ rid = a.ref_ids;
-    const float* shx = sm.shift[w][0];
-    const float* shy = sm.shift[w][1];
-    const float* shz = sm.shift[w][2];
-    bool shifting = false;  // the fast pass stages shifted candidates, the exact pass the originals
-    auto fetch = [&cr, &shifting, pre, begs, rs, ri, rid, rshift, M, nan4, shx, shy, shz](int32_t k, float4& v,
-                                                                                         int32_t& jo) {
-        v = nan4;
-        jo = 0;
+    int32_t cr = 0;
+    bool shifting = shift_mode;  // the fast pass tests shifted candidates, the exact pass the originals
+    auto fetch = [&](int32_t k) {
+        float4 v = nan4;
         if (k < M) {
-            while (pre[cr + 1] <= k) ++cr;
-            const int32_t j = begs[cr] + (k - pre[cr]);
-            v = __ldg(&rs[j]);
+            while (rpre[cr + 1] <= k) ++cr;
+            v = __ldg(&rs[rbeg[cr] + (k - rpre[cr])]);
             if (PERIODIC && shifting) {
-                v.x += shx[cr];
-                if (DIM > 1) v.y += shy[cr];
-                if (DIM > 2) v.z += shz[cr];
+                v.x += sm.shift[w][0][cr];
+                if (DIM > 1) v.y += sm.shift[w][1][cr];
+                if (DIM > 2) v.z += sm.shift[w][2][cr];
             }
-            jo = __ldg(&ri[j]);
-            jo = rid ? __ldg(&rid[jo]) : jo - rshift;
         }
+        return v;
     };
-    // the unit's chunk loop; `exact` redoes it deciding in-band pairs with the reference test.  A
-    // unit of more than kSegChunks chunks (the windowed launch, WIN) writes its record window by
-    // window; the others keep every mask in shared memory and write their one window after the loop.
-    int32_t qcount = 0;
+    const WrapCtx wc = wrap_ctx(u.periodic_mask, u.ext);
+    const float qmax = u.qmax;
+    const bool exact_all = u.exact_all != 0;
+    const float dl = u.shift_delta;
+    const int K4 = (nb + 3) & ~3;
+    const float4* qsm = sm.q[w];
+    uint32_t count = 0;
     bool unc = false;
-    for (int pass = 0; pass < 2; ++pass) {
-        const bool exact = pass == 1;
-        shifting = shift_mode && !exact;
-        cr = 0;
-        qcount = 0;
-        if (WIN) sm.qbefore[w][lane] = 0;  // this query's hits before the current window
-        float4 nxt;
-        int32_t nxt_j;
-        fetch(lane, nxt, nxt_j);
-        for (int32_t c = 0; c < nchunks; ++c) {
-            const int32_t cw = WIN ? c % kSegChunks : c;
-            // stage candidate `lane` of this chunk: stream lane / Q, slot lane % Q
-            sm.cand[w][(lane / Q) * (Q + 1) + (lane & (Q - 1))] = nxt;
-            if (stage) sm.sj[w][cw][lane] = nxt_j;
-            fetch(((c + 1) << 5) + lane, nxt, nxt_j);  // prefetch the next chunk's candidate
-            __syncwarp();
-            uint32_t m;
-            if (exact) {
-                m = stream_mask_exact<DIM, PERIODIC, MODE>(unit_exact_ctx(u, MODE), my_cand, Q, myq, qs, band)
-                    << (Q == 32 ? 0 : Q * ls);
-            } else if (shift_mode) {  // shifted candidates: the non-periodic test
-                if (Q == 32) m = stream_mask<DIM, false, MODE, 32>(wc, my_cand, myq, qs, band_s, unc);
-                else if (Q == 16) m = stream_mask<DIM, false, MODE, 16>(wc, my_cand, myq, qs, band_s, unc) << (16 * ls);
-                else m = stream_mask<DIM, false, MODE, 8>(wc, my_cand, myq, qs, band_s, unc) << (8 * ls);
-            } else if (Q == 32) {
-                m = stream_mask<DIM, PERIODIC, MODE, 32>(wc, my_cand, myq, qs, band, unc);
-            } else if (Q == 16) {
-                m = stream_mask<DIM, PERIODIC, MODE, 16>(wc, my_cand, myq, qs, band, unc) << (16 * ls);
-            } else {
-                m = stream_mask<DIM, PERIODIC, MODE, 8>(wc, my_cand, myq, qs, band, unc) << (8 * ls);
-            }
-            if (Q <= 16) m |= __shfl_xor_sync(0xffffffffu, m, 16);
-            if (Q == 8) m |= __shfl_xor_sync(0xffffffffu, m, 8);
-            if (lane < nb) {
-                qcount += __popc(m);
-                if (stage) sm.mask[w][lane * kMaskStride + cw] = m;
-            }
-            __syncwarp();
-            if (WIN && stage && (cw == kSegChunks - 1 || c == nchunks - 1))  // the window is complete
-                flush_window(sm, w, lane, nb, c, qcount);
+    float4 nxt = fetch(lane);
+    for (int32_t c = 0; c < nchunks; ++c) {
+        const float4 cv = nxt;
+        nxt = fetch(((c + 1) << 5) + lane);  // the next chunk's candidate, ahead of its use
+        const float cw = cand_share<MODE>(cv.w);
+        const float t = cand_tmax<MODE>(cw, qmax);
+        float band = exact_all ? inf : kBandEps * t * t;
+        // shifted candidates: the band also covers the shift's rounding (|d2 error| <= 2 T delta + delta^2)
+        if (seam) band += fmaf(2.0f * t, dl, dl * dl);
+        uint32_t hit;
+        if (shift_mode) hit = chunk_hits<DIM, false, MODE>(wc, qsm, K4, cv, cw, band, unc);
+        else hit = chunk_hits<DIM, PERIODIC, MODE>(wc, qsm, K4, cv, cw, band, unc);
+        const uint32_t m = warp_transpose32(hit, lane);
+        if (lane < nb) {
+            count += __popc(m);
+            if (stage) msk[c * nb + lane] = m;
         }
-        if (exact || !__any_sync(0xffffffffu, unc)) break;
-        if (lane == 0) atomicAdd(a.num_exact, 1);  // the unit is walked again with exact decisions
     }
-    if (!WIN && stage && nchunks > 0) {  // the one window: [nchunks][zeros: nb][masks][candidates]
-        int32_t* r = sm.rec_ptr[w] + 1;
-        if (lane < nb) r[lane] = 0;
-        for (int q = 0; q < nb; ++q)
-            if (lane < nchunks) r[nb + q * nchunks + lane] = sm.mask[w][q * kMaskStride + lane];
-        int32_t* rj = r + nb + nb * nchunks;
-        for (int32_t c = 0; c < nchunks; ++c) rj[c * 32 + lane] = sm.sj[w][c][lane];
+    if (__any_sync(0xffffffffu, unc)) {  // some pair lies in the band: walk again with exact decisions
+        if (lane == 0) atomicAdd(a.num_exact, 1);
+        const ExactCtx xc = unit_exact_ctx(u, MODE);
+        shifting = false;
+        cr = 0;
+        count = 0;
+        nxt = fetch(lane);
+        for (int32_t c = 0; c < nchunks; ++c) {
+            const float4 cv = nxt;
+            nxt = fetch(((c + 1) << 5) + lane);
+            const float t = cand_tmax<MODE>(cand_share<MODE>(cv.w), qmax);
+            const float band = exact_all ? inf : kBandEps * t * t;
+            const uint32_t m = warp_transpose32(chunk_hits_exact<DIM, MODE>(xc, qsm, sm.qh[w], K4, cv, band), lane);
+            if (lane < nb) {
+                count += __popc(m);
+                if (stage) msk[c * nb + lane] = m;
+            }
+        }
     }
-    if (active) a.counts[qorig] = qcount;
-    if (!stage && lane == 0) {
+    if (active) a.counts[qorig] = (int32_t)count;
+    if (lane == 0 && !stage) {
         a.rec[unit] = -1;
-        int32_t f = atomicAdd(a.num_flagged, 1);
-        a.flagged[f] = unit;
+        if (nchunks > 0) {  // not staged: the emit walk tests the unit again
+            const int32_t f = atomicAdd(a.num_flagged, 1);
+            a.flagged[f] = unit;
+        }
     }
     __syncwarp();
 }
@@ -1492,23 +1468,20 @@ __device__ __forceinline__ uint32_t next_units(const WalkArgs& a, int32_t* count
     return __ballot_sync(0xffffffffu, mine);  // bit k: unit base + k belongs to this launch
 }
 
-// WIN = false: every unit that fits one record window (the others go to the big-unit list);
-// WIN = true: the big-unit list, recorded window by window.
-template <int DIM, bool PERIODIC, int MODE, bool WIN>
+template <int DIM, bool PERIODIC, int MODE>
 __global__ void __launch_bounds__(kWalkWarps * 32, PERIODIC ? kWalkMinBlocksPeriodic : kWalkMinBlocks)
     walk_count_kernel(WalkArgs a) {
-    extern __shared__ __align__(16) unsigned char smem_raw[];
-    WalkSmem& sm = *reinterpret_cast<WalkSmem*>(smem_raw);
+    __shared__ WalkSmem sm;
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-    const int32_t nunits = WIN ? *a.num_big : *a.num_units;
-    int32_t* counter = &a.work[(WIN ? 16 : 0) + (a.class_filter >= 0 ? 2 + a.class_filter : 0)];
+    const int32_t nunits = *a.num_units;
+    int32_t* counter = &a.work[a.class_filter >= 0 ? 2 + a.class_filter : 0];
     int cur = -1;
     for (;;) {
         int32_t base;
-        uint32_t todo = next_units(a, counter, WIN ? a.big : nullptr, nunits, lane, base);
+        uint32_t todo = next_units(a, counter, nullptr, nunits, lane, base);
         if (base >= nunits) break;
         while (todo) {
-            const int32_t unit = WIN ? a.big[base + (__ffs(todo) - 1)] : base + (__ffs(todo) - 1);
+            const int32_t unit = base + (__ffs(todo) - 1);
             todo &= todo - 1;
             const int32_t grp = a.unit_group[unit];
             const int cloud = a.num_clouds == 1 ? 0 : a.group_cloud[grp];
@@ -1522,7 +1495,7 @@ __global__ void __launch_bounds__(kWalkWarps * 32, PERIODIC ? kWalkMinBlocksPeri
                 if (lane == 0) a.rec[unit] = -1;
                 continue;
             }
-            count_unit<DIM, PERIODIC, MODE, WIN>(a, sm, unit, grp, lane, w);
+            count_unit<DIM, PERIODIC, MODE>(a, sm, unit, grp, lane, w);
         }
     }
 }
@@ -1634,17 +1607,22 @@ __global__ void __launch_bounds__(kWalkWarps * 32) walk_emit_kernel(WalkArgs a) 
 }
 
 // Emit pass for staged units: expand each unit's record into its queries' CSR/COO slots, one warp
-// per unit.  Lane q expands query q's hit bits into a shared output table (source chunk and bit of
-// each of the unit's outputs, in output order); then lanes = output positions read the table and
-// write consecutive slots.  A unit with more than kExpandTab outputs locates each output by binary
-// searches over the prefixes instead.
+// per unit, window by window of kExpandWin chunks.  The window's candidate columns are gathered
+// into shared memory once (consecutive sorted indices: coalesced reads of the sort index), lanes
+// over (query, chunk) pairs expand their hit bits into a shared output table (source chunk and bit
+// of every output, in output order), and lanes over output positions write consecutive slots.  A
+// window of more than kExpandTab outputs is written query by query instead.
 constexpr int kExpandWarps = 8;
-constexpr int kExpandTab = 2048;
+constexpr int kExpandWin = 16;    // chunks per window: 512 candidates
+constexpr int kExpandTab = 2048;  // outputs one table holds
 struct ExpandSmem {
-    uint16_t tab[kExpandWarps][kExpandTab];        // (query << 10) | (chunk << 5) | bit, in output order
-    int32_t qpre[kExpandWarps][33];                // exclusive output prefix over queries
-    int64_t qoff[kExpandWarps][32];                // output position of each query's first hit of the window
-    int64_t qbase[kExpandWarps][32];               // the query's row start
+    int32_t col[kExpandWarps][kExpandWin * 32];    // output column of each candidate of the window
+    uint32_t mask[kExpandWarps][kExpandWin * 32];  // the window's masks, [chunk][query]
+    uint16_t tab[kExpandWarps][kExpandTab];        // (query << 9) | (chunk << 5) | bit, in output order
+    int32_t run_beg[kExpandWarps][32];
+    int32_t run_pre[kExpandWarps][33];
+    int32_t qpre[kExpandWarps][33];                // exclusive output prefix over queries (this window)
+    int64_t qoff[kExpandWarps][32];                // output position of each query's next hit
     int32_t qrow[kExpandWarps][32];
 };
 
@@ -1652,14 +1630,14 @@ struct ExpandArgs {
     const int32_t* __restrict__ stage;
     const int32_t* __restrict__ rec;
     const int32_t* __restrict__ num_units;
-    const int32_t* __restrict__ unit_cap;
     const int32_t* __restrict__ unit_t0;
     const int32_t* __restrict__ unit_group;
-    const int32_t* __restrict__ group_start;
     const int32_t* __restrict__ group_cloud;
     const int32_t* __restrict__ qsidx;
+    const int32_t* __restrict__ rsidx;
     const int64_t* __restrict__ offsets;
     const int32_t* __restrict__ query_ids;
+    const int32_t* __restrict__ ref_ids;
     const CloudParams* __restrict__ table;
     int32_t num_clouds;
     int32_t local_index;
@@ -1668,52 +1646,63 @@ struct ExpandArgs {
     int64_t out_cap;
 };
 
-__global__ void __launch_bounds__(kExpandWarps * 32, 5) expand_records_kernel(ExpandArgs a) {
+__global__ void __launch_bounds__(kExpandWarps * 32, 3) expand_records_kernel(ExpandArgs a) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     ExpandSmem& sm = *reinterpret_cast<ExpandSmem*>(smem_raw);
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
     const int32_t nu = *a.num_units;
     const int64_t warps = (int64_t)gridDim.x * kExpandWarps;
-    uint16_t* tab = sm.tab[w];
+    int32_t* __restrict__ rbeg = sm.run_beg[w];
+    int32_t* __restrict__ rpre = sm.run_pre[w];
+    int32_t* __restrict__ cols = sm.col[w];
+    uint32_t* __restrict__ mks = sm.mask[w];
+    uint16_t* __restrict__ tab = sm.tab[w];
     int64_t u = (int64_t)blockIdx.x * kExpandWarps + w;
     int32_t r0n = u < nu ? a.rec[u] : -1;
-    int32_t t0n = u < nu ? a.unit_t0[u] : 0;
-    int32_t gn = u < nu ? a.unit_group[u] : 0;
     for (; u < nu; u += warps) {
-        const int32_t r0 = r0n, t0 = t0n, grp = gn;
-        if (u + warps < nu) {  // the next unit's header, ahead of its use
-            r0n = a.rec[u + warps];
-            t0n = a.unit_t0[u + warps];
-            gn = a.unit_group[u + warps];
+        const int32_t r0 = r0n;
+        if (u + warps < nu) r0n = a.rec[u + warps];  // the next unit's record, ahead of its use
+        if (r0 < 0) continue;  // no candidates, or re-tested by the emit walk
+        const int32_t* rec = a.stage + r0;
+        const int32_t nchunks = rec[0], R = rec[1], nb = rec[2];
+        const uint32_t* masks = reinterpret_cast<const uint32_t*>(rec + kRecHeader + 2 * R + 1);
+        const int32_t t0 = a.unit_t0[u];
+        int32_t rshift = 0, qshift = 0;
+        if (a.local_index) {
+            const CloudParams& cp = a.table[a.num_clouds == 1 ? 0 : a.group_cloud[a.unit_group[u]]];
+            rshift = cp.ref_base;
+            qshift = cp.query_base;
         }
-        if (r0 < 0) continue;  // re-tested by the emit walk
-        const int32_t nchunks_all = a.stage[r0];
-        if (nchunks_all <= 0) continue;  // no candidates, no outputs
-        const int32_t nb = min(*a.unit_cap, a.group_start[grp + 1] - t0);
+        if (lane < R) rbeg[lane] = rec[kRecHeader + lane];
+        if (lane <= R) rpre[lane] = rec[kRecHeader + R + lane];
         if (lane < nb) {
             const int32_t row = a.qsidx[t0 + lane];
-            int32_t qrow = row;
-            if (a.query_ids) qrow = a.query_ids[row];
-            else if (a.local_index) qrow -= a.table[a.num_clouds == 1 ? 0 : a.group_cloud[grp]].query_base;
-            sm.qrow[w][lane] = qrow;
-            sm.qbase[w][lane] = a.offsets[row];
+            sm.qrow[w][lane] = a.query_ids ? a.query_ids[row] : row - qshift;
+            sm.qoff[w][lane] = a.offsets[row];
         }
-        // one window of at most kSegChunks chunks at a time; a window's hits of a query follow the
-        // query's hits of the earlier windows
-        for (int32_t c0 = 0; c0 < nchunks_all; c0 += kSegChunks) {
-            const int32_t win = c0 / kSegChunks;
-            const int32_t nchunks = min(kSegChunks, nchunks_all - c0);
-            const int32_t* r = a.stage + r0 + 1 + (int64_t)win * (nb + (nb + 32) * kSegChunks);
-            const int32_t nm = nb * nchunks;
-            const uint32_t* mk = reinterpret_cast<const uint32_t*>(r + nb);  // [query][chunk]
-            const int32_t* cands = r + nb + nm;                              // [chunk][32]
-            int32_t total = 0;
-            __syncwarp();
-            if (lane < nb) {
-                sm.qoff[w][lane] = sm.qbase[w][lane] + r[lane];
-                for (int c = 0; c < nchunks; ++c) total += __popc(mk[lane * nchunks + c]);
+        __syncwarp();
+        const int32_t M = rpre[R];
+        int32_t cr = 0;  // run of this lane's candidate, moving forward only
+        for (int32_t c0 = 0; c0 < nchunks; c0 += kExpandWin) {
+            const int32_t nc = min(kExpandWin, nchunks - c0);
+            for (int32_t cc = 0; cc < nc; ++cc) {
+                const int32_t k = ((c0 + cc) << 5) + lane;
+                int32_t col = 0;
+                if (k < M) {
+                    while (rpre[cr + 1] <= k) ++cr;
+                    const int32_t jl = __ldg(&a.rsidx[rbeg[cr] + (k - rpre[cr])]);
+                    col = a.ref_ids ? __ldg(&a.ref_ids[jl]) : jl - rshift;
+                }
+                cols[(cc << 5) + lane] = col;
             }
-            const int32_t qinc = warp_inclusive_scan(total);
+            const int32_t nm = nc * nb;
+            const uint32_t* src = masks + (int64_t)c0 * nb;
+            for (int32_t i = lane; i < nm; i += 32) mks[i] = __ldcs(&src[i]);
+            __syncwarp();
+            int32_t tot = 0;
+            if (lane < nb)
+                for (int32_t cc = 0; cc < nc; ++cc) tot += __popc(mks[cc * nb + lane]);
+            const int32_t qinc = warp_inclusive_scan(tot);
             sm.qpre[w][lane + 1] = qinc;
             if (lane == 0) sm.qpre[w][0] = 0;
             const int32_t n = __shfl_sync(0xffffffffu, qinc, 31);
@@ -1721,59 +1710,54 @@ __global__ void __launch_bounds__(kExpandWarps * 32, 5) expand_records_kernel(Ex
                 // lanes over (query, chunk) pairs in output order; each expands its few hit bits
                 int32_t carry = 0;
                 int pq = 0, pc = lane;  // pair (query, chunk) of p = base + lane, advanced without division
-                while (pc >= nchunks) { pc -= nchunks; ++pq; }
+                while (pc >= nc) { pc -= nc; ++pq; }
                 for (int32_t base = 0; base < nm; base += 32) {
-                    const int32_t p = base + lane;
-                    uint32_t m = p < nm ? mk[p] : 0u;
+                    uint32_t m = base + lane < nm ? mks[pc * nb + pq] : 0u;
                     const int32_t cnt = __popc(m);
                     const int32_t inc = warp_inclusive_scan(cnt);
                     int32_t k = carry + inc - cnt;
                     carry += __shfl_sync(0xffffffffu, inc, 31);
-                    const int32_t tag = (pq << 10) | (pc << 5);
+                    const int32_t tag = (pq << 9) | (pc << 5);
                     while (m) {
                         const int bit = __ffs(m) - 1;
                         m &= m - 1;
                         tab[k++] = (uint16_t)(tag | bit);
                     }
                     pc += 32;
-                    while (pc >= nchunks) { pc -= nchunks; ++pq; }
+                    while (pc >= nc) { pc -= nc; ++pq; }
                 }
                 __syncwarp();
 #pragma unroll 4
                 for (int32_t o = lane; o < n; o += 32) {
                     const int32_t v = tab[o];
-                    const int q = v >> 10;
+                    const int q = v >> 9;
                     const int64_t pos = sm.qoff[w][q] + (o - sm.qpre[w][q]);
                     if (pos < a.out_cap) {
-                        a.col_out[pos] = (int64_t)cands[v & 0x3ff];
-                        if (a.row_out) a.row_out[pos] = (int64_t)sm.qrow[w][q];
+                        __stcs(reinterpret_cast<long long*>(&a.col_out[pos]), (long long)cols[v & 0x1ff]);
+                        if (a.row_out) __stcs(reinterpret_cast<long long*>(&a.row_out[pos]), (long long)sm.qrow[w][q]);
                     }
                 }
             } else {
-                __syncwarp();
-                for (int32_t o = lane; o < n; o += 32) {
-                    int lo = 0, hi = nb;  // query: qpre[lo] <= o < qpre[hi]
-                    while (hi - lo > 1) {
-                        const int mid = (lo + hi) >> 1;
-                        if (sm.qpre[w][mid] <= o) lo = mid; else hi = mid;
-                    }
-                    const int q = lo;
-                    int32_t tq = o - sm.qpre[w][q];
-                    int c = 0;  // chunk holding the query's tq-th hit (tq < hits of q, so c < nchunks)
-                    for (; c < nchunks; ++c) {
-                        const int32_t pcnt = __popc(mk[q * nchunks + c]);
-                        if (tq < pcnt) break;
-                        tq -= pcnt;
-                    }
-                    if (c >= nchunks) continue;
-                    const int bit = __fns(mk[q * nchunks + c], 0, tq + 1);
-                    const int64_t pos = sm.qoff[w][q] + (o - sm.qpre[w][q]);
-                    if (pos < a.out_cap) {
-                        a.col_out[pos] = (int64_t)cands[c * 32 + bit];
-                        if (a.row_out) a.row_out[pos] = (int64_t)sm.qrow[w][q];
+                // many outputs: query by query, lanes over the window's chunks
+                for (int32_t q = 0; q < nb; ++q) {
+                    uint32_t m = lane < nc ? mks[lane * nb + q] : 0u;
+                    const int32_t cnt = __popc(m);
+                    const int32_t inc = warp_inclusive_scan(cnt);
+                    int64_t pos = sm.qoff[w][q] + (inc - cnt);
+                    const long long row = sm.qrow[w][q];
+                    while (m) {
+                        const int bit = __ffs(m) - 1;
+                        m &= m - 1;
+                        if (pos < a.out_cap) {
+                            a.col_out[pos] = (int64_t)cols[(lane << 5) + bit];
+                            if (a.row_out) a.row_out[pos] = row;
+                        }
+                        ++pos;
                     }
                 }
             }
+            __syncwarp();
+            if (lane < nb) sm.qoff[w][lane] += tot;
             __syncwarp();
         }
     }
@@ -2214,8 +2198,6 @@ static WalkArgs make_walk(const HostBatch& b, const Structure& S, const Scratch&
     a.flagged = W.flagged;
     a.num_flagged = W.num_flagged;
     a.num_exact = W.num_exact;
-    a.big = W.big;
-    a.num_big = W.num_big;
     a.cursor = W.cursor;
     a.query_ids = b.query_ids;
     a.ref_ids = b.ref_ids;
@@ -2260,21 +2242,8 @@ static cudaError_t ensure_smem(F* kernel, int bytes, uint64_t* done_mask) {
 
 template <int D, bool P, int M>
 struct CountLaunch {
-    static cudaError_t launch(const WalkArgs& a, dim3 g, dim3 b, size_t smem, cudaStream_t st) {
-        static uint64_t done = 0;
-        cudaError_t e = ensure_smem(walk_count_kernel<D, P, M, false>, (int)smem, &done);
-        if (e != cudaSuccess) return e;
-        walk_count_kernel<D, P, M, false><<<g, b, smem, st>>>(a);
-        return cudaGetLastError();
-    }
-};
-template <int D, bool P, int M>
-struct CountWindowedLaunch {
-    static cudaError_t launch(const WalkArgs& a, dim3 g, dim3 b, size_t smem, cudaStream_t st) {
-        static uint64_t done = 0;
-        cudaError_t e = ensure_smem(walk_count_kernel<D, P, M, true>, (int)smem, &done);
-        if (e != cudaSuccess) return e;
-        walk_count_kernel<D, P, M, true><<<g, b, smem, st>>>(a);
+    static cudaError_t launch(const WalkArgs& a, dim3 g, dim3 b, size_t, cudaStream_t st) {
+        walk_count_kernel<D, P, M><<<g, b, 0, st>>>(a);
         return cudaGetLastError();
     }
 };
@@ -2441,9 +2410,7 @@ static int count_impl(const HostBatch& b, const Structure& S, const Scratch& W, 
         a.stage = stage;
         a.stage_cap = stage_cap;
         prof_mark(TCR_PROFILE_COUNT_WALK, 0, st);
-        TCR_CUDA(launch_walks<CountLaunch>(b, a, dim3(walk_blocks(nq)), dim3(kWalkWarps * 32), sizeof(WalkSmem), st));
-        TCR_CUDA(launch_walks<CountWindowedLaunch>(b, a, dim3(walk_blocks(nq)), dim3(kWalkWarps * 32),
-                                                   sizeof(WalkSmem), st));
+        TCR_CUDA(launch_walks<CountLaunch>(b, a, dim3(walk_blocks(nq)), dim3(kWalkWarps * 32), 0, st));
         prof_mark(TCR_PROFILE_COUNT_WALK, 1, st);
         stray_kernel<false><<<grid_for(nq, 128, num_sms() * 4), 128, 0, st>>>(a);
         note_launches(1);
@@ -2477,14 +2444,14 @@ static int emit_impl(const HostBatch& b, const Structure& S, const Scratch& W, c
         e.stage = stage;
         e.rec = W.rec;
         e.num_units = W.num_units;
-        e.unit_cap = W.unit_cap;
         e.unit_t0 = W.unit_t0;
         e.unit_group = W.unit_group;
-        e.group_start = a.group_start;
         e.group_cloud = a.group_cloud;
         e.qsidx = a.qsidx;
+        e.rsidx = S.rsidx;
         e.offsets = offsets;
         e.query_ids = b.query_ids;
+        e.ref_ids = b.ref_ids;
         e.table = W.table;
         e.num_clouds = b.C;
         e.local_index = b.local_index;
