@@ -19,7 +19,7 @@ import numpy as np
 import torch
 
 from . import _lib
-from .search import _as_f32, _domain_host, _ptr, _require_cuda
+from .search import _as_f32, _check_device_fault, _domain_host, _ptr, _require_cuda
 from .util import DomainDescription, PointCloud, SparseCOO, SparseCSR
 
 CLOUD_DTYPE = np.dtype([("dim", "<i4"), ("periodic_mask", "<i4"), ("domain_min", "<f4", (3,)),
@@ -134,6 +134,7 @@ def run_batch(table, mode, self_search, fmt, device, local_index=True, query_ids
                                   _ptr(row), _ptr(col), cap, sptr), "tcr_batch_emit")
     mark("emit", True)
     stream.synchronize()
+    _check_device_fault(info)
     if int(info[1]) != 0:
         raise ValueError(f"{int(info[1])} cloud(s) have no valid cell grid for their domain and support (the "
                          "support is not smaller than the domain extent, or a support/domain value is not finite)")

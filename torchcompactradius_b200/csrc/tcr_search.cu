@@ -83,6 +83,7 @@ struct Structure {
     GridParams* grid;         // [C] per cloud
     int32_t* num_cells;       // [1]
     int32_t* bad_grids;       // [1] clouds with points on both sides and no valid grid
+    int32_t* fault;           // [1] a bounded wait of the build gave up (its result is not valid)
     float4* rsorted;          // [nr] wrapped reference points in (cloud, cell) order, .w = support
     int32_t* rsidx;           // [nr] global index of each sorted point
     int32_t* cell_start;      // [nr+1]
@@ -100,6 +101,7 @@ static Structure carve_structure(void* buf, int64_t nr, int64_t C, int64_t map_t
     s.grid = c.take<GridParams>(C);
     s.num_cells = c.take<int32_t>(1);
     s.bad_grids = c.take<int32_t>(1);
+    s.fault = c.take<int32_t>(1);
     s.rsorted = c.take<float4>(nr);
     s.rsidx = c.take<int32_t>(nr);
     s.cell_start = c.take<int32_t>(nr + 1);
@@ -112,6 +114,10 @@ static Structure carve_structure(void* buf, int64_t nr, int64_t C, int64_t map_t
     if (bytes) *bytes = c.off;
     return s;
 }
+
+// Scans of one phase (build: the incremental build's unmoved points, the cell table; count: query
+// groups, work units, offsets), each with its own look-back slot; the phase's init kernel zeroes them.
+constexpr int kScanSlots = 3;
 
 // Per-search scratch.
 struct Scratch {
@@ -134,10 +140,11 @@ struct Scratch {
     float4* pack;           // [max(nq,nr)] packed input points before sorting
     void* keys[2];          // [max(nq,nr)] 64-bit slots (32-bit keys use the first half)
     int32_t* vals[2];
-    int32_t* hist;
-    int32_t* tile_sums;
-    int64_t* scan_tiles64;  // [scan_tiles(max)]
-    int32_t* scan_tiles32;  // [scan_tiles(max)]
+    unsigned long long* sort_status;  // [sort_status_words(max)] look-back words of the radix sorts
+    unsigned long long* scan_status;  // [kScanSlots][scan_tiles(max + 1)] look-back words of a phase's scans
+    int32_t* scan_ticket;             // [kScanSlots]
+    int32_t* fault;                   // [1] a bounded wait of the query phases gave up
+    int64_t scan_stride;              // scan_tiles(max + 1): words per scan slot
     float4* qsorted;        // [nq]
     int32_t* qsidx;         // [nq] global query index of each sorted query
     int32_t* qgroup_start;  // [nq+1]
@@ -184,10 +191,11 @@ static Scratch carve_scratch(void* buf, int64_t nq, int64_t nr, int64_t C, bool 
     s.keys[1] = c.take<unsigned long long>(nmax);
     s.vals[0] = c.take<int32_t>(nmax);
     s.vals[1] = c.take<int32_t>(nmax);
-    s.hist = c.take<int32_t>(sort_hist_elems(nmax));
-    s.tile_sums = c.take<int32_t>(scan_tiles(sort_hist_elems(nmax)));
-    s.scan_tiles64 = c.take<int64_t>(scan_tiles(nmax + 1));
-    s.scan_tiles32 = c.take<int32_t>(scan_tiles(nmax + 1));
+    s.sort_status = c.take<unsigned long long>(sort_status_words(nmax));
+    s.scan_stride = scan_tiles(nmax + 1);
+    s.scan_status = c.take<unsigned long long>(kScanSlots * s.scan_stride);
+    s.scan_ticket = c.take<int32_t>(kScanSlots);
+    s.fault = c.take<int32_t>(1);
     const int64_t q = std::max<int64_t>(nq, 1);
     s.qsorted = c.take<float4>(q);
     s.qsidx = c.take<int32_t>(q);
@@ -221,10 +229,14 @@ static SortWorkspaceT<K> sort_workspace(const Scratch& W) {
     s.keys[1] = reinterpret_cast<K*>(W.keys[1]);
     s.vals[0] = W.vals[0];
     s.vals[1] = W.vals[1];
-    s.hist = W.hist;
-    s.tile_sums = W.tile_sums;
+    s.status = W.sort_status;
     s.state = reinterpret_cast<SortStateT<K>*>(W.sort_state);
+    s.fault = W.fault;
     return s;
+}
+
+static LookbackSlot lookback_slot(const Scratch& W, int k, int32_t* fault) {
+    return LookbackSlot{W.scan_status + k * W.scan_stride, W.scan_ticket + k, fault};
 }
 
 // ------------------------------------------------------------------------------------------
@@ -342,8 +354,16 @@ __global__ void support_stats_kernel(const CloudParams* __restrict__ table, cons
     }
 }
 
+// Zeroes a phase's look-back slots (statuses and tickets) and its fault word.
+__device__ __forceinline__ void zero_lookback(const Scratch& W, int32_t* fault) {
+    zero_words(W.scan_status, kScanSlots * W.scan_stride);
+    if (blockIdx.x == 0 && threadIdx.x < kScanSlots) W.scan_ticket[threadIdx.x] = 0;
+    if (blockIdx.x == 0 && threadIdx.x == 0) *fault = 0;
+}
+
+// Start of a build: per-cloud statistics and flags, counters, the sort state, the look-back slots.
 template <typename K>
-__global__ void grid_init_kernel(GridParams* g, int C, int32_t* bad_grids, SortStateT<K>* st) {
+__global__ void grid_init_kernel(GridParams* g, int C, Structure S, Scratch W) {
     for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < C; c += gridDim.x * blockDim.x) {
         g[c].ref_stats.max_key = 0;
         g[c].ref_stats.bad = 0;
@@ -352,9 +372,14 @@ __global__ void grid_init_kernel(GridParams* g, int C, int32_t* bad_grids, SortS
         g[c].error = 0;
         g[c].out_of_grid = 0;
     }
-    if (blockIdx.x == 0 && threadIdx.x == 0) {
-        *bad_grids = 0;
-        sort_state_reset(st);
+    zero_lookback(W, S.fault);
+    if (blockIdx.x == 0) {
+        if (threadIdx.x == 0) {
+            *S.bad_grids = 0;
+            *S.num_cells = 0;
+            S.cell_start[0] = 0;  // no reference points: no cells
+        }
+        sort_state_reset(reinterpret_cast<SortStateT<K>*>(W.sort_state));
     }
 }
 
@@ -362,12 +387,14 @@ template <typename K>
 __global__ void sort_state_init_kernel(SortStateT<K>* st) { sort_state_reset(st); }
 
 // Per cloud: util.py:28-79 compute_h and cellTable.py:27-29, float32 throughout.
+// same_sup: the query supports are the reference support array (statistics reduced once).
 __global__ void grid_params_kernel(const CloudParams* __restrict__ table, GridParams* grid, int C,
-                                   int32_t* bad_grids) {
+                                   int32_t* bad_grids, int same_sup) {
     const float grow = 1.00010001659393310546875f;  // fl32(1e-4 + 1)
     for (int cl = blockIdx.x * blockDim.x + threadIdx.x; cl < C; cl += gridDim.x * blockDim.x) {
         const CloudParams& sp = table[cl];
         GridParams* g = &grid[cl];
+        if (same_sup) g->build_query_stats = g->ref_stats;
         // computeGridSupport: scatter reads the reference supports, gather the query supports,
         // (super)symmetric both (torch.max propagates NaN, as the key maximum does).
         uint32_t key = 0;
@@ -439,11 +466,14 @@ __global__ void grid_params_kernel(const CloudParams* __restrict__ table, GridPa
 }
 
 // Per cloud: the query-side parameters of the lean test.
+// same_sup: the queries are the reference points with the same support array, whose statistics the
+// build reduced already.
 __global__ void query_params_kernel(const CloudParams* __restrict__ table, const GridParams* __restrict__ grid, int C,
-                                    QueryParams* qp, int32_t* exact_clouds) {
+                                    QueryParams* qp, int32_t* exact_clouds, int same_sup) {
     for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < C; c += gridDim.x * blockDim.x) {
         const CloudParams& cp = table[c];
         QueryParams& q = qp[c];
+        if (same_sup) q.stats = grid[c].ref_stats;
         const bool has_q = cp.query_sup != nullptr;
         const float qmax = has_q ? key_float(q.stats.max_key) : 0.0f;
         q.qmax = (cp.mode == kScatter) ? 0.0f : qmax;
@@ -454,12 +484,16 @@ __global__ void query_params_kernel(const CloudParams* __restrict__ table, const
     }
 }
 
-// Zeroes the per-search counters and the per-cloud query statistics.
-__global__ void count_init_kernel(Scratch W, int C, int unit_cap) {
+// Zeroes the per-search counters, the per-cloud query statistics, the per-query counts and the
+// look-back slots of the query phases.
+__global__ void count_init_kernel(Scratch W, int C, int unit_cap, int64_t nq) {
     for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < C; c += gridDim.x * blockDim.x) {
         W.qparams[c].stats.max_key = 0;
         W.qparams[c].stats.bad = 0;
     }
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < nq; i += (int64_t)gridDim.x * blockDim.x)
+        W.counts[i] = 0;
+    zero_lookback(W, W.fault);
     if (blockIdx.x == 0 && threadIdx.x == 0) {
         for (int k = 0; k < kWorkCounters; ++k) W.work[k] = 0;
         *W.num_stray = 0;
@@ -672,6 +706,8 @@ struct CellOut {
     int32_t* cell_bucket;
     int32_t* cell_cloud;
     unsigned long long* map;
+    int32_t n_points;
+    __device__ void finish(int64_t cells) const { cell_start[cells] = n_points; }  // end of the last cell
     __device__ void operator()(int64_t i, int32_t ex, int32_t flag) const {
         if (!flag) return;
         const K* k = st->sel[key_passes<K>()] ? keys1 : keys0;
@@ -734,6 +770,7 @@ struct StayIn {
 };
 template <typename K>
 struct StayOut {
+    __device__ void finish(int64_t) const {}
     const K* keys;        // the pack output, input order
     K* stay_keys;
     int32_t* stay_idx;
@@ -760,12 +797,15 @@ __global__ void inc_check_kernel(const K* __restrict__ stay_keys, const int32_t*
     if (!__all_sync(0xffffffffu, ok) && (threadIdx.x & 31) == 0) atomicOr(bad, 1);
 }
 
-// Chooses the path: the moved points' sort and the merge, or the full sort (one thread).
+// Chooses the path: the moved points' sort and the merge, or the full sort (one block; its thread
+// 0 decides).
 template <typename K>
 __global__ void inc_decide_kernel(SortStateT<K>* full, SortStateT<K>* moved, const int32_t* counts, int64_t n) {
     const int64_t n_stay = counts[0];
     const bool fallback = counts[1] != 0 || 2 * n_stay < n;  // wrong hint, or most points moved
     sort_state_reset(moved);
+    __syncthreads();
+    if (threadIdx.x != 0) return;
     if (fallback) {
         moved->key_min = moved->key_max = 0;  // no moved sort
         return;
@@ -820,10 +860,6 @@ __global__ void inc_merge_kernel(const K* __restrict__ stay_keys, const int32_t*
     }
 }
 
-__global__ void finish_cells_kernel(int32_t* cell_start, const int32_t* num_cells, int64_t n) {
-    cell_start[*num_cells] = (int32_t)n;
-}
-
 // ------------------------------------------------------------------------------------------
 // query side
 
@@ -857,6 +893,8 @@ struct QueryGroupOut {
     int32_t* group_start;
     int32_t* group_coords;
     int32_t* group_cloud;
+    int32_t n_points;
+    __device__ void finish(int64_t groups) const { group_start[groups] = n_points; }  // end of the last group
     __device__ void operator()(int64_t i, int32_t ex, int32_t flag) const {
         if (!flag) return;
         const K* k = st->sel[key_passes<K>()] ? keys1 : keys0;
@@ -886,6 +924,7 @@ struct BoundedUnitCountIn {
     }
 };
 struct BoundedUnitOut {
+    __device__ void finish(int64_t) const {}
     const int32_t* group_start;
     const int32_t* num_groups;
     int32_t* unit_group;
@@ -1919,6 +1958,7 @@ struct CountIn {
     __device__ int64_t operator()(int64_t i) const { return i < n ? (int64_t)counts[i] : 0; }
 };
 struct OffsetOut {
+    __device__ void finish(int64_t) const {}
     int64_t n;
     int64_t* offsets;
     int32_t* indptr;
@@ -1930,11 +1970,12 @@ struct OffsetOut {
     }
 };
 
-__global__ void info_kernel(const int32_t* bad_grids, const int64_t* total, const int32_t* num_stray,
+__global__ void info_kernel(const int32_t* bad_grids, const int32_t* build_fault, const int32_t* fault,
+                            const int64_t* total, const int32_t* num_stray,
                             const int32_t* exact_clouds, const unsigned long long* cursor, const int32_t* num_flagged,
                             const int32_t* num_exact, const int32_t* inc_count, int64_t n_ref, int64_t* info) {
     info[0] = *total;
-    info[1] = *bad_grids;
+    info[1] = (*build_fault || *fault) ? -1 : *bad_grids;  // -1: a bounded wait gave up
     info[2] = *num_stray;
     info[3] = *exact_clouds;
     info[4] = (int64_t)*cursor;
@@ -2285,12 +2326,14 @@ static unsigned walk_blocks(int64_t nq) {
 
 template <typename K>
 static int build_impl(const HostBatch& b, const Structure& S, const Scratch& W, cudaStream_t st) {
-    const SortWorkspaceT<K> sw = sort_workspace<K>(W);
+    SortWorkspaceT<K> sw = sort_workspace<K>(W);
+    sw.fault = S.fault;  // the build's waits report into the structure
     const int C = b.C;
     const int64_t nr = b.nr, nq = b.nq;
     int rc = upload_table(b, W, st);
     if (rc) return rc;
-    grid_init_kernel<K><<<grid_for(C, 128), 128, 0, st>>>(S.grid, C, S.bad_grids, sw.state);
+    grid_init_kernel<K><<<grid_for(std::max<int64_t>(C, kScanSlots * W.scan_stride), 256), 256, 0, st>>>(S.grid, C, S,
+                                                                                                       W);
     note_launches(1);
     // computeGridSupport: which supports set hMax depends on the mode
     if (b.any_ref_sup && nr > 0) {
@@ -2299,16 +2342,15 @@ static int build_impl(const HostBatch& b, const Structure& S, const Scratch& W, 
             (int64_t)sizeof(GridParams));
         note_launches(1);
     }
-    if (b.any_query_sup && nq > 0) {
+    if (b.any_query_sup && nq > 0 && !b.same_sorted) {
         support_stats_kernel<<<grid_for(nq, 256, num_sms() * 8), 256, 0, st>>>(
             W.table, W.query_prefix, C, nq, 1,
             reinterpret_cast<char*>(S.grid) + offsetof(GridParams, build_query_stats), (int64_t)sizeof(GridParams));
         note_launches(1);
     }
-    grid_params_kernel<<<grid_for(C, 128), 128, 0, st>>>(W.table, S.grid, C, S.bad_grids);
+    grid_params_kernel<<<grid_for(C, 128), 128, 0, st>>>(W.table, S.grid, C, S.bad_grids, b.same_sorted ? 1 : 0);
     note_launches(1);
     TCR_CUDA(cudaMemsetAsync(S.map, 0xff, sizeof(unsigned long long) * S.map_total, st));
-    TCR_CUDA(cudaMemsetAsync(S.num_cells, 0, sizeof(int32_t), st));
     if (nr > 0) {
         const bool inc = b.lin_hint != nullptr;
         pack_points_kernel<K><<<grid_for(nr, 256), 256, 0, st>>>(W.table, S.grid, W.ref_prefix, C, nr, 0, 2, 1, W.pack,
@@ -2324,10 +2366,10 @@ static int build_impl(const HostBatch& b, const Structure& S, const Scratch& W, 
             mw.state = reinterpret_cast<SortStateT<K>*>(W.moved_state);
             TCR_CUDA(cudaMemsetAsync(W.inc_count, 0, 2 * sizeof(int32_t), st));
             StayOut<K> so{sw.keys[0], reinterpret_cast<K*>(W.stay_keys), W.stay_idx, mw.keys[0], mw.vals[0]};
-            TCR_CUDA(device_exclusive_scan<int32_t>(StayIn{W.stay}, so, nr, W.scan_tiles32, W.inc_count, st));
+            TCR_CUDA(device_exclusive_scan<int32_t>(StayIn{W.stay}, so, nr, lookback_slot(W, 0, S.fault), W.inc_count, st));
             inc_check_kernel<K><<<grid_for(nr, 256), 256, 0, st>>>(reinterpret_cast<const K*>(W.stay_keys),
                                                                    W.inc_count, W.inc_count + 1);
-            inc_decide_kernel<K><<<1, 1, 0, st>>>(sw.state, mw.state, W.inc_count, nr);
+            inc_decide_kernel<K><<<1, 256, 0, st>>>(sw.state, mw.state, W.inc_count, nr);
             note_launches(2);
             TCR_CUDA(radix_sort_pairs<K>(mw, nr, st));
             inc_merge_kernel<K><<<grid_for(nr, 256), 256, 0, st>>>(
@@ -2341,12 +2383,10 @@ static int build_impl(const HostBatch& b, const Structure& S, const Scratch& W, 
                                                                    b.lin_out, b.order_out);
         note_launches(1);
         CellOut<K> co{W.table, S.grid, sw.keys[0], sw.keys[1], sw.state, S.rsorted, S.cell_start, S.cell_lin,
-                      S.cell_coords, S.cell_bucket, S.cell_cloud, S.map};
+                      S.cell_coords, S.cell_bucket, S.cell_cloud, S.map, (int32_t)nr};
         RunFlagIn<K> fi{sw.keys[0], sw.keys[1], sw.state};
-        TCR_CUDA(device_exclusive_scan<int32_t>(fi, co, nr, W.scan_tiles32, S.num_cells, st));
+        TCR_CUDA(device_exclusive_scan<int32_t>(fi, co, nr, lookback_slot(W, 1, S.fault), S.num_cells, st));
     }
-    finish_cells_kernel<<<1, 1, 0, st>>>(S.cell_start, S.num_cells, nr);
-    note_launches(1);
     TCR_CUDA(cudaGetLastError());
     return TCR_OK;
 }
@@ -2360,18 +2400,19 @@ static int count_impl(const HostBatch& b, const Structure& S, const Scratch& W, 
     int rc = upload_table(b, W, st);
     if (rc) return rc;
     const int unit_cap = g_unit_cap;
-    count_init_kernel<<<grid_for(C, 128), 128, 0, st>>>(W, C, unit_cap);
+    count_init_kernel<<<grid_for(std::max<int64_t>({(int64_t)C, nq, kScanSlots * W.scan_stride}), 256), 256, 0, st>>>(
+        W, C, unit_cap, nq);
     note_launches(1);
-    if (b.any_query_sup && nq > 0) {
+    if (b.any_query_sup && nq > 0 && !b.same_sorted) {
         support_stats_kernel<<<grid_for(nq, 256, num_sms() * 8), 256, 0, st>>>(
             W.table, W.query_prefix, C, nq, 1, reinterpret_cast<char*>(W.qparams) + offsetof(QueryParams, stats),
             (int64_t)sizeof(QueryParams));
         note_launches(1);
     }
-    query_params_kernel<<<grid_for(C, 128), 128, 0, st>>>(W.table, S.grid, C, W.qparams, W.exact_clouds);
+    query_params_kernel<<<grid_for(C, 128), 128, 0, st>>>(W.table, S.grid, C, W.qparams, W.exact_clouds,
+                                                          b.same_sorted ? 1 : 0);
     note_launches(1);
     if (nq > 0) {
-        TCR_CUDA(cudaMemsetAsync(W.counts, 0, sizeof(int32_t) * nq, st));
         const int32_t* gstart;
         const int32_t* ngroups;
         if (b.self) {
@@ -2385,7 +2426,7 @@ static int count_impl(const HostBatch& b, const Structure& S, const Scratch& W, 
         } else {
             // sort the queries by their own (cloud, cell)
             const SortWorkspaceT<K> sw = sort_workspace<K>(W);
-            sort_state_init_kernel<K><<<1, 1, 0, st>>>(sw.state);
+            sort_state_init_kernel<K><<<1, 256, 0, st>>>(sw.state);
             note_launches(1);
             pack_points_kernel<K><<<grid_for(nq, 256), 256, 0, st>>>(W.table, S.grid, W.query_prefix, C, nq, 1, 1, 0,
                                                                      W.pack, sw.keys[0], sw.vals[0], sw.state);
@@ -2395,17 +2436,15 @@ static int count_impl(const HostBatch& b, const Structure& S, const Scratch& W, 
                                                                        W.qsorted, W.qsidx);
             note_launches(1);
             QueryGroupOut<K> qo{W.table, S.grid, sw.keys[0], sw.keys[1], sw.state, W.qsorted,
-                                W.qgroup_start, W.qgroup_coords, W.qgroup_cloud};
+                                W.qgroup_start, W.qgroup_coords, W.qgroup_cloud, (int32_t)nq};
             RunFlagIn<K> fi{sw.keys[0], sw.keys[1], sw.state};
-            TCR_CUDA(device_exclusive_scan<int32_t>(fi, qo, nq, W.scan_tiles32, W.num_qgroups, st));
-            finish_cells_kernel<<<1, 1, 0, st>>>(W.qgroup_start, W.num_qgroups, nq);
-            note_launches(1);
+            TCR_CUDA(device_exclusive_scan<int32_t>(fi, qo, nq, lookback_slot(W, 0, W.fault), W.num_qgroups, st));
             gstart = W.qgroup_start;
             ngroups = W.num_qgroups;
         }
         BoundedUnitCountIn ui{gstart, ngroups, unit_cap};
         BoundedUnitOut uo{gstart, ngroups, W.unit_group, W.unit_t0, unit_cap};
-        TCR_CUDA(device_exclusive_scan<int32_t>(ui, uo, nq, W.scan_tiles32, W.num_units, st));
+        TCR_CUDA(device_exclusive_scan<int32_t>(ui, uo, nq, lookback_slot(W, 1, W.fault), W.num_units, st));
         WalkArgs a = make_walk(b, S, W);
         a.stage = stage;
         a.stage_cap = stage_cap;
@@ -2417,8 +2456,8 @@ static int count_impl(const HostBatch& b, const Structure& S, const Scratch& W, 
     }
     CountIn ci{W.counts, nq};
     OffsetOut oo{nq, offsets, indptr_out, row_entries_out};
-    TCR_CUDA(device_exclusive_scan<int64_t>(ci, oo, nq + 1, W.scan_tiles64, W.total, st));
-    info_kernel<<<1, 1, 0, st>>>(S.bad_grids, W.total, W.num_stray, W.exact_clouds, W.cursor, W.num_flagged,
+    TCR_CUDA(device_exclusive_scan<int64_t>(ci, oo, nq + 1, lookback_slot(W, 2, W.fault), W.total, st));
+    info_kernel<<<1, 1, 0, st>>>(S.bad_grids, S.fault, W.fault, W.total, W.num_stray, W.exact_clouds, W.cursor, W.num_flagged,
                                  W.num_exact, b.lin_hint && b.nr > 0 ? W.inc_count : nullptr, b.nr, W.info);
     note_launches(1);
     if (info_out) TCR_CUDA(cudaMemcpyAsync(info_out, W.info, 8 * sizeof(int64_t), cudaMemcpyDeviceToHost, st));
@@ -2671,8 +2710,9 @@ int tcr_count_f64(const tcr_search_desc* d, const tcr_f64_inputs* in, const void
     cudaStream_t st = (cudaStream_t)stream;
     rc = upload_table(b, W, st);
     if (rc) return rc;
-    count_init_kernel<<<1, 128, 0, st>>>(W, b.C, g_unit_cap);
-    query_params_kernel<<<1, 128, 0, st>>>(W.table, S.grid, b.C, W.qparams, W.exact_clouds);
+    count_init_kernel<<<grid_for(std::max<int64_t>({(int64_t)b.C, b.nq, kScanSlots * W.scan_stride}), 256), 256, 0,
+                        st>>>(W, b.C, g_unit_cap, b.nq);
+    query_params_kernel<<<1, 128, 0, st>>>(W.table, S.grid, b.C, W.qparams, W.exact_clouds, 0);
     note_launches(2);
     const int64_t nq = b.nq;
     if (b.nr > 0) {
@@ -2686,8 +2726,8 @@ int tcr_count_f64(const tcr_search_desc* d, const tcr_f64_inputs* in, const void
     }
     CountIn ci{W.counts, nq};
     OffsetOut oo{nq, offsets, indptr_out, row_entries_out};
-    TCR_CUDA(device_exclusive_scan<int64_t>(ci, oo, nq + 1, W.scan_tiles64, W.total, st));
-    info_kernel<<<1, 1, 0, st>>>(S.bad_grids, W.total, W.num_stray, W.exact_clouds, W.cursor, W.num_flagged,
+    TCR_CUDA(device_exclusive_scan<int64_t>(ci, oo, nq + 1, lookback_slot(W, 2, W.fault), W.total, st));
+    info_kernel<<<1, 1, 0, st>>>(S.bad_grids, S.fault, W.fault, W.total, W.num_stray, W.exact_clouds, W.cursor, W.num_flagged,
                                  W.num_exact, nullptr, b.nr, W.info);
     note_launches(1);
     if (info_out) TCR_CUDA(cudaMemcpyAsync(info_out, W.info, 8 * sizeof(int64_t), cudaMemcpyDeviceToHost, st));

@@ -22,7 +22,7 @@ import torch
 
 from . import _lib
 from .batched import batch_desc, cloud_table
-from .search import _as_f32, _domain_host, _ptr, _require_cuda
+from .search import _as_f32, _check_device_fault, _domain_host, _ptr, _require_cuda
 from .util import DomainDescription, PointCloud, SparseCOO, SparseCSR
 
 
@@ -105,6 +105,7 @@ class SearchPlan:
         self.graph = g
 
     def _check(self):
+        _check_device_fault(self.info)
         if int(self.info[1]) != 0:
             raise ValueError(f"{int(self.info[1])} cloud(s) have no valid cell grid for their domain and support")
 

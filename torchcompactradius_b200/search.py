@@ -228,7 +228,16 @@ class CompactHashMap:
         return f"CompactHashMap(n={self._n}, dim={self._dim}, hashMapLength={self.hashMapLength})"
 
 
+def _check_device_fault(info):
+    """info[1] == -1: a bounded wait inside a one-pass scan or sort gave up (the device did not make
+    progress); the result is not valid."""
+    if int(info[1]) < 0:
+        raise RuntimeError("a device-wide scan or sort of the search did not complete (a bounded wait gave up); "
+                           "the result is not valid")
+
+
 def _check_info(info):
+    _check_device_fault(info)
     if int(info[1]) != 0:
         raise ValueError("no valid cell grid for this domain and support (the support is not smaller than the "
                          "domain extent, or a support/domain value is not finite)")
