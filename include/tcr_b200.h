@@ -20,7 +20,7 @@
 extern "C" {
 #endif
 
-#define TCR_ABI_VERSION 8
+#define TCR_ABI_VERSION 9
 
 #define TCR_OK 0
 #define TCR_ERR_INVALID (-1) /* bad argument or workspace too small */
@@ -187,14 +187,15 @@ int tcr_build_structure(const tcr_search_desc* d, void* structure, int64_t struc
 
 /* Counts the neighbours of every query and scans them.  Replaces the countNeighbors operator
  * (cppSrc/neighborhood.h:140-146, cppWrapper.cpp:39) plus the cumsum of cppSearch.py:81-84.
- * Every (query, candidate) pair is tested once here: each work unit (<= 32 queries of one cell
- * with <= 768 candidates) writes a record of its hit masks and candidate indices to `stage`
- * (device int32, stage_capacity words) for tcr_emit to expand into place.  Units that do not fit
- * (or every unit when stage is NULL / capacity 0) are tested again by tcr_emit.
+ * Every (query, candidate) pair is tested once here: each work unit (<= 32 queries of one cell)
+ * writes a record of its candidate runs and of one 32-bit hit mask per (query, 32 candidates) to
+ * `stage` (device int32, stage_capacity words) for tcr_emit to expand into place.  Units that do
+ * not fit (or every unit when stage is NULL / capacity 0) are tested again by tcr_emit.
  * offsets: device int64 [n_query+1] (exclusive scan, offsets[n_query] = total pairs).
  * indptr_out (device int32 [n_query+1]) and row_entries_out (device int64 [n_query]) are the
  * SparseCSR fields of util.py:321-358 and may be NULL.  info_out (host, 8 x int64, may be NULL)
- * receives, asynchronously on `stream`: {total pairs, grid error flag, queries walked serially,
+ * receives, asynchronously on `stream`: {total pairs, clouds without a valid grid (-1: a bounded
+ * wait of a device-wide scan or sort gave up and nothing of the search is valid), queries walked serially,
  * exact-only mode, staging words the units asked for, units left for tcr_emit to re-test, units
  * re-tested with exact decisions because a pair lay within the fast test's rounding band, and
  * for a batch built with a linear-cell hint the points its incremental re-sort sorted (-1: it fell
@@ -257,8 +258,10 @@ int tcr_search_noalloc(const tcr_search_desc* d, int64_t* offsets, int32_t* indp
  * moduloOp, the squared sum, sqrt and the threshold in double.  These two calls replace tcr_count /
  * tcr_emit for such inputs.  The structure is built by tcr_build_structure from float32 copies of
  * the wrapped positions and supports, with hcell set to a cell size no smaller than the reference's
- * double hCell (so every pair within the double support lies in a query's 3^d stencil); each
- * candidate is then decided on the double arrays below by the reference's double expression.
+ * double hCell (so every pair within the double support lies in a query's 3^d stencil); the walks
+ * test candidates on the float32 copies and decide every pair whose float32 test lies within the
+ * copies' rounding of the threshold on the double arrays below, by the reference's double
+ * expression.
  * ------------------------------------------------------------------------------------------- */
 typedef struct tcr_f64_inputs {
     const double* query_pos;  /* device [n_query*dim], wrapped as the reference wraps queries
@@ -274,16 +277,18 @@ typedef struct tcr_f64_inputs {
 } tcr_f64_inputs;
 
 /* countNeighbors at scalar_t = double (neighborhoodDynamic.h:37-74) + the offsets scan; d describes
- * the float32 copies the structure was built from (hcell > 0, clamped_grid 0). */
+ * the float32 copies the structure was built from (hcell > 0, clamped_grid 0).  stage and the other
+ * arguments as in tcr_count. */
 int tcr_count_f64(const tcr_search_desc* d, const tcr_f64_inputs* in, const void* structure, void* scratch,
-                  int64_t scratch_bytes, int64_t* offsets, int32_t* indptr_out, int64_t* row_entries_out,
-                  int64_t* info_out, void* stream);
+                  int64_t scratch_bytes, int32_t* stage, int64_t stage_capacity, int64_t* offsets,
+                  int32_t* indptr_out, int64_t* row_entries_out, int64_t* info_out, void* stream);
 
 /* buildNeighborList at scalar_t = double (neighborhoodDynamic.h:76-115): writes each query's pairs
- * from offsets[q] in stencil order. */
+ * from offsets[q] in stencil order (same stage as tcr_count_f64; the other arguments as in
+ * tcr_emit). */
 int tcr_emit_f64(const tcr_search_desc* d, const tcr_f64_inputs* in, const void* structure, void* scratch,
-                 int64_t scratch_bytes, const int64_t* offsets, int64_t* row_out, int64_t* col_out,
-                 int64_t out_capacity, void* stream);
+                 int64_t scratch_bytes, const int32_t* stage, const int64_t* offsets, int64_t* row_out,
+                 int64_t* col_out, int64_t out_capacity, void* stream);
 
 /* ---------------------------------------------------------------------------------------------
  * Reductions of values onto an index: the reference's scatter operators scatter_sum, scatter_mul,

@@ -35,7 +35,7 @@ def test_descriptor_layout_matches_library():
     assert ctypes.sizeof(_lib.SearchDesc) == _lib.load().tcr_desc_bytes()
     assert ctypes.sizeof(_lib.CloudDesc) == _lib.load().tcr_cloud_desc_bytes()
     assert ctypes.sizeof(_lib.BatchDesc) == _lib.load().tcr_batch_desc_bytes()
-    assert _lib.load().tcr_version() == 8
+    assert _lib.load().tcr_version() == 9
 
 
 def _batch(clouds, mode=0, self_search=1):

@@ -137,8 +137,10 @@ SIGNATURES = {
     "tcr_batch_count": (ctypes.c_int, [_batch_p, _vp, _vp, _i64, _vp, _i64, _vp, _vp, _vp, _vp, _vp]),
     "tcr_batch_emit": (ctypes.c_int, [_batch_p, _vp, _vp, _i64, _vp, _vp, _vp, _vp, _i64, _vp]),
     "tcr_search_noalloc": (ctypes.c_int, [_desc_p, _vp, _vp, _vp, _vp, _vp, _i64, ctypes.POINTER(_i64), _vp]),
-    "tcr_count_f64": (ctypes.c_int, [_desc_p, ctypes.POINTER(F64Inputs), _vp, _vp, _i64, _vp, _vp, _vp, _vp, _vp]),
-    "tcr_emit_f64": (ctypes.c_int, [_desc_p, ctypes.POINTER(F64Inputs), _vp, _vp, _i64, _vp, _vp, _vp, _i64, _vp]),
+    "tcr_count_f64": (ctypes.c_int, [_desc_p, ctypes.POINTER(F64Inputs), _vp, _vp, _i64, _vp, _i64, _vp, _vp, _vp,
+                                     _vp, _vp]),
+    "tcr_emit_f64": (ctypes.c_int, [_desc_p, ctypes.POINTER(F64Inputs), _vp, _vp, _i64, _vp, _vp, _vp, _vp, _i64,
+                                    _vp]),
     "tcr_scatter_desc_bytes": (_i64, []),
     "tcr_index_stats": (ctypes.c_int, [_vp, _i64, _vp, _vp, _vp]),
     "tcr_scatter_sizes": (ctypes.c_int, [_scatter_p, ctypes.POINTER(_i64)]),

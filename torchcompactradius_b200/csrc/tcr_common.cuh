@@ -42,6 +42,29 @@ static inline int set_error(int code, const char* fmt, ...) {
     return code;
 }
 
+// Checked build (-DTCR_CHECKED, debugging only): TCR_IN(i, n) verifies 0 <= i < n before an
+// access; a failing check records its source line, the index and the bound (the first failure
+// wins) and the access is skipped.  tcr_debug_checks() reads the record.  In a normal build the
+// check is the constant true and costs nothing.
+#ifdef TCR_CHECKED
+static __device__ unsigned long long g_check[3];
+__device__ __forceinline__ bool tcr_in_range(long long i, long long n, int line) {
+    if (i >= 0 && i < n) return true;
+    if (atomicCAS(&g_check[0], 0ull, (unsigned long long)line) == 0ull) {
+        g_check[1] = (unsigned long long)i;
+        g_check[2] = (unsigned long long)n;
+    }
+    return false;
+}
+#define TCR_IN(i, n) ::tcr::tcr_in_range((long long)(i), (long long)(n), __LINE__)
+#define TCR_GUARD(i, n) TCR_IN(i, n)
+#else
+#define TCR_IN(i, n) true
+// An index taken from device data (sort indices, cell ranges, staged records) is range-checked in
+// every build before it addresses memory; an out-of-range index skips the access.
+#define TCR_GUARD(i, n) ((unsigned long long)(long long)(i) < (unsigned long long)(long long)(n))
+#endif
+
 enum Mode : int { kGather = 0, kScatter = 1, kSymmetric = 2, kSuperSymmetric = 3 };
 
 constexpr int kMaxDim = 3;
@@ -98,6 +121,8 @@ struct QueryParams {
     SupportStats stats;      // over this search's query supports
     float qmax;              // largest query support (band of the fast test)
     int32_t exact_all;       // decide every pair with the exact reference test
+    uint32_t coord_key;      // float64 inputs: float_key of the largest |coordinate| of the double positions
+    int32_t pad;
 };
 
 // Ordered uint32 encoding of floats: a < b  <=>  key(a) < key(b); NaN maps above +inf.

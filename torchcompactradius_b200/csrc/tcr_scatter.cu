@@ -210,13 +210,6 @@ __global__ void stats_init_kernel(int64_t* stats) {
     stats[0] = LLONG_MAX;
     stats[1] = LLONG_MIN;
     stats[2] = 0;
-    stats[3] = 0;  // the index sort's fault word (low half)
-}
-
-// A look-back wait of the index sort gave up: mark the index invalid (minimum below zero) so that
-// no fold runs and the caller, which reads the statistics, raises.
-__global__ void sort_fault_kernel(const int32_t* fault, int64_t* stats) {
-    if (*fault) stats[0] = LLONG_MIN;
 }
 
 // One warp's contribution to stats (min, max, descents); every lane of the warp calls it.
@@ -262,7 +255,7 @@ __device__ __forceinline__ bool stats_allow(const int64_t* stats, int64_t N, boo
 // index for a full index), with all ones for an index outside [0, N) so that it sorts past every
 // slot; the values are the element's e (index over e) or flat src position (full index).
 template <typename K>
-__global__ void sort_init_kernel(SortStateT<K>* st) { sort_state_reset(st); }  // one block
+__global__ void sort_init_kernel(SortStateT<K>* st) { sort_state_reset(st); }
 
 template <typename K, bool FULL>
 __global__ void __launch_bounds__(kThreads) pack_keys_kernel(const int64_t* __restrict__ idx, int64_t M, int64_t E,
@@ -692,7 +685,8 @@ struct Work {
     void* state;
     void* keys[2];
     int32_t* vals[2];
-    unsigned long long* status;  // the index sort's look-back words
+    int32_t* hist;
+    int32_t* tile_sums;
 };
 
 int64_t carve_work(const Plan& p, char* base, Work& w) {
@@ -703,7 +697,7 @@ int64_t carve_work(const Plan& p, char* base, Work& w) {
     w.ngaps = c.take<unsigned long long>(1);
     w.state = w.keys[0] = w.keys[1] = nullptr;
     w.vals[0] = w.vals[1] = nullptr;
-    w.status = nullptr;
+    w.hist = w.tile_sums = nullptr;
     if (p.path != 0) {
         const int64_t kb = p.wide ? 8 : 4;
         w.state = p.wide ? (void*)c.take<SortState64>(1) : (void*)c.take<SortState32>(1);
@@ -711,7 +705,9 @@ int64_t carve_work(const Plan& p, char* base, Work& w) {
         w.keys[1] = c.take<char>(p.M * kb);
         w.vals[0] = c.take<int32_t>(p.M);
         w.vals[1] = c.take<int32_t>(p.M);
-        w.status = c.take<unsigned long long>(sort_status_words(p.M));
+        const int64_t nh = sort_hist_elems(p.M);
+        w.hist = c.take<int32_t>(nh);
+        w.tile_sums = c.take<int32_t>(scan_tiles(nh));
     }
     return c.off;
 }
@@ -751,7 +747,7 @@ cudaError_t sort_path(const tcr_scatter_desc* d, const Plan& p, const Work& w, c
     SortStateT<K>* state = static_cast<SortStateT<K>*>(w.state);
     K* k0 = static_cast<K*>(w.keys[0]);
     K* k1 = static_cast<K*>(w.keys[1]);
-    sort_init_kernel<K><<<1, kBins, 0, st>>>(state);
+    sort_init_kernel<K><<<1, 1, 0, st>>>(state);
     if (p.path == 2)
         pack_keys_kernel<K, true><<<grid_for(p.M), kThreads, 0, st>>>(d->index, p.M, d->E, d->K, d->N, k0, w.vals[0],
                                                                        state, w.stats);
@@ -764,13 +760,11 @@ cudaError_t sort_path(const tcr_scatter_desc* d, const Plan& p, const Work& w, c
     ws.keys[1] = k1;
     ws.vals[0] = w.vals[0];
     ws.vals[1] = w.vals[1];
-    ws.status = w.status;
+    ws.hist = w.hist;
+    ws.tile_sums = w.tile_sums;
     ws.state = state;
-    ws.fault = reinterpret_cast<int32_t*>(w.stats + 3);
     cudaError_t e = radix_sort_pairs<K>(ws, p.M, st);
     if (e != cudaSuccess) return e;
-    sort_fault_kernel<<<1, 1, 0, st>>>(ws.fault, w.stats);
-    note_launches(1);
     const int32_t* sel = &state->sel[key_passes<K>()];
     const unsigned mgrid = grid_resident(mark_runs_kernel<K, false>, (p.M + kMarkKeys - 1) / kMarkKeys);
     mark_runs_kernel<K, false><<<mgrid, kThreads, 0, st>>>(k0, k1, sel, p.M, p.nslots, w.off, w.gaps, w.ngaps, p.gap_cap,

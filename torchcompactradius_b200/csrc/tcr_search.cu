@@ -83,7 +83,6 @@ struct Structure {
     GridParams* grid;         // [C] per cloud
     int32_t* num_cells;       // [1]
     int32_t* bad_grids;       // [1] clouds with points on both sides and no valid grid
-    int32_t* fault;           // [1] a bounded wait of the build gave up (its result is not valid)
     float4* rsorted;          // [nr] wrapped reference points in (cloud, cell) order, .w = support
     int32_t* rsidx;           // [nr] global index of each sorted point
     int32_t* cell_start;      // [nr+1]
@@ -101,7 +100,6 @@ static Structure carve_structure(void* buf, int64_t nr, int64_t C, int64_t map_t
     s.grid = c.take<GridParams>(C);
     s.num_cells = c.take<int32_t>(1);
     s.bad_grids = c.take<int32_t>(1);
-    s.fault = c.take<int32_t>(1);
     s.rsorted = c.take<float4>(nr);
     s.rsidx = c.take<int32_t>(nr);
     s.cell_start = c.take<int32_t>(nr + 1);
@@ -114,10 +112,6 @@ static Structure carve_structure(void* buf, int64_t nr, int64_t C, int64_t map_t
     if (bytes) *bytes = c.off;
     return s;
 }
-
-// Scans of one phase (build: the incremental build's unmoved points, the cell table; count: query
-// groups, work units, offsets), each with its own look-back slot; the phase's init kernel zeroes them.
-constexpr int kScanSlots = 3;
 
 // Per-search scratch.
 struct Scratch {
@@ -140,11 +134,10 @@ struct Scratch {
     float4* pack;           // [max(nq,nr)] packed input points before sorting
     void* keys[2];          // [max(nq,nr)] 64-bit slots (32-bit keys use the first half)
     int32_t* vals[2];
-    unsigned long long* sort_status;  // [sort_status_words(max)] look-back words of the radix sorts
-    unsigned long long* scan_status;  // [kScanSlots][scan_tiles(max + 1)] look-back words of a phase's scans
-    int32_t* scan_ticket;             // [kScanSlots]
-    int32_t* fault;                   // [1] a bounded wait of the query phases gave up
-    int64_t scan_stride;              // scan_tiles(max + 1): words per scan slot
+    int32_t* hist;
+    int32_t* tile_sums;
+    int64_t* scan_tiles64;  // [scan_tiles(max)]
+    int32_t* scan_tiles32;  // [scan_tiles(max)]
     float4* qsorted;        // [nq]
     int32_t* qsidx;         // [nq] global query index of each sorted query
     int32_t* qgroup_start;  // [nq+1]
@@ -191,11 +184,10 @@ static Scratch carve_scratch(void* buf, int64_t nq, int64_t nr, int64_t C, bool 
     s.keys[1] = c.take<unsigned long long>(nmax);
     s.vals[0] = c.take<int32_t>(nmax);
     s.vals[1] = c.take<int32_t>(nmax);
-    s.sort_status = c.take<unsigned long long>(sort_status_words(nmax));
-    s.scan_stride = scan_tiles(nmax + 1);
-    s.scan_status = c.take<unsigned long long>(kScanSlots * s.scan_stride);
-    s.scan_ticket = c.take<int32_t>(kScanSlots);
-    s.fault = c.take<int32_t>(1);
+    s.hist = c.take<int32_t>(sort_hist_elems(nmax));
+    s.tile_sums = c.take<int32_t>(scan_tiles(sort_hist_elems(nmax)));
+    s.scan_tiles64 = c.take<int64_t>(scan_tiles(nmax + 1));
+    s.scan_tiles32 = c.take<int32_t>(scan_tiles(nmax + 1));
     const int64_t q = std::max<int64_t>(nq, 1);
     s.qsorted = c.take<float4>(q);
     s.qsidx = c.take<int32_t>(q);
@@ -229,14 +221,10 @@ static SortWorkspaceT<K> sort_workspace(const Scratch& W) {
     s.keys[1] = reinterpret_cast<K*>(W.keys[1]);
     s.vals[0] = W.vals[0];
     s.vals[1] = W.vals[1];
-    s.status = W.sort_status;
+    s.hist = W.hist;
+    s.tile_sums = W.tile_sums;
     s.state = reinterpret_cast<SortStateT<K>*>(W.sort_state);
-    s.fault = W.fault;
     return s;
-}
-
-static LookbackSlot lookback_slot(const Scratch& W, int k, int32_t* fault) {
-    return LookbackSlot{W.scan_status + k * W.scan_stride, W.scan_ticket + k, fault};
 }
 
 // ------------------------------------------------------------------------------------------
@@ -354,14 +342,7 @@ __global__ void support_stats_kernel(const CloudParams* __restrict__ table, cons
     }
 }
 
-// Zeroes a phase's look-back slots (statuses and tickets) and its fault word.
-__device__ __forceinline__ void zero_lookback(const Scratch& W, int32_t* fault) {
-    zero_words(W.scan_status, kScanSlots * W.scan_stride);
-    if (blockIdx.x == 0 && threadIdx.x < kScanSlots) W.scan_ticket[threadIdx.x] = 0;
-    if (blockIdx.x == 0 && threadIdx.x == 0) *fault = 0;
-}
-
-// Start of a build: per-cloud statistics and flags, counters, the sort state, the look-back slots.
+// Start of a build: per-cloud statistics and flags, counters, the sort state.
 template <typename K>
 __global__ void grid_init_kernel(GridParams* g, int C, Structure S, Scratch W) {
     for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < C; c += gridDim.x * blockDim.x) {
@@ -372,19 +353,20 @@ __global__ void grid_init_kernel(GridParams* g, int C, Structure S, Scratch W) {
         g[c].error = 0;
         g[c].out_of_grid = 0;
     }
-    zero_lookback(W, S.fault);
-    if (blockIdx.x == 0) {
-        if (threadIdx.x == 0) {
-            *S.bad_grids = 0;
-            *S.num_cells = 0;
-            S.cell_start[0] = 0;  // no reference points: no cells
-        }
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        *S.bad_grids = 0;
+        *S.num_cells = 0;
         sort_state_reset(reinterpret_cast<SortStateT<K>*>(W.sort_state));
     }
 }
 
 template <typename K>
 __global__ void sort_state_init_kernel(SortStateT<K>* st) { sort_state_reset(st); }
+
+// End of the last cell (or query group): cell_start[C] = n.
+__global__ void finish_cells_kernel(int32_t* cell_start, const int32_t* num_cells, int64_t n) {
+    cell_start[*num_cells] = (int32_t)n;
+}
 
 // Per cloud: util.py:28-79 compute_h and cellTable.py:27-29, float32 throughout.
 // same_sup: the query supports are the reference support array (statistics reduced once).
@@ -484,16 +466,15 @@ __global__ void query_params_kernel(const CloudParams* __restrict__ table, const
     }
 }
 
-// Zeroes the per-search counters, the per-cloud query statistics, the per-query counts and the
-// look-back slots of the query phases.
+// Zeroes the per-search counters, the per-cloud query statistics and the per-query counts.
 __global__ void count_init_kernel(Scratch W, int C, int unit_cap, int64_t nq) {
     for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < C; c += gridDim.x * blockDim.x) {
         W.qparams[c].stats.max_key = 0;
         W.qparams[c].stats.bad = 0;
+        W.qparams[c].coord_key = 0;
     }
     for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < nq; i += (int64_t)gridDim.x * blockDim.x)
         W.counts[i] = 0;
-    zero_lookback(W, W.fault);
     if (blockIdx.x == 0 && threadIdx.x == 0) {
         for (int k = 0; k < kWorkCounters; ++k) W.work[k] = 0;
         *W.num_stray = 0;
@@ -707,9 +688,8 @@ struct CellOut {
     int32_t* cell_cloud;
     unsigned long long* map;
     int32_t n_points;
-    __device__ void finish(int64_t cells) const { cell_start[cells] = n_points; }  // end of the last cell
     __device__ void operator()(int64_t i, int32_t ex, int32_t flag) const {
-        if (!flag) return;
+        if (!flag || !TCR_IN(ex, n_points)) return;
         const K* k = st->sel[key_passes<K>()] ? keys1 : keys0;
         const K key = k[i];
         const int cloud = key_cloud(key);
@@ -746,6 +726,7 @@ __global__ void gather_sorted_kernel(const float4* __restrict__ pack, const int3
     const int64_t stride = (int64_t)gridDim.x * blockDim.x;
     for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
         const int32_t p = v[i];
+        if (!TCR_IN(p, n)) continue;
         sorted[i] = pack[p];
         sidx[i] = p;
         if (lin_out) lin_out[i] = (int32_t)(key_low(k[i]) ^ 0x80000000u);
@@ -770,7 +751,6 @@ struct StayIn {
 };
 template <typename K>
 struct StayOut {
-    __device__ void finish(int64_t) const {}
     const K* keys;        // the pack output, input order
     K* stay_keys;
     int32_t* stay_idx;
@@ -797,15 +777,12 @@ __global__ void inc_check_kernel(const K* __restrict__ stay_keys, const int32_t*
     if (!__all_sync(0xffffffffu, ok) && (threadIdx.x & 31) == 0) atomicOr(bad, 1);
 }
 
-// Chooses the path: the moved points' sort and the merge, or the full sort (one block; its thread
-// 0 decides).
+// Chooses the path: the moved points' sort and the merge, or the full sort (one thread).
 template <typename K>
 __global__ void inc_decide_kernel(SortStateT<K>* full, SortStateT<K>* moved, const int32_t* counts, int64_t n) {
     const int64_t n_stay = counts[0];
     const bool fallback = counts[1] != 0 || 2 * n_stay < n;  // wrong hint, or most points moved
     sort_state_reset(moved);
-    __syncthreads();
-    if (threadIdx.x != 0) return;
     if (fallback) {
         moved->key_min = moved->key_max = 0;  // no moved sort
         return;
@@ -894,7 +871,6 @@ struct QueryGroupOut {
     int32_t* group_coords;
     int32_t* group_cloud;
     int32_t n_points;
-    __device__ void finish(int64_t groups) const { group_start[groups] = n_points; }  // end of the last group
     __device__ void operator()(int64_t i, int32_t ex, int32_t flag) const {
         if (!flag) return;
         const K* k = st->sel[key_passes<K>()] ? keys1 : keys0;
@@ -924,16 +900,17 @@ struct BoundedUnitCountIn {
     }
 };
 struct BoundedUnitOut {
-    __device__ void finish(int64_t) const {}
     const int32_t* group_start;
     const int32_t* num_groups;
     int32_t* unit_group;
     int32_t* unit_t0;
     int32_t cap;
+    int64_t bound = 1ll << 62;  // entries of unit_group / unit_t0 (checked build)
     __device__ void operator()(int64_t g, int32_t ex, int32_t nunits) const {
         if (g >= *num_groups) return;
         const int32_t s = group_start[g];
         for (int32_t u = 0; u < nunits; ++u) {
+            if (!TCR_IN(ex + u, bound)) break;
             unit_group[ex + u] = (int32_t)g;
             unit_t0[ex + u] = s + u * cap;
         }
@@ -951,6 +928,55 @@ struct BoundedUnitOut {
 // pass expands the records into CSR/COO slots.  A unit that finds the staging list full is only
 // counted and is walked again by the emit walk, which writes its pairs directly.
 
+// Float64 inputs (tcr_count_f64 / tcr_emit_f64): the walks find and test candidates on the float32
+// copies and decide every pair inside the widened rounding band on these double arrays with the
+// reference's double expression.  qpos == null: a float32 search.
+struct F64Walk {
+    const double* qpos;      // [nq * dim] queries, wrapped as the reference wraps them
+    const double* qsup;      // [nq] or null
+    const double4* rsorted;  // [nr] the references in the structure's cell order, .w = support
+    double ext[3];           // max - min of the domain, in double
+};
+
+// common.h:106-129 and neighborhoodDynamic.h:59-70 at scalar_t = double: per dimension
+// diff = moduloOp(x_i, x_j, max - min) = ((x_i - x_j + h/2) - floor((x_i - x_j + h/2) / h) * h) - h/2
+// on periodic dimensions, x_i - x_j otherwise; sum += diff * diff; sqrt(sum) < the mode's
+// threshold.  Explicit intrinsics keep every operation rounded on its own (no FMA).
+__device__ __noinline__ bool f64_pair_test(int dim, int mask, int mode, const double* ext, const double* xi,
+                                           double hi, const double* xj, double hj) {
+    double sum = 0.0;
+    for (int d = 0; d < dim; ++d) {
+        double diff;
+        if ((mask >> d) & 1) {
+            const double h = ext[d];
+            const double half = __ddiv_rn(h, 2.0);
+            const double t = __dadd_rn(__dsub_rn(xi[d], xj[d]), half);
+            diff = __dsub_rn(__dsub_rn(t, __dmul_rn(floor(__ddiv_rn(t, h)), h)), half);
+        } else {
+            diff = __dsub_rn(xi[d], xj[d]);
+        }
+        sum = __dadd_rn(sum, __dmul_rn(diff, diff));
+    }
+    const double dist = __dsqrt_rn(sum);
+    double thr;
+    switch (mode) {
+        case kGather: thr = hi; break;
+        case kScatter: thr = hj; break;
+        case kSymmetric: thr = __ddiv_rn(__dadd_rn(hi, hj), 2.0); break;
+        default: thr = hi < hj ? hj : hi; break;  // std::max
+    }
+    return dist < thr;
+}
+
+// Pair (cloud-local query qi, sorted reference j) of a float64 search decided on the double arrays.
+__device__ __noinline__ bool f64_pair_decide(F64Walk f, int dim, int mask, int mode, int64_t qi, int32_t j) {
+    double xi[3] = {0.0, 0.0, 0.0};
+    for (int d = 0; d < dim; ++d) xi[d] = f.qpos[qi * dim + d];
+    const double4 c = f.rsorted[j];
+    const double xj[3] = {c.x, c.y, c.z};
+    return f64_pair_test(dim, mask, mode, f.ext, xi, f.qsup ? f.qsup[qi] : 0.0, xj, c.w);
+}
+
 // The unit's cloud, as the walk kernels read it (shared memory, warp-uniform).
 struct UnitCtx {
     int32_t cloud, dim, periodic_mask, dedupe;
@@ -960,6 +986,7 @@ struct UnitCtx {
     int32_t qshift, rshift;  // subtracted from global query / reference indices (cloud-local numbering)
     float dmin[3], hcell[3], ext[3];
     float rmax, qmax;        // largest reference / query support (band of the fast test)
+    float f64_err;           // float64 inputs: bound on the error of a float32 coordinate difference
     int32_t shift_ok;        // periodic dims all hold >= 6 cells: candidates across a seam are shifted
     float shift_delta;       // bound on the error a shift adds to a difference
     int64_t map_base, map_cap;
@@ -1010,6 +1037,8 @@ struct WalkArgs {
     int64_t* row_out;             // emit: COO rows or null
     int64_t* col_out;             // emit: columns
     int64_t out_cap;              // emit: entries of row_out/col_out; writes beyond are dropped
+    F64Walk f64;                  // float64 inputs, or qpos == null
+    int64_t nq_total, nr_total;   // point counts (bounds of the checked build)
 };
 
 __device__ __forceinline__ void load_unit_ctx(UnitCtx& u, const WalkArgs& a, int cloud) {
@@ -1051,6 +1080,9 @@ __device__ __forceinline__ void load_unit_ctx(UnitCtx& u, const WalkArgs& a, int
     u.shift_delta = delta;
     u.map_base = cp.map_base;
     u.map_cap = cp.map_cap;
+    // a float32 copy of a double coordinate x is off by <= |x| 2^-24, the float difference adds one
+    // rounding: 2^-21 of the largest |coordinate| bounds a difference's error with room to spare
+    u.f64_err = a.f64.qpos ? key_float(q.coord_key) * 4.76837158203125e-7f : 0.0f;
 }
 
 __device__ __forceinline__ ExactCtx unit_exact_ctx(const UnitCtx& u, int mode) {
@@ -1090,7 +1122,7 @@ __device__ __forceinline__ void stencil_lookup(const WalkArgs& a, const UnitCtx&
     if (dup) return;
     const int32_t lin = linear_index(u.dim, c, u.count);
     const int32_t cell = map_find(a.map + u.map_base, u.map_cap, lin);
-    if (cell < 0) return;
+    if (cell < 0 || !TCR_GUARD(cell, a.nr_total)) return;
     // queryHashMap matches the linear index inside bucket hash(c) only.
     if ((uint32_t)__ldg(&a.cell_bucket[cell]) != ref_hash(u.dim, c, u.hash_len)) return;
     beg = __ldg(&a.cell_start[cell]);
@@ -1205,6 +1237,7 @@ __host__ __device__ __forceinline__ int64_t record_words(int32_t runs, int32_t n
 struct WalkSmem {
     float4 q[kWalkWarps][32];        // the unit's queries: x, y, z and the query's share of the test
     float qh[kWalkWarps][32];        // the queries' supports (for the exact re-test)
+    int32_t qid[kWalkWarps][32];     // the queries' cloud-local indices (float64 re-test)
     int32_t run_beg[kWalkWarps][32];
     int32_t run_pre[kWalkWarps][33];
     float shift[kWalkWarps][3][32];  // per run: +-ext on the dimensions its cells lie across a seam
@@ -1288,10 +1321,11 @@ __device__ __forceinline__ uint32_t chunk_hits(const WrapCtx& wc, const float4* 
 }
 
 // The same with every pair inside the band decided by the reference's exact test, on the original
-// (unshifted) candidate; rare units only, so out of line.
+// (unshifted) candidate of sorted index j -- in double on the double arrays for float64 inputs;
+// rare units only, so out of line.
 template <int DIM, int MODE>
-__device__ __noinline__ uint32_t chunk_hits_exact(ExactCtx xc, const float4* qsm, const float* qh, int K4, float4 cv,
-                                                  float band) {
+__device__ __noinline__ uint32_t chunk_hits_exact(ExactCtx xc, const float4* qsm, const float* qh, const int32_t* qid,
+                                                  int K4, float4 cv, int32_t j, float band, F64Walk f64) {
     const WrapCtx wc = wrap_ctx(xc.periodic_mask, xc.ext);
     const float cw = cand_share<MODE>(cv.w);
     uint32_t hit = 0;
@@ -1300,7 +1334,9 @@ __device__ __noinline__ uint32_t chunk_hits_exact(ExactCtx xc, const float4* qsm
         bool wu = false;
         const float r = pair_residual<DIM, true, MODE>(wc, q, cv, cw, wu);
         bool in = r < 0.0f;
-        if ((fabsf(r) <= band) || wu) in = exact_pair_test(xc, q, qh[k], cv, cv.w);
+        if ((fabsf(r) <= band) || wu)
+            in = f64.qpos ? f64_pair_decide(f64, DIM, xc.periodic_mask, MODE, qid[k], j)
+                          : exact_pair_test(xc, q, qh[k], cv, cv.w);
         hit = (hit << 1) | (in ? 1u : 0u);
     }
     return hit;
@@ -1363,23 +1399,24 @@ __device__ __forceinline__ void count_unit(const WalkArgs& a, WalkSmem& sm, int3
     bool active = false;
     int32_t qorig = 0;
     float4 qv = nan4;
-    if (lane < nb) {
+    if (lane < nb && TCR_IN(t0 + lane, a.nq_total)) {
         const int32_t t = t0 + lane;
         qv = a.qsorted[t];
         qorig = a.qsidx[t];
-        active = true;
-        if (!a.no_stray_check || u.out_of_grid) {
+        active = TCR_IN(qorig, a.nq_total);
+        if (active && (!a.no_stray_check || u.out_of_grid)) {
             int32_t qc[3];
             cell_of(DIM, u.dedupe, u.dmin, u.hcell, u.count, qv, qc);
             active = same_cell<DIM>(qc, gc);
         }
         if (!active) {  // own cell differs from the group's (aliasing or wrap rounding): serial path
             const int32_t k = atomicAdd(a.num_stray, 1);
-            a.stray[k] = t;
+            if (TCR_IN(k, a.nq_total)) a.stray[k] = t;
             qv = nan4;
         }
     }
     sm.qh[w][lane] = qv.w;
+    sm.qid[w][lane] = qorig - u.qshift;
     sm.q[w][lane] = make_float4(qv.x, qv.y, qv.z, query_share<MODE>(qv.w));  // rows >= nb: NaN, never hit
     // the unit's record, reserved up front
     const int32_t nchunks = (M + 31) >> 5;
@@ -1415,11 +1452,13 @@ __device__ __forceinline__ void count_unit(const WalkArgs& a, WalkSmem& sm, int3
     const float4* __restrict__ rs = a.rsorted;
     int32_t cr = 0;
     bool shifting = shift_mode;  // the fast pass tests shifted candidates, the exact pass the originals
-    auto fetch = [&](int32_t k) {
+    auto fetch = [&](int32_t k, int32_t& j) {
         float4 v = nan4;
+        j = 0;
         if (k < M) {
             while (rpre[cr + 1] <= k) ++cr;
-            v = __ldg(&rs[rbeg[cr] + (k - rpre[cr])]);
+            j = rbeg[cr] + (k - rpre[cr]);
+            if (TCR_GUARD(j, a.nr_total)) v = __ldg(&rs[j]);
             if (PERIODIC && shifting) {
                 v.x += sm.shift[w][0][cr];
                 if (DIM > 1) v.y += sm.shift[w][1][cr];
@@ -1432,17 +1471,21 @@ __device__ __forceinline__ void count_unit(const WalkArgs& a, WalkSmem& sm, int3
     const float qmax = u.qmax;
     const bool exact_all = u.exact_all != 0;
     const float dl = u.shift_delta;
+    const float fe = u.f64_err;
     const int K4 = (nb + 3) & ~3;
     const float4* qsm = sm.q[w];
     uint32_t count = 0;
     bool unc = false;
-    float4 nxt = fetch(lane);
+    int32_t jn;
+    float4 nxt = fetch(lane, jn);
     for (int32_t c = 0; c < nchunks; ++c) {
         const float4 cv = nxt;
-        nxt = fetch(((c + 1) << 5) + lane);  // the next chunk's candidate, ahead of its use
+        nxt = fetch(((c + 1) << 5) + lane, jn);  // the next chunk's candidate, ahead of its use
         const float cw = cand_share<MODE>(cv.w);
         const float t = cand_tmax<MODE>(cw, qmax);
         float band = exact_all ? inf : kBandEps * t * t;
+        // float64 inputs: the band also covers the rounding of the coordinates to float32
+        if (fe > 0.0f) band += fmaf(2.0f * 1.7320508f * t, fe, 3.0f * fe * fe);
         // shifted candidates: the band also covers the shift's rounding (|d2 error| <= 2 T delta + delta^2)
         if (seam) band += fmaf(2.0f * t, dl, dl * dl);
         uint32_t hit;
@@ -1451,7 +1494,8 @@ __device__ __forceinline__ void count_unit(const WalkArgs& a, WalkSmem& sm, int3
         const uint32_t m = warp_transpose32(hit, lane);
         if (lane < nb) {
             count += __popc(m);
-            if (stage) msk[c * nb + lane] = m;
+            if (stage && TCR_IN((int64_t)(msk - reinterpret_cast<uint32_t*>(a.stage)) + c * nb + lane, a.stage_cap))
+                msk[c * nb + lane] = m;
         }
     }
     if (__any_sync(0xffffffffu, unc)) {  // some pair lies in the band: walk again with exact decisions
@@ -1460,13 +1504,17 @@ __device__ __forceinline__ void count_unit(const WalkArgs& a, WalkSmem& sm, int3
         shifting = false;
         cr = 0;
         count = 0;
-        nxt = fetch(lane);
+        int32_t jc;
+        nxt = fetch(lane, jn);
         for (int32_t c = 0; c < nchunks; ++c) {
             const float4 cv = nxt;
-            nxt = fetch(((c + 1) << 5) + lane);
+            jc = jn;
+            nxt = fetch(((c + 1) << 5) + lane, jn);
             const float t = cand_tmax<MODE>(cand_share<MODE>(cv.w), qmax);
-            const float band = exact_all ? inf : kBandEps * t * t;
-            const uint32_t m = warp_transpose32(chunk_hits_exact<DIM, MODE>(xc, qsm, sm.qh[w], K4, cv, band), lane);
+            float band = exact_all ? inf : kBandEps * t * t;
+            if (fe > 0.0f) band += fmaf(2.0f * 1.7320508f * t, fe, 3.0f * fe * fe);
+            const uint32_t m = warp_transpose32(
+                chunk_hits_exact<DIM, MODE>(xc, qsm, sm.qh[w], sm.qid[w], K4, cv, jc, band, a.f64), lane);
             if (lane < nb) {
                 count += __popc(m);
                 if (stage) msk[c * nb + lane] = m;
@@ -1474,11 +1522,11 @@ __device__ __forceinline__ void count_unit(const WalkArgs& a, WalkSmem& sm, int3
         }
     }
     if (active) a.counts[qorig] = (int32_t)count;
-    if (lane == 0 && !stage) {
+    if (lane == 0 && !stage && TCR_IN(unit, a.nq_total)) {
         a.rec[unit] = -1;
         if (nchunks > 0) {  // not staged: the emit walk tests the unit again
             const int32_t f = atomicAdd(a.num_flagged, 1);
-            a.flagged[f] = unit;
+            if (TCR_IN(f, a.nq_total)) a.flagged[f] = unit;
         }
     }
     __syncwarp();
@@ -1587,22 +1635,29 @@ __device__ __forceinline__ void emit_unit(const WalkArgs& a, EmitSmem& sm, int32
         int32_t j = 0;
         if (k < M) {
             j = cand_index(sm.pre[w], sm.beg[w], S, k);
-            cv = __ldg(&a.rsorted[j]);
+            if (TCR_GUARD(j, a.nr_total)) cv = __ldg(&a.rsorted[j]);
+            else j = 0;
         }
         int32_t jl = __ldg(&a.rsidx[j]);
         jl = a.ref_ids ? __ldg(&a.ref_ids[jl]) : jl - u.rshift;
         const int64_t jorig = (int64_t)jl;
         const float cw = cand_share<MODE>(cv.w);
-        const float band = exact_all ? __int_as_float(0x7f800000) : cand_band<MODE>(cw, qmax);
+        float band = exact_all ? __int_as_float(0x7f800000) : cand_band<MODE>(cw, qmax);
+        if (u.f64_err > 0.0f) {  // float64 inputs: the coordinates' rounding to float32 widens the band
+            const float t = cand_tmax<MODE>(cw, qmax), fe = u.f64_err;
+            band += fmaf(2.0f * 1.7320508f * t, fe, 3.0f * fe * fe);
+        }
         for (int qi = 0; qi < nb; ++qi) {
             const float4 q = sm.q[w][qi];
             bool in, unc;
             lean_test<DIM, PERIODIC, MODE>(wc, q, cv, cw, band, in, unc);
             const uint32_t ub = __ballot_sync(0xffffffffu, unc);
-            if (ub) in = unc ? exact_pair_test(unit_exact_ctx(u, MODE), q, q.w, cv, cv.w) : in;
+            int32_t qrow = __shfl_sync(0xffffffffu, qorig, qi);
+            if (ub && unc)
+                in = a.f64.qpos ? f64_pair_decide(a.f64, DIM, u.periodic_mask, MODE, qrow - u.qshift, j)
+                                : exact_pair_test(unit_exact_ctx(u, MODE), q, q.w, cv, cv.w);
             const uint32_t b = __ballot_sync(0xffffffffu, in);
             const int64_t qb = __shfl_sync(0xffffffffu, obase, qi);
-            int32_t qrow = __shfl_sync(0xffffffffu, qorig, qi);
             qrow = a.query_ids ? __ldg(&a.query_ids[qrow]) : qrow - u.qshift;
             if (in) {
                 const int64_t pos = qb + __popc(b & lt);
@@ -1683,6 +1738,7 @@ struct ExpandArgs {
     int64_t* __restrict__ row_out;
     int64_t* __restrict__ col_out;
     int64_t out_cap;
+    int64_t stage_cap, nq, nr;  // bounds of the checked build
 };
 
 __global__ void __launch_bounds__(kExpandWarps * 32, 3) expand_records_kernel(ExpandArgs a) {
@@ -1702,8 +1758,11 @@ __global__ void __launch_bounds__(kExpandWarps * 32, 3) expand_records_kernel(Ex
         const int32_t r0 = r0n;
         if (u + warps < nu) r0n = a.rec[u + warps];  // the next unit's record, ahead of its use
         if (r0 < 0) continue;  // no candidates, or re-tested by the emit walk
+        if (!TCR_GUARD(r0 + 3, a.stage_cap)) continue;
         const int32_t* rec = a.stage + r0;
         const int32_t nchunks = rec[0], R = rec[1], nb = rec[2];
+        if (!TCR_GUARD(R, 28) || !TCR_GUARD(nb - 1, 32) || !TCR_GUARD(r0 + record_words(R, nchunks, nb) - 1, a.stage_cap))
+            continue;
         const uint32_t* masks = reinterpret_cast<const uint32_t*>(rec + kRecHeader + 2 * R + 1);
         const int32_t t0 = a.unit_t0[u];
         int32_t rshift = 0, qshift = 0;
@@ -1714,10 +1773,12 @@ __global__ void __launch_bounds__(kExpandWarps * 32, 3) expand_records_kernel(Ex
         }
         if (lane < R) rbeg[lane] = rec[kRecHeader + lane];
         if (lane <= R) rpre[lane] = rec[kRecHeader + R + lane];
-        if (lane < nb) {
+        if (lane < nb && TCR_GUARD(t0 + lane, a.nq)) {
             const int32_t row = a.qsidx[t0 + lane];
-            sm.qrow[w][lane] = a.query_ids ? a.query_ids[row] : row - qshift;
-            sm.qoff[w][lane] = a.offsets[row];
+            if (TCR_GUARD(row, a.nq)) {
+                sm.qrow[w][lane] = a.query_ids ? a.query_ids[row] : row - qshift;
+                sm.qoff[w][lane] = a.offsets[row];
+            }
         }
         __syncwarp();
         const int32_t M = rpre[R];
@@ -1729,7 +1790,8 @@ __global__ void __launch_bounds__(kExpandWarps * 32, 3) expand_records_kernel(Ex
                 int32_t col = 0;
                 if (k < M) {
                     while (rpre[cr + 1] <= k) ++cr;
-                    const int32_t jl = __ldg(&a.rsidx[rbeg[cr] + (k - rpre[cr])]);
+                    const int32_t j = rbeg[cr] + (k - rpre[cr]);
+                    const int32_t jl = TCR_GUARD(j, a.nr) ? __ldg(&a.rsidx[j]) : 0;
                     col = a.ref_ids ? __ldg(&a.ref_ids[jl]) : jl - rshift;
                 }
                 cols[(cc << 5) + lane] = col;
@@ -1771,7 +1833,7 @@ __global__ void __launch_bounds__(kExpandWarps * 32, 3) expand_records_kernel(Ex
                     const int32_t v = tab[o];
                     const int q = v >> 9;
                     const int64_t pos = sm.qoff[w][q] + (o - sm.qpre[w][q]);
-                    if (pos < a.out_cap) {
+                    if (TCR_GUARD(pos, a.out_cap)) {
                         __stcs(reinterpret_cast<long long*>(&a.col_out[pos]), (long long)cols[v & 0x1ff]);
                         if (a.row_out) __stcs(reinterpret_cast<long long*>(&a.row_out[pos]), (long long)sm.qrow[w][q]);
                     }
@@ -1787,7 +1849,7 @@ __global__ void __launch_bounds__(kExpandWarps * 32, 3) expand_records_kernel(Ex
                     while (m) {
                         const int bit = __ffs(m) - 1;
                         m &= m - 1;
-                        if (pos < a.out_cap) {
+                        if (TCR_GUARD(pos, a.out_cap)) {
                             a.col_out[pos] = (int64_t)cols[(lane << 5) + bit];
                             if (a.row_out) a.row_out[pos] = row;
                         }
@@ -1824,7 +1886,9 @@ __global__ void stray_kernel(WalkArgs a) {
             stencil_lookup(a, u, qc, o, beg, cnt);
             for (int32_t j = beg; j < beg + cnt; ++j) {
                 const float4 cv = a.rsorted[j];
-                if (exact_pair_test(xc, q, q.w, cv, cv.w)) {
+                const bool in = a.f64.qpos ? f64_pair_decide(a.f64, u.dim, u.periodic_mask, a.mode, qorig - u.qshift, j)
+                                           : exact_pair_test(xc, q, q.w, cv, cv.w);
+                if (in) {
                     if (EMIT) {
                         if (pos < a.out_cap) {
                             const int32_t jl = a.rsidx[j];
@@ -1846,8 +1910,9 @@ __global__ void stray_kernel(WalkArgs a) {
 // float64 inputs (the reference dispatches its operators on float and double,
 // neighborhoodDynamic_cpu.cpp:504,531).  The structure is built from float32 copies with a cell
 // size no smaller than the reference's double one, so every pair within the double support lies
-// in the query's 3^d stencil; each candidate is then decided on the caller's double positions and
-// supports by the reference's double expression.
+// in the query's 3^d stencil; the walks then test candidates on the float32 copies with a band
+// widened by the copies' rounding, and every pair inside the band is decided on the caller's double
+// positions and supports by the reference's double expression.
 struct F64Args {
     const double* qpos;  // [nq * dim], wrapped as the reference wraps queries
     const double* qsup;  // [nq] or null
@@ -1856,99 +1921,37 @@ struct F64Args {
     double4* rsorted;    // [nr] the references in the structure's cell order, .w = support
     double ext[3];       // max - min of the domain, in double
     int64_t nq, nr;
-    int32_t self_order;  // queries are the references: walk them in cell order (rsidx)
 };
 
-// The double references in cell order, so that a stencil cell's candidates are one contiguous run.
-__global__ void f64_sort_refs_kernel(const int32_t* __restrict__ rsidx, F64Args f, int dim) {
-    for (int64_t j = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; j < f.nr; j += (int64_t)gridDim.x * blockDim.x) {
+static F64Walk f64_walk(const F64Args& f) {
+    F64Walk w;
+    w.qpos = f.qpos;
+    w.qsup = f.qsup;
+    w.rsorted = f.rsorted;
+    for (int d = 0; d < 3; ++d) w.ext[d] = f.ext[d];
+    return w;
+}
+
+// The double references in cell order (a stencil cell's candidates are one contiguous run), and the
+// largest |coordinate| of the double positions (NaN ignored, rounded up) for the band of the float
+// test.
+__global__ void f64_prep_kernel(const int32_t* __restrict__ rsidx, F64Args f, int dim, QueryParams* qp) {
+    float m = 0.0f;
+    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    for (int64_t j = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; j < f.nr; j += stride) {
         const int64_t jl = rsidx[j];
         double4 v = make_double4(0.0, 0.0, 0.0, f.rsup ? f.rsup[jl] : 0.0);
         v.x = f.rpos[jl * dim];
         if (dim > 1) v.y = f.rpos[jl * dim + 1];
         if (dim > 2) v.z = f.rpos[jl * dim + 2];
         f.rsorted[j] = v;
+        m = fmaxf(m, __double2float_ru(fmax(fabs(v.x), fmax(fabs(v.y), fabs(v.z)))));
     }
-}
-
-// common.h:106-129 and neighborhoodDynamic.h:59-70 at scalar_t = double: per dimension
-// diff = moduloOp(x_i, x_j, max - min) = ((x_i - x_j + h/2) - floor((x_i - x_j + h/2) / h) * h) - h/2
-// on periodic dimensions, x_i - x_j otherwise; sum += diff * diff; sqrt(sum) < the mode's
-// threshold.  Explicit intrinsics keep every operation rounded on its own (no FMA).
-__device__ __noinline__ bool f64_pair_test(int dim, int mask, int mode, const double* ext, const double* xi,
-                                           double hi, const double* xj, double hj) {
-    double sum = 0.0;
-    for (int d = 0; d < dim; ++d) {
-        double diff;
-        if ((mask >> d) & 1) {
-            const double h = ext[d];
-            const double half = __ddiv_rn(h, 2.0);
-            const double t = __dadd_rn(__dsub_rn(xi[d], xj[d]), half);
-            diff = __dsub_rn(__dsub_rn(t, __dmul_rn(floor(__ddiv_rn(t, h)), h)), half);
-        } else {
-            diff = __dsub_rn(xi[d], xj[d]);
-        }
-        sum = __dadd_rn(sum, __dmul_rn(diff, diff));
-    }
-    const double dist = __dsqrt_rn(sum);
-    double thr;
-    switch (mode) {
-        case kGather: thr = hi; break;
-        case kScatter: thr = hj; break;
-        case kSymmetric: thr = __ddiv_rn(__dadd_rn(hi, hj), 2.0); break;
-        default: thr = hi < hj ? hj : hi; break;  // std::max
-    }
-    return dist < thr;
-}
-
-// One thread per query: the query's cell from its float32 copy, the 3^d stencil of the structure,
-// every candidate tested in double.  A self search walks the queries in cell order, so the threads
-// of a warp share stencils and read the same candidate runs.  Count pass (EMIT = false) writes
-// counts[q]; emit pass writes the row's pairs from offsets[q] in stencil order.
-template <bool EMIT>
-__global__ void __launch_bounds__(128) f64_walk_kernel(WalkArgs a, F64Args f) {
-    UnitCtx u;
-    load_unit_ctx(u, a, 0);
-    const CloudParams& cp = a.table[0];
-    const int S = u.dim == 1 ? 3 : (u.dim == 2 ? 9 : 27);
-    const int dim = u.dim;
-    for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < f.nq; t += (int64_t)gridDim.x * blockDim.x) {
-        const int64_t q = f.self_order ? (int64_t)a.rsidx[t] : t;
-        if (u.error) {
-            if (!EMIT) a.counts[q] = 0;
-            continue;
-        }
-        const float4 qf = wrap_point(cp.dim, cp.periodic_mask, cp.dmin, cp.ext,
-                                     load_point(cp.query_pos, cp.query_sup, q, cp.dim), 1);
-        int32_t qc[3];
-        cell_of(u.dim, u.dedupe, u.dmin, u.hcell, u.count, qf, qc);
-        double xi[3] = {0.0, 0.0, 0.0};
-        for (int d = 0; d < dim; ++d) xi[d] = f.qpos[q * dim + d];
-        const double hi = f.qsup ? f.qsup[q] : 0.0;
-        int64_t pos = EMIT ? a.offsets[q] : 0;
-        int32_t n = 0;
-        for (int o = 0; o < S; ++o) {
-            int32_t beg, cnt;
-            stencil_lookup(a, u, qc, o, beg, cnt);
-            for (int32_t j = beg; j < beg + cnt; ++j) {
-                const double4 c = f.rsorted[j];
-                const double xj[3] = {c.x, c.y, c.z};
-                if (f64_pair_test(dim, u.periodic_mask, a.mode, f.ext, xi, hi, xj, c.w)) {
-                    const int32_t jl = a.rsidx[j];
-                    if (EMIT) {
-                        if (pos < a.out_cap) {
-                            a.col_out[pos] = (int64_t)(a.ref_ids ? a.ref_ids[jl] : jl - u.rshift);
-                            if (a.row_out) a.row_out[pos] = a.query_ids ? a.query_ids[q] : q - u.qshift;
-                        }
-                        ++pos;
-                    } else {
-                        ++n;
-                    }
-                }
-            }
-        }
-        if (!EMIT) a.counts[q] = n;
-    }
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < f.nq * dim; i += stride)
+        m = fmaxf(m, __double2float_ru(fabs(f.qpos[i])));
+#pragma unroll
+    for (int o = 16; o; o >>= 1) m = fmaxf(m, __shfl_xor_sync(0xffffffffu, m, o));
+    if ((threadIdx.x & 31) == 0 && m > 0.0f) atomicMax(&qp->coord_key, float_key(m));
 }
 
 // counts -> offsets (int64, nq+1), optional CSR indptr (int32) and rowEntries (int64).
@@ -1958,7 +1961,6 @@ struct CountIn {
     __device__ int64_t operator()(int64_t i) const { return i < n ? (int64_t)counts[i] : 0; }
 };
 struct OffsetOut {
-    __device__ void finish(int64_t) const {}
     int64_t n;
     int64_t* offsets;
     int32_t* indptr;
@@ -1970,12 +1972,11 @@ struct OffsetOut {
     }
 };
 
-__global__ void info_kernel(const int32_t* bad_grids, const int32_t* build_fault, const int32_t* fault,
-                            const int64_t* total, const int32_t* num_stray,
+__global__ void info_kernel(const int32_t* bad_grids, const int64_t* total, const int32_t* num_stray,
                             const int32_t* exact_clouds, const unsigned long long* cursor, const int32_t* num_flagged,
                             const int32_t* num_exact, const int32_t* inc_count, int64_t n_ref, int64_t* info) {
     info[0] = *total;
-    info[1] = (*build_fault || *fault) ? -1 : *bad_grids;  // -1: a bounded wait gave up
+    info[1] = *bad_grids;
     info[2] = *num_stray;
     info[3] = *exact_clouds;
     info[4] = (int64_t)*cursor;
@@ -2242,6 +2243,8 @@ static WalkArgs make_walk(const HostBatch& b, const Structure& S, const Scratch&
     a.cursor = W.cursor;
     a.query_ids = b.query_ids;
     a.ref_ids = b.ref_ids;
+    a.nq_total = b.nq;
+    a.nr_total = b.nr;
     return a;
 }
 
@@ -2326,14 +2329,12 @@ static unsigned walk_blocks(int64_t nq) {
 
 template <typename K>
 static int build_impl(const HostBatch& b, const Structure& S, const Scratch& W, cudaStream_t st) {
-    SortWorkspaceT<K> sw = sort_workspace<K>(W);
-    sw.fault = S.fault;  // the build's waits report into the structure
+    const SortWorkspaceT<K> sw = sort_workspace<K>(W);
     const int C = b.C;
     const int64_t nr = b.nr, nq = b.nq;
     int rc = upload_table(b, W, st);
     if (rc) return rc;
-    grid_init_kernel<K><<<grid_for(std::max<int64_t>(C, kScanSlots * W.scan_stride), 256), 256, 0, st>>>(S.grid, C, S,
-                                                                                                       W);
+    grid_init_kernel<K><<<grid_for(C, 128), 128, 0, st>>>(S.grid, C, S, W);
     note_launches(1);
     // computeGridSupport: which supports set hMax depends on the mode
     if (b.any_ref_sup && nr > 0) {
@@ -2366,10 +2367,10 @@ static int build_impl(const HostBatch& b, const Structure& S, const Scratch& W, 
             mw.state = reinterpret_cast<SortStateT<K>*>(W.moved_state);
             TCR_CUDA(cudaMemsetAsync(W.inc_count, 0, 2 * sizeof(int32_t), st));
             StayOut<K> so{sw.keys[0], reinterpret_cast<K*>(W.stay_keys), W.stay_idx, mw.keys[0], mw.vals[0]};
-            TCR_CUDA(device_exclusive_scan<int32_t>(StayIn{W.stay}, so, nr, lookback_slot(W, 0, S.fault), W.inc_count, st));
+            TCR_CUDA(device_exclusive_scan<int32_t>(StayIn{W.stay}, so, nr, W.scan_tiles32, W.inc_count, st));
             inc_check_kernel<K><<<grid_for(nr, 256), 256, 0, st>>>(reinterpret_cast<const K*>(W.stay_keys),
                                                                    W.inc_count, W.inc_count + 1);
-            inc_decide_kernel<K><<<1, 256, 0, st>>>(sw.state, mw.state, W.inc_count, nr);
+            inc_decide_kernel<K><<<1, 1, 0, st>>>(sw.state, mw.state, W.inc_count, nr);
             note_launches(2);
             TCR_CUDA(radix_sort_pairs<K>(mw, nr, st));
             inc_merge_kernel<K><<<grid_for(nr, 256), 256, 0, st>>>(
@@ -2385,8 +2386,10 @@ static int build_impl(const HostBatch& b, const Structure& S, const Scratch& W, 
         CellOut<K> co{W.table, S.grid, sw.keys[0], sw.keys[1], sw.state, S.rsorted, S.cell_start, S.cell_lin,
                       S.cell_coords, S.cell_bucket, S.cell_cloud, S.map, (int32_t)nr};
         RunFlagIn<K> fi{sw.keys[0], sw.keys[1], sw.state};
-        TCR_CUDA(device_exclusive_scan<int32_t>(fi, co, nr, lookback_slot(W, 1, S.fault), S.num_cells, st));
+        TCR_CUDA(device_exclusive_scan<int32_t>(fi, co, nr, W.scan_tiles32, S.num_cells, st));
     }
+    finish_cells_kernel<<<1, 1, 0, st>>>(S.cell_start, S.num_cells, nr);
+    note_launches(1);
     TCR_CUDA(cudaGetLastError());
     return TCR_OK;
 }
@@ -2394,14 +2397,13 @@ static int build_impl(const HostBatch& b, const Structure& S, const Scratch& W, 
 template <typename K>
 static int count_impl(const HostBatch& b, const Structure& S, const Scratch& W, int32_t* stage, int64_t stage_cap,
                       int64_t* offsets, int32_t* indptr_out, int64_t* row_entries_out, int64_t* info_out,
-                      cudaStream_t st) {
+                      cudaStream_t st, const F64Args* f64) {
     const int C = b.C;
     const int64_t nq = b.nq;
     int rc = upload_table(b, W, st);
     if (rc) return rc;
     const int unit_cap = g_unit_cap;
-    count_init_kernel<<<grid_for(std::max<int64_t>({(int64_t)C, nq, kScanSlots * W.scan_stride}), 256), 256, 0, st>>>(
-        W, C, unit_cap, nq);
+    count_init_kernel<<<grid_for(std::max<int64_t>(C, nq), 256), 256, 0, st>>>(W, C, unit_cap, nq);
     note_launches(1);
     if (b.any_query_sup && nq > 0 && !b.same_sorted) {
         support_stats_kernel<<<grid_for(nq, 256, num_sms() * 8), 256, 0, st>>>(
@@ -2412,6 +2414,11 @@ static int count_impl(const HostBatch& b, const Structure& S, const Scratch& W, 
     query_params_kernel<<<grid_for(C, 128), 128, 0, st>>>(W.table, S.grid, C, W.qparams, W.exact_clouds,
                                                           b.same_sorted ? 1 : 0);
     note_launches(1);
+    if (f64 && (b.nr > 0 || nq > 0)) {
+        f64_prep_kernel<<<grid_for(std::max<int64_t>(b.nr, nq * b.clouds[0].dim), 256), 256, 0, st>>>(
+            S.rsidx, *f64, b.clouds[0].dim, W.qparams);
+        note_launches(1);
+    }
     if (nq > 0) {
         const int32_t* gstart;
         const int32_t* ngroups;
@@ -2426,7 +2433,7 @@ static int count_impl(const HostBatch& b, const Structure& S, const Scratch& W, 
         } else {
             // sort the queries by their own (cloud, cell)
             const SortWorkspaceT<K> sw = sort_workspace<K>(W);
-            sort_state_init_kernel<K><<<1, 256, 0, st>>>(sw.state);
+            sort_state_init_kernel<K><<<1, 1, 0, st>>>(sw.state);
             note_launches(1);
             pack_points_kernel<K><<<grid_for(nq, 256), 256, 0, st>>>(W.table, S.grid, W.query_prefix, C, nq, 1, 1, 0,
                                                                      W.pack, sw.keys[0], sw.vals[0], sw.state);
@@ -2438,14 +2445,17 @@ static int count_impl(const HostBatch& b, const Structure& S, const Scratch& W, 
             QueryGroupOut<K> qo{W.table, S.grid, sw.keys[0], sw.keys[1], sw.state, W.qsorted,
                                 W.qgroup_start, W.qgroup_coords, W.qgroup_cloud, (int32_t)nq};
             RunFlagIn<K> fi{sw.keys[0], sw.keys[1], sw.state};
-            TCR_CUDA(device_exclusive_scan<int32_t>(fi, qo, nq, lookback_slot(W, 0, W.fault), W.num_qgroups, st));
+            TCR_CUDA(device_exclusive_scan<int32_t>(fi, qo, nq, W.scan_tiles32, W.num_qgroups, st));
+            finish_cells_kernel<<<1, 1, 0, st>>>(W.qgroup_start, W.num_qgroups, nq);
+            note_launches(1);
             gstart = W.qgroup_start;
             ngroups = W.num_qgroups;
         }
         BoundedUnitCountIn ui{gstart, ngroups, unit_cap};
-        BoundedUnitOut uo{gstart, ngroups, W.unit_group, W.unit_t0, unit_cap};
-        TCR_CUDA(device_exclusive_scan<int32_t>(ui, uo, nq, lookback_slot(W, 1, W.fault), W.num_units, st));
+        BoundedUnitOut uo{gstart, ngroups, W.unit_group, W.unit_t0, unit_cap, nq};
+        TCR_CUDA(device_exclusive_scan<int32_t>(ui, uo, nq, W.scan_tiles32, W.num_units, st));
         WalkArgs a = make_walk(b, S, W);
+        if (f64) a.f64 = f64_walk(*f64);
         a.stage = stage;
         a.stage_cap = stage_cap;
         prof_mark(TCR_PROFILE_COUNT_WALK, 0, st);
@@ -2456,8 +2466,8 @@ static int count_impl(const HostBatch& b, const Structure& S, const Scratch& W, 
     }
     CountIn ci{W.counts, nq};
     OffsetOut oo{nq, offsets, indptr_out, row_entries_out};
-    TCR_CUDA(device_exclusive_scan<int64_t>(ci, oo, nq + 1, lookback_slot(W, 2, W.fault), W.total, st));
-    info_kernel<<<1, 1, 0, st>>>(S.bad_grids, S.fault, W.fault, W.total, W.num_stray, W.exact_clouds, W.cursor, W.num_flagged,
+    TCR_CUDA(device_exclusive_scan<int64_t>(ci, oo, nq + 1, W.scan_tiles64, W.total, st));
+    info_kernel<<<1, 1, 0, st>>>(S.bad_grids, W.total, W.num_stray, W.exact_clouds, W.cursor, W.num_flagged,
                                  W.num_exact, b.lin_hint && b.nr > 0 ? W.inc_count : nullptr, b.nr, W.info);
     note_launches(1);
     if (info_out) TCR_CUDA(cudaMemcpyAsync(info_out, W.info, 8 * sizeof(int64_t), cudaMemcpyDeviceToHost, st));
@@ -2466,11 +2476,12 @@ static int count_impl(const HostBatch& b, const Structure& S, const Scratch& W, 
 
 static int emit_impl(const HostBatch& b, const Structure& S, const Scratch& W, const int32_t* stage,
                      const int64_t* offsets, int64_t* row_out, int64_t* col_out, int64_t out_capacity,
-                     cudaStream_t st) {
+                     cudaStream_t st, const F64Args* f64) {
     const int64_t nq = b.nq;
     if (out_capacity < 0 || (out_capacity > 0 && !col_out)) return set_error(TCR_ERR_INVALID, "bad output buffer");
     if (nq <= 0) return TCR_OK;
     WalkArgs a = make_walk(b, S, W);
+    if (f64) a.f64 = f64_walk(*f64);
     a.offsets = offsets;
     a.row_out = row_out;
     a.col_out = col_out;
@@ -2497,6 +2508,9 @@ static int emit_impl(const HostBatch& b, const Structure& S, const Scratch& W, c
         e.row_out = row_out;
         e.col_out = col_out;
         e.out_cap = out_capacity;
+        e.stage_cap = 0x7fffffffLL;  // the records lie below the staging capacity of tcr_count (< 2^31 words)
+        e.nq = nq;
+        e.nr = b.nr;
         static uint64_t expand_attr_done = 0;
         TCR_CUDA(ensure_smem(expand_records_kernel, (int)sizeof(ExpandSmem), &expand_attr_done));
         prof_mark(TCR_PROFILE_EXPAND, 0, st);
@@ -2526,7 +2540,7 @@ static int run_build(const HostBatch& b, void* structure, int64_t structure_byte
 
 static int run_count(const HostBatch& b, const void* structure, void* scratch, int64_t scratch_bytes, int32_t* stage,
                      int64_t stage_capacity, int64_t* offsets, int32_t* indptr_out, int64_t* row_entries_out,
-                     int64_t* info_out, void* stream) {
+                     int64_t* info_out, void* stream, const F64Args* f64 = nullptr) {
     int64_t need_w = 0;
     batch_sizes(b, nullptr, &need_w);
     if (!structure || !scratch || scratch_bytes < need_w || !offsets)
@@ -2537,21 +2551,21 @@ static int run_count(const HostBatch& b, const void* structure, void* scratch, i
     const Scratch W = carve_scratch(scratch, b.nq, b.nr, b.C, b.lin_hint != nullptr, nullptr);
     cudaStream_t st = (cudaStream_t)stream;
     return b.wide ? count_impl<unsigned long long>(b, S, W, stage, stage_capacity, offsets, indptr_out,
-                                                   row_entries_out, info_out, st)
+                                                   row_entries_out, info_out, st, f64)
                   : count_impl<uint32_t>(b, S, W, stage, stage_capacity, offsets, indptr_out, row_entries_out,
-                                         info_out, st);
+                                         info_out, st, f64);
 }
 
 static int run_emit(const HostBatch& b, const void* structure, void* scratch, int64_t scratch_bytes,
                     const int32_t* stage, const int64_t* offsets, int64_t* row_out, int64_t* col_out,
-                    int64_t out_capacity, void* stream) {
+                    int64_t out_capacity, void* stream, const F64Args* f64 = nullptr) {
     int64_t need_w = 0;
     batch_sizes(b, nullptr, &need_w);
     if (!structure || !scratch || scratch_bytes < need_w || !offsets)
         return set_error(TCR_ERR_INVALID, "workspace too small or offsets missing");
     const Structure S = carve_structure(const_cast<void*>(structure), b.nr, b.C, b.map_total, nullptr);
     const Scratch W = carve_scratch(scratch, b.nq, b.nr, b.C, b.lin_hint != nullptr, nullptr);
-    return emit_impl(b, S, W, stage, offsets, row_out, col_out, out_capacity, (cudaStream_t)stream);
+    return emit_impl(b, S, W, stage, offsets, row_out, col_out, out_capacity, (cudaStream_t)stream, f64);
 }
 
 }  // namespace tcr
@@ -2603,6 +2617,18 @@ int tcr_profile_kernel_ms(int32_t kernel, float* ms) {
     TCR_CUDA(cudaEventElapsedTime(ms, g_prof_ev[kernel][0], g_prof_ev[kernel][1]));
     return TCR_OK;
 }
+
+#ifdef TCR_CHECKED
+// Checked build only: the first failed bounds check (source line, index, bound), then cleared.
+int tcr_debug_checks(int64_t* out3) {
+    unsigned long long h[3] = {0, 0, 0};
+    TCR_CUDA(cudaMemcpyFromSymbol(h, g_check, sizeof(h)));
+    const unsigned long long z[3] = {0, 0, 0};
+    TCR_CUDA(cudaMemcpyToSymbol(g_check, z, sizeof(z)));
+    for (int k = 0; k < 3; ++k) out3[k] = (int64_t)h[k];
+    return TCR_OK;
+}
+#endif
 
 int tcr_set_tuning(int32_t unit_queries, int32_t walk_blocks_per_sm) {
     if (unit_queries != 0 && unit_queries != 8 && unit_queries != 16 && unit_queries != 32)
@@ -2687,13 +2713,12 @@ static int f64_args(const tcr_search_desc* d, const tcr_f64_inputs* in, F64Args&
     for (int k = 0; k < 3; ++k) f.ext[k] = in->domain_max[k] - in->domain_min[k];
     f.nq = d->n_query;
     f.nr = d->n_ref;
-    f.self_order = d->self_search ? 1 : 0;
     return TCR_OK;
 }
 
 int tcr_count_f64(const tcr_search_desc* d, const tcr_f64_inputs* in, const void* structure, void* scratch,
-                  int64_t scratch_bytes, int64_t* offsets, int32_t* indptr_out, int64_t* row_entries_out,
-                  int64_t* info_out, void* stream) {
+                  int64_t scratch_bytes, int32_t* stage, int64_t stage_capacity, int64_t* offsets,
+                  int32_t* indptr_out, int64_t* row_entries_out, int64_t* info_out, void* stream) {
     NvtxRange nvtx_("tcr_count_f64");
     HostBatch b;
     int rc = batch_of_desc(d, 1, b);
@@ -2701,43 +2726,13 @@ int tcr_count_f64(const tcr_search_desc* d, const tcr_f64_inputs* in, const void
     F64Args f;
     rc = f64_args(d, in, f);
     if (rc) return rc;
-    int64_t need_w = 0;
-    batch_sizes(b, nullptr, &need_w);
-    if (!structure || !scratch || scratch_bytes < need_w || !offsets)
-        return set_error(TCR_ERR_INVALID, "workspace too small or offsets missing");
-    const Structure S = carve_structure(const_cast<void*>(structure), b.nr, b.C, b.map_total, nullptr);
-    const Scratch W = carve_scratch(scratch, b.nq, b.nr, b.C, false, nullptr);
-    cudaStream_t st = (cudaStream_t)stream;
-    rc = upload_table(b, W, st);
-    if (rc) return rc;
-    count_init_kernel<<<grid_for(std::max<int64_t>({(int64_t)b.C, b.nq, kScanSlots * W.scan_stride}), 256), 256, 0,
-                        st>>>(W, b.C, g_unit_cap, b.nq);
-    query_params_kernel<<<1, 128, 0, st>>>(W.table, S.grid, b.C, W.qparams, W.exact_clouds, 0);
-    note_launches(2);
-    const int64_t nq = b.nq;
-    if (b.nr > 0) {
-        f64_sort_refs_kernel<<<grid_for(b.nr, 256), 256, 0, st>>>(S.rsidx, f, d->dim);
-        note_launches(1);
-    }
-    if (nq > 0) {
-        WalkArgs a = make_walk(b, S, W);
-        f64_walk_kernel<false><<<grid_for(nq, 128, num_sms() * 8), 128, 0, st>>>(a, f);
-        note_launches(1);
-    }
-    CountIn ci{W.counts, nq};
-    OffsetOut oo{nq, offsets, indptr_out, row_entries_out};
-    TCR_CUDA(device_exclusive_scan<int64_t>(ci, oo, nq + 1, lookback_slot(W, 2, W.fault), W.total, st));
-    info_kernel<<<1, 1, 0, st>>>(S.bad_grids, S.fault, W.fault, W.total, W.num_stray, W.exact_clouds, W.cursor, W.num_flagged,
-                                 W.num_exact, nullptr, b.nr, W.info);
-    note_launches(1);
-    if (info_out) TCR_CUDA(cudaMemcpyAsync(info_out, W.info, 8 * sizeof(int64_t), cudaMemcpyDeviceToHost, st));
-    TCR_CUDA(cudaGetLastError());
-    return TCR_OK;
+    return run_count(b, structure, scratch, scratch_bytes, stage, stage_capacity, offsets, indptr_out, row_entries_out,
+                     info_out, stream, &f);
 }
 
 int tcr_emit_f64(const tcr_search_desc* d, const tcr_f64_inputs* in, const void* structure, void* scratch,
-                 int64_t scratch_bytes, const int64_t* offsets, int64_t* row_out, int64_t* col_out,
-                 int64_t out_capacity, void* stream) {
+                 int64_t scratch_bytes, const int32_t* stage, const int64_t* offsets, int64_t* row_out,
+                 int64_t* col_out, int64_t out_capacity, void* stream) {
     NvtxRange nvtx_("tcr_emit_f64");
     HostBatch b;
     int rc = batch_of_desc(d, 1, b);
@@ -2745,27 +2740,7 @@ int tcr_emit_f64(const tcr_search_desc* d, const tcr_f64_inputs* in, const void*
     F64Args f;
     rc = f64_args(d, in, f);
     if (rc) return rc;
-    int64_t need_w = 0;
-    batch_sizes(b, nullptr, &need_w);
-    if (!structure || !scratch || scratch_bytes < need_w || !offsets)
-        return set_error(TCR_ERR_INVALID, "workspace too small or offsets missing");
-    if (out_capacity < 0 || (out_capacity > 0 && !col_out)) return set_error(TCR_ERR_INVALID, "bad output buffer");
-    const Structure S = carve_structure(const_cast<void*>(structure), b.nr, b.C, b.map_total, nullptr);
-    const Scratch W = carve_scratch(scratch, b.nq, b.nr, b.C, false, nullptr);
-    cudaStream_t st = (cudaStream_t)stream;
-    rc = upload_table(b, W, st);
-    if (rc) return rc;
-    const int64_t nq = b.nq;
-    if (nq <= 0) return TCR_OK;
-    WalkArgs a = make_walk(b, S, W);
-    a.offsets = offsets;
-    a.row_out = row_out;
-    a.col_out = col_out;
-    a.out_cap = out_capacity;
-    f64_walk_kernel<true><<<grid_for(nq, 128, num_sms() * 8), 128, 0, st>>>(a, f);
-    note_launches(1);
-    TCR_CUDA(cudaGetLastError());
-    return TCR_OK;
+    return run_emit(b, structure, scratch, scratch_bytes, stage, offsets, row_out, col_out, out_capacity, stream, &f);
 }
 
 int tcr_batch_sizes(const tcr_batch_desc* bd, int64_t* structure_bytes, int64_t* scratch_bytes) {
