@@ -1379,9 +1379,12 @@ __device__ __forceinline__ void count_unit(const WalkArgs& a, WalkSmem& sm, int3
     const int32_t pbeg = __shfl_up_sync(0xffffffffu, beg, 1);
     const int32_t pcnt = __shfl_up_sync(0xffffffffu, cnt, 1);
     bool cont = lane > 0 && pcnt > 0 && pbeg + pcnt == beg;
-    if (shift_mode) {
+    if (shift_mode) {  // every lane takes part in the shuffles (no short-circuit around them)
 #pragma unroll
-        for (int d = 0; d < DIM; ++d) cont = cont && __shfl_up_sync(0xffffffffu, sh[d], 1) == sh[d];
+        for (int d = 0; d < DIM; ++d) {
+            const float psh = __shfl_up_sync(0xffffffffu, sh[d], 1);
+            cont = cont && psh == sh[d];
+        }
     }
     const bool starts = cnt > 0 && !cont;
     const uint32_t smask = __ballot_sync(0xffffffffu, starts);
