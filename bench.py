@@ -427,7 +427,7 @@ def bench_served(dev, seconds=1.0, slots=2):
                 r.wait(120)
 
         tuner = Autotuner(reps=2)
-        tuned = tuner.tune(all_scenes, key="served")
+        tuned = tuner.tune(all_scenes, key="served", apply=srv.set_tuning)
         srv.batches = srv.batched_requests = 0
         torch.cuda.synchronize()
         reqs = []
@@ -465,22 +465,24 @@ def bench_served(dev, seconds=1.0, slots=2):
         served_capacity = {"value": sum(counted) / (t_end - t0), "unit": "pairs/s", "seconds": t_end - t0,
                            "batches": srv.batches, "mean_batch": srv.batched_requests / max(srv.batches, 1)}
 
-    # ---- per call -----------------------------------------------------------------------
-    pos = [x.to(dev) for x, h in scenes]  # (the same engine tuning as the server)
+    # ---- per call (the same engine tuning as the server) ---------------------------------
+    from torchcompactradius_b200 import context
+    pos = [x.to(dev) for x, h in scenes]
     sup = [torch.full((x.shape[0],), h, device=dev) for x, h in scenes]
-    for k in range(len(scenes)):
-        tcr.radiusSearch(tcr.PointCloud(pos[k], sup[k]), mode="gather", domain=dom, algorithm="compact")
-    torch.cuda.synchronize()
-    lat, pairs = [], 0
-    t0 = time.perf_counter()
-    for ta, k in arrivals:
-        while time.perf_counter() - t0 < ta:
-            time.sleep(0.0001)
-        pos[k] = pos[k] + torch.randn(pos[k].shape, device=dev) * (0.05 * scenes[k][1])
-        adj = tcr.radiusSearch(tcr.PointCloud(pos[k], sup[k]), mode="gather", domain=dom, algorithm="compact")
-        pairs += adj.row.numel()  # radiusSearch returns after the host has read the pair count
-        lat.append(1e3 * (time.perf_counter() - (t0 + ta)))
-    t_end = time.perf_counter()
+    with context.use(context.SearchContext(unit_queries=tuned[0], walk_blocks_per_sm=tuned[1])):
+        for k in range(len(scenes)):
+            tcr.radiusSearch(tcr.PointCloud(pos[k], sup[k]), mode="gather", domain=dom, algorithm="compact")
+        torch.cuda.synchronize()
+        lat, pairs = [], 0
+        t0 = time.perf_counter()
+        for ta, k in arrivals:
+            while time.perf_counter() - t0 < ta:
+                time.sleep(0.0001)
+            pos[k] = pos[k] + torch.randn(pos[k].shape, device=dev) * (0.05 * scenes[k][1])
+            adj = tcr.radiusSearch(tcr.PointCloud(pos[k], sup[k]), mode="gather", domain=dom, algorithm="compact")
+            pairs += adj.row.numel()  # radiusSearch returns after the host has read the pair count
+            lat.append(1e3 * (time.perf_counter() - (t0 + ta)))
+        t_end = time.perf_counter()
     per_call = {"value": pairs / (t_end - t0), "unit": "pairs/s", "requests": len(arrivals),
                 "p50_ms": pct(lat, 0.5), "p99_ms": pct(lat, 0.99), "seconds": t_end - t0,
                 "note": "falls behind the arrivals, so value is its capacity"}

@@ -20,7 +20,7 @@
 extern "C" {
 #endif
 
-#define TCR_ABI_VERSION 9
+#define TCR_ABI_VERSION 10
 
 #define TCR_OK 0
 #define TCR_ERR_INVALID (-1) /* bad argument or workspace too small */
@@ -59,6 +59,11 @@ typedef struct tcr_search_desc {
                                  cell coordinates clamped into [0, count), stencil cells outside the grid
                                  skipped, wrapped stencil cells on periodic dims with < 3 cells visited
                                  once (the reference visits them twice and reports those pairs twice) */
+    /* Tuning of this search (no reference counterpart; 0 keeps the default; no setting changes a
+     * result): queries per work unit of the walks -- 32, 16 or 8 -- and resident walk blocks per
+     * SM (1..64).  tcr_count and tcr_emit of one search must be given the same unit_queries. */
+    int32_t unit_queries;
+    int32_t walk_blocks_per_sm;
     int32_t reserved;
 } tcr_search_desc;
 
@@ -110,6 +115,9 @@ typedef struct tcr_batch_desc {
     /* Optional (device int32 [total references]): the global input index of every reference point
      * in the new cell order -- the permutation that puts a cloud's points in that order. */
     int32_t* ref_order_out;
+    /* Tuning of this batch, as in tcr_search_desc (0: the defaults). */
+    int32_t unit_queries;
+    int32_t walk_blocks_per_sm;
 } tcr_batch_desc;
 
 /* Message of the last failing call on this thread. */
@@ -137,12 +145,6 @@ int64_t tcr_kernel_launches(void);
 #define TCR_PROFILE_EXPAND 1
 int tcr_profile_kernels(int32_t enable);
 int tcr_profile_kernel_ms(int32_t kernel, float* ms);
-
-/* Run-time tuning for later searches of this process (no reference counterpart; the autotuner of
- * torchcompactradius_b200.tuning picks them): queries per work unit of the walks -- 32, 16 or 8,
- * i.e. 1, 2 or 4 lanes per query -- and resident walk blocks per SM (1..64).  0 keeps the default
- * (32, 12).  No setting changes a result; a search uses the unit size in force at its tcr_count. */
-int tcr_set_tuning(int32_t unit_queries, int32_t walk_blocks_per_sm);
 
 /* Byte sizes of the persistent structure (reference-side cell table and hash map, kept for
  * reuse like the reference's CompactHashMap, compactHashing/datastructure.py:8-31) and of the

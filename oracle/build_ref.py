@@ -1,7 +1,7 @@
 """Build recipe for the reference's own C++ CPU operators (test infrastructure only).
 
 Compiles the torchCompactRadius CPU sources where they lie (``src/torchCompactRadius/cppSrc``
-of the reference checkout, default ``/root/reference``) with ``torch.utils.cpp_extension.load``
+of the reference checkout named by ``--reference`` or ``TCR_REFERENCE``) with ``torch.utils.cpp_extension.load``
 into ``oracle/_ref/``.  The reference's own build system (``setup.py``/``dsl.py``) is not used:
 the sources compile as they are, with the flags its ``setup.py:127-139`` gives the host compiler
 (``-O2 -fopenmp``).  Nothing is copied out of the reference tree; only the compiled ``.so``
@@ -12,7 +12,7 @@ buildNeighborList, computeHashIndices, ...}`` (reference ``cppSrc/cppWrapper.cpp
 It is loaded only by the tests, by ``__graft_entry__.smoke`` and by ``bench.py``'s reference /
 CPU-baseline arms, as the checker; the product path never touches it.
 
-Usage: ``python oracle/build_ref.py [--reference /root/reference]``
+Usage: ``python oracle/build_ref.py --reference <checkout>`` (or ``TCR_REFERENCE=<checkout>``)
 """
 import argparse
 import glob
@@ -31,7 +31,7 @@ def ref_library_path():
     return cands[0] if cands else None
 
 
-def build(reference_root="/root/reference", verbose=False):
+def build(reference_root, verbose=False):
     src = os.path.join(reference_root, "src", "torchCompactRadius", "cppSrc")
     if not os.path.isdir(src):
         raise FileNotFoundError(f"reference sources not found at {src}")
@@ -64,7 +64,10 @@ def build(reference_root="/root/reference", verbose=False):
 
 if __name__ == "__main__":
     ap = argparse.ArgumentParser()
-    ap.add_argument("--reference", default="/root/reference")
+    ap.add_argument("--reference", default=os.environ.get("TCR_REFERENCE"),
+                    help="reference checkout (default: the TCR_REFERENCE environment variable)")
     ap.add_argument("-v", action="store_true")
     a = ap.parse_args()
+    if not a.reference:
+        ap.error("give --reference or set TCR_REFERENCE")
     print(build(a.reference, a.v))

@@ -2,7 +2,7 @@
 
 Run where the reference checkout exists and its CPU operators are built by ``oracle/build_ref.py``:
 
-    PYTHONDONTWRITEBYTECODE=1 python tests/golden/make_f64_golden.py [--reference /root/reference]
+    PYTHONDONTWRITEBYTECODE=1 python tests/golden/make_f64_golden.py --reference <checkout>
 
 For every case of ``f64_cases.f64_cases()`` it calls the reference's public
 ``torchCompactRadius.radiusSearch(..., algorithm='compact', format='csr')`` with float64 positions,
@@ -25,8 +25,11 @@ import f64_cases  # noqa: E402
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("--reference", default="/root/reference")
+    ap.add_argument("--reference", default=os.environ.get("TCR_REFERENCE"),
+                    help="reference checkout (default: the TCR_REFERENCE environment variable)")
     a = ap.parse_args()
+    if not a.reference:
+        ap.error("give --reference or set TCR_REFERENCE")
     sys.path[:0] = [os.path.join(REPO, "oracle", "_ref"), os.path.join(a.reference, "src")]
     import torch
     import torchCompactRadius as tcr

@@ -1,9 +1,9 @@
 """Generates the golden fixtures from the reference package itself.
 
-Run in a container where the reference checkout exists (default /root/reference) and its CPU
+Run where the reference checkout exists (named by --reference or TCR_REFERENCE) and its CPU
 operators have been built by ``oracle/build_ref.py``:
 
-    PYTHONDONTWRITEBYTECODE=1 python tests/golden/make_golden.py [--reference /root/reference]
+    PYTHONDONTWRITEBYTECODE=1 python tests/golden/make_golden.py --reference <checkout>
 
 For every case it calls the reference's public ``torchCompactRadius.radiusSearch(...,
 algorithm='compact')`` with an explicit ``DomainDescription`` and records, per case, the SHA-256
@@ -27,8 +27,11 @@ import cases  # noqa: E402
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("--reference", default="/root/reference")
+    ap.add_argument("--reference", default=os.environ.get("TCR_REFERENCE"),
+                    help="reference checkout (default: the TCR_REFERENCE environment variable)")
     a = ap.parse_args()
+    if not a.reference:
+        ap.error("give --reference or set TCR_REFERENCE")
     sys.path[:0] = [os.path.join(REPO, "oracle", "_ref"), os.path.join(a.reference, "src")]
     import torch
     import torchCompactRadius as tcr

@@ -35,7 +35,7 @@ def test_descriptor_layout_matches_library():
     assert ctypes.sizeof(_lib.SearchDesc) == _lib.load().tcr_desc_bytes()
     assert ctypes.sizeof(_lib.CloudDesc) == _lib.load().tcr_cloud_desc_bytes()
     assert ctypes.sizeof(_lib.BatchDesc) == _lib.load().tcr_batch_desc_bytes()
-    assert _lib.load().tcr_version() == 9
+    assert _lib.load().tcr_version() == 10
 
 
 def _batch(clouds, mode=0, self_search=1):
@@ -144,13 +144,36 @@ def test_coo_csr_helpers():
     assert back.row.tolist() == row.tolist() and back.col.tolist() == col.tolist()
 
 
-def test_tuning_is_validated():
-    from torchcompactradius_b200 import _lib
+def test_tuning_travels_in_the_descriptor_and_is_validated():
+    """The engine keeps no tuning state: each batch descriptor carries its own, checked on use."""
+    import threading
+
+    from torchcompactradius_b200 import _lib, context, tuning
     lib = _lib.load()
-    assert lib.tcr_set_tuning(12, 0) == -1 and b"unit_queries" in lib.tcr_last_error()
-    assert lib.tcr_set_tuning(0, 65) == -1
-    assert lib.tcr_set_tuning(16, 8) == 0
-    assert lib.tcr_set_tuning(0, 0) == 0  # back to the defaults
+    b, keep = _batch([(3, 1000, 1000)])
+    s, w = ctypes.c_int64(), ctypes.c_int64()
+    b.unit_queries = 12
+    assert lib.tcr_batch_sizes(ctypes.byref(b), ctypes.byref(s), ctypes.byref(w)) == -1
+    assert b"unit_queries" in lib.tcr_last_error()
+    b.unit_queries, b.walk_blocks_per_sm = 0, 65
+    assert lib.tcr_batch_sizes(ctypes.byref(b), ctypes.byref(s), ctypes.byref(w)) == -1
+    b.unit_queries, b.walk_blocks_per_sm = 16, 8
+    assert lib.tcr_batch_sizes(ctypes.byref(b), ctypes.byref(s), ctypes.byref(w)) == 0
+    with pytest.raises(ValueError):
+        tuning.set_tuning(12, 0)
+    # a setting made on one thread does not reach another thread's searches
+    tuning.set_tuning(16, 8)
+    seen = []
+    t = threading.Thread(target=lambda: seen.append(context.current().tuning()))
+    t.start()
+    t.join()
+    assert context.current().tuning() == (16, 8) and seen == [(0, 0)]
+    ctx = context.SearchContext(unit_queries=8)
+    with context.use(ctx):
+        d = context.apply_tuning(_lib.SearchDesc())
+        assert (d.unit_queries, d.walk_blocks_per_sm) == (8, 0)
+    tuning.set_tuning(0, 0)
+    assert context.current().tuning() == (0, 0)
 
 
 def test_scatter_descriptor_and_validation_without_device_work():

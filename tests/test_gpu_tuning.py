@@ -23,15 +23,14 @@ def test_every_setting_gives_the_same_result(dim, periodic, mode):
     h0 = (32 * dx * dx / np.pi) ** 0.5 if dim == 2 else (3 * 50 * dx ** 3 / (4 * np.pi)) ** (1 / 3)
     h = (h0 * (0.9 + 0.2 * torch.rand(n, generator=g))).cuda()
     dom = tcr.DomainDescription(torch.full((dim,), -1.0), torch.full((dim,), 1.0), torch.tensor([periodic] * dim), dim)
-    try:
+    from torchcompactradius_b200 import context
+    with context.use(context.SearchContext()):
         set_tuning(32, 12)
         ref = _search(x, h, dom, mode)
         for cfg in CANDIDATES + [(8, 1), (16, 64)]:
             set_tuning(*cfg)
             got = _search(x, h, dom, mode)
             assert torch.equal(got.indices, ref.indices) and torch.equal(got.indptr, ref.indptr), cfg
-    finally:
-        set_tuning(0, 0)
 
 
 def test_autotuner_picks_a_candidate_and_remembers_it():
@@ -42,9 +41,9 @@ def test_autotuner_picks_a_candidate_and_remembers_it():
     dom = tcr.DomainDescription(torch.full((3,), -1.0), torch.full((3,), 1.0), torch.tensor([False] * 3), 3)
     tuner = Autotuner(reps=2)
     key = signature([3], [False], 50000, "gather", 50)
-    try:
+    from torchcompactradius_b200 import context
+    with context.use(context.SearchContext()) as ctx:
         best = tuner.tune(lambda: _search(x, h, dom, "gather"), key)
         assert best in tuner.candidates and len(tuner.timings[key]) == len(tuner.candidates)
+        assert ctx.tuning() == best
         assert tuner.tune(lambda: None, key) == best  # remembered: no timing the second time
-    finally:
-        set_tuning(0, 0)

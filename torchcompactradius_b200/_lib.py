@@ -37,6 +37,8 @@ class SearchDesc(ctypes.Structure):
         ("ref_ids", ctypes.c_void_p),
         ("hcell", ctypes.c_float * 3),
         ("clamped_grid", ctypes.c_int32),
+        ("unit_queries", ctypes.c_int32),
+        ("walk_blocks_per_sm", ctypes.c_int32),
         ("reserved", ctypes.c_int32),
     ]
 
@@ -74,6 +76,8 @@ class BatchDesc(ctypes.Structure):
         ("ref_lin_hint", ctypes.c_void_p),
         ("ref_lin_out", ctypes.c_void_p),
         ("ref_order_out", ctypes.c_void_p),
+        ("unit_queries", ctypes.c_int32),
+        ("walk_blocks_per_sm", ctypes.c_int32),
     ]
 
 
@@ -125,7 +129,6 @@ SIGNATURES = {
     "tcr_batch_desc_bytes": (_i64, []),
     "tcr_kernel_launches": (_i64, []),
     "tcr_profile_kernels": (ctypes.c_int, [_i32]),
-    "tcr_set_tuning": (ctypes.c_int, [_i32, _i32]),
     "tcr_profile_kernel_ms": (ctypes.c_int, [_i32, ctypes.POINTER(ctypes.c_float)]),
     "tcr_search_sizes": (ctypes.c_int, [_i64, _i64, _i32, ctypes.POINTER(_i64), ctypes.POINTER(_i64)]),
     "tcr_structure_offsets": (ctypes.c_int, [_i64, ctypes.POINTER(_i64), _i32]),

@@ -19,6 +19,7 @@ import numpy as np
 import torch
 
 from . import _lib
+from . import context as _context
 from .search import _as_f32, _check_device_fault, _domain_host, _ptr, _require_cuda
 from .util import DomainDescription, PointCloud, SparseCOO, SparseCSR
 
@@ -27,10 +28,6 @@ CLOUD_DTYPE = np.dtype([("dim", "<i4"), ("periodic_mask", "<i4"), ("domain_min",
                         ("n_ref", "<i8"), ("query_pos", "<u8"), ("query_sup", "<u8"), ("ref_pos", "<u8"),
                         ("ref_sup", "<u8"), ("hcell", "<f4", (3,)), ("clamped_grid", "<i4"), ("reserved", "<i4")],
                        align=True)
-
-# Pairs and staging words per query of the previous batch: they size the next one's buffers.
-_pairs_per_query = [64.0]
-_stage_per_query = [64.0]
 
 
 def cloud_table(n):
@@ -60,7 +57,7 @@ def batch_desc(table, mode, self_search, local_index=True, query_ids=None, ref_i
     b.ref_lin_hint = None if lin_hint is None else lin_hint.data_ptr()
     b.ref_lin_out = None if lin_out is None else lin_out.data_ptr()
     b.ref_order_out = None if order_out is None else order_out.data_ptr()
-    return b
+    return _context.apply_tuning(b)
 
 
 class BatchBuffers:
@@ -97,8 +94,9 @@ def run_batch(table, mode, self_search, fmt, device, local_index=True, query_ids
     offsets = bufs.get("offsets", nq + 1, torch.int64)
     counts = bufs.get("counts", nq, torch.int64)
     indptr = bufs.get("indptr", nq + 1, torch.int32) if fmt == "csr" else None
-    cap = int(min(0x7fffffff, _pairs_per_query[0] * 1.25 * nq + 4096))
-    stage_cap = int(min(0x7fffffff, _stage_per_query[0] * 1.1 * nq + 65536))
+    ctx = _context.current()
+    cap = int(min(0x7fffffff, ctx.batch_pairs_per_query * 1.25 * nq + 4096))
+    stage_cap = int(min(0x7fffffff, ctx.batch_stage_per_query * 1.1 * nq + 65536))
     stage = bufs.get("stage", stage_cap, torch.int32)
     if fresh_outputs:  # outputs owned by the caller, not reused by the next search on these buffers
         offsets = torch.empty(nq + 1, dtype=torch.int64, device=device)
@@ -140,8 +138,8 @@ def run_batch(table, mode, self_search, fmt, device, local_index=True, query_ids
                          "support is not smaller than the domain extent, or a support/domain value is not finite)")
     total = int(info[0])
     if nq:
-        _pairs_per_query[0] = max(total / nq, 1.0)
-        _stage_per_query[0] = max(int(info[4]) / nq, 1.0)
+        ctx.batch_pairs_per_query = max(total / nq, 1.0)
+        ctx.batch_stage_per_query = max(int(info[4]) / nq, 1.0)
     if fmt == "csr" and total > 0x7fffffff:
         raise ValueError(f"{total} pairs do not fit the int32 indptr of SparseCSR")
     if total > cap:  # the estimate was short: emit again into exact buffers (the count is kept)

@@ -61,11 +61,11 @@ constexpr int64_t kBatchMapMin = 64;     // per cloud of a batch
 // for the count walk of the units recorded window by window.
 constexpr int kWorkCounters = 32;
 
-// Run-time tuning (tcr_set_tuning): queries per work unit -- 32, 16 or 8, i.e. 1, 2 or 4 lanes of
-// the walk per query -- and resident walk blocks per SM.  Neither changes a result: a query's
+// Default tuning of a search (tcr_search_desc / tcr_batch_desc unit_queries and walk_blocks_per_sm):
+// queries per work unit and resident walk blocks per SM.  Neither changes a result: a query's
 // candidates and their order do not depend on how queries are grouped into units.
-static int g_unit_cap = 32;
-static int g_walk_blocks_per_sm = 12;
+constexpr int kDefaultUnitQueries = 32;
+constexpr int kDefaultWalkBlocksPerSM = 12;
 
 struct Carve {
     char* base;
@@ -1236,6 +1236,7 @@ __host__ __device__ __forceinline__ int64_t record_words(int32_t runs, int32_t n
 
 struct WalkSmem {
     float4 q[kWalkWarps][32];        // the unit's queries: x, y, z and the query's share of the test
+    float4 qp[kWalkWarps][32];       // the same as 16 query pairs for the packed test (store_query_pair)
     float qh[kWalkWarps][32];        // the queries' supports (for the exact re-test)
     int32_t qid[kWalkWarps][32];     // the queries' cloud-local indices (float64 re-test)
     int32_t run_beg[kWalkWarps][32];
@@ -1315,6 +1316,69 @@ __device__ __forceinline__ uint32_t chunk_hits(const WrapCtx& wc, const float4* 
             const float r = pair_residual<DIM, P, MODE>(wc, q, cv, cw, wu);
             hit = __funnelshift_l(__float_as_uint(r), hit, 1);
             unc |= (fabsf(r) <= band) || wu;
+        }
+    }
+    return hit;
+}
+
+// Query pairs for the packed test: pair p holds queries 2p and 2p + 1 as two float4,
+// {x0, x1, y0, y1} and {z0, z1, s0, s1}, where s is the pair-share of packed_share.
+template <int MODE>
+__device__ __forceinline__ float packed_share(float hq) {
+    return MODE == kGather ? -(hq * hq) : (MODE == kSymmetric ? 0.5f * hq : hq);
+}
+__device__ __forceinline__ void store_query_pair(float4* qp, int lane, float x, float y, float z, float s) {
+    float* f = reinterpret_cast<float*>(qp + 2 * (lane >> 1));
+    const int hi = lane & 1;
+    f[hi] = x;
+    f[2 + hi] = y;
+    f[4 + hi] = z;
+    f[6 + hi] = s;
+}
+
+// chunk_hits for non-wrapping differences (non-periodic clouds and pre-shifted seam candidates) in
+// gather, scatter and symmetric mode, two queries per instruction: the differences and the squared
+// distance run as packed float32x2 operations (each element rounded exactly as the scalar operation),
+// so the residuals and hit bits equal chunk_hits's bit for bit.  umin collects the smallest |r|
+// (NaN rows are ignored by fminf); the caller compares it with the candidate's band once per chunk.
+template <int DIM, int MODE>
+__device__ __forceinline__ uint32_t chunk_hits_x2(const float4* __restrict__ qp, int K4, const float4& cv, float cw,
+                                                  float& umin) {
+    const float2 ncx = make_float2(-cv.x, -cv.x), ncy = make_float2(-cv.y, -cv.y), ncz = make_float2(-cv.z, -cv.z);
+    const float2 ncw = make_float2(-cv.w, -cv.w), pcw = make_float2(cv.w, cv.w);
+    uint32_t hit = 0;
+    for (int p = (K4 >> 1) - 2; p >= 0; p -= 2) {
+#pragma unroll
+        for (int i = 1; i >= 0; --i) {
+            const float4 a = qp[2 * (p + i)];
+            const float4 b = qp[2 * (p + i) + 1];
+            const float2 dx = __fadd2_rn(make_float2(a.x, a.y), ncx);
+            float2 d2 = __fmul2_rn(dx, dx);
+            if (DIM > 1) {
+                const float2 dy = __fadd2_rn(make_float2(a.z, a.w), ncy);
+                d2 = __ffma2_rn(dy, dy, d2);
+            }
+            if (DIM > 2) {
+                const float2 dz = __fadd2_rn(make_float2(b.x, b.y), ncz);
+                d2 = __ffma2_rn(dz, dz, d2);
+            }
+            float r0, r1;
+            if (MODE == kGather) {  // d2 - hq^2, the share holding -hq^2
+                const float2 r = __fadd2_rn(d2, make_float2(b.z, b.w));
+                r0 = r.x;
+                r1 = r.y;
+            } else if (MODE == kScatter) {  // d2 - hc^2
+                const float2 r = __ffma2_rn(ncw, pcw, d2);
+                r0 = r.x;
+                r1 = r.y;
+            } else {  // symmetric: thr = hq / 2 + hc / 2, d2 - thr^2
+                const float t0 = b.z + cw, t1 = b.w + cw;
+                r0 = fmaf(-t0, t0, d2.x);
+                r1 = fmaf(-t1, t1, d2.y);
+            }
+            hit = __funnelshift_l(__float_as_uint(r1), hit, 1);
+            hit = __funnelshift_l(__float_as_uint(r0), hit, 1);
+            umin = fminf(umin, fminf(fabsf(r0), fabsf(r1)));
         }
     }
     return hit;
@@ -1421,6 +1485,7 @@ __device__ __forceinline__ void count_unit(const WalkArgs& a, WalkSmem& sm, int3
     sm.qh[w][lane] = qv.w;
     sm.qid[w][lane] = qorig - u.qshift;
     sm.q[w][lane] = make_float4(qv.x, qv.y, qv.z, query_share<MODE>(qv.w));  // rows >= nb: NaN, never hit
+    store_query_pair(sm.qp[w], lane, qv.x, qv.y, qv.z, packed_share<MODE>(qv.w));
     // the unit's record, reserved up front
     const int32_t nchunks = (M + 31) >> 5;
     bool stage = false;
@@ -1492,8 +1557,15 @@ __device__ __forceinline__ void count_unit(const WalkArgs& a, WalkSmem& sm, int3
         // shifted candidates: the band also covers the shift's rounding (|d2 error| <= 2 T delta + delta^2)
         if (seam) band += fmaf(2.0f * t, dl, dl * dl);
         uint32_t hit;
-        if (shift_mode) hit = chunk_hits<DIM, false, MODE>(wc, qsm, K4, cv, cw, band, unc);
-        else hit = chunk_hits<DIM, PERIODIC, MODE>(wc, qsm, K4, cv, cw, band, unc);
+        if (MODE != kSuperSymmetric && (!PERIODIC || shift_mode)) {
+            float umin = inf;
+            hit = chunk_hits_x2<DIM, MODE>(sm.qp[w], K4, cv, cw, umin);
+            unc |= umin <= band;
+        } else if (shift_mode) {
+            hit = chunk_hits<DIM, false, MODE>(wc, qsm, K4, cv, cw, band, unc);
+        } else {
+            hit = chunk_hits<DIM, PERIODIC, MODE>(wc, qsm, K4, cv, cw, band, unc);
+        }
         const uint32_t m = warp_transpose32(hit, lane);
         if (lane < nb) {
             count += __popc(m);
@@ -1705,10 +1777,13 @@ __global__ void __launch_bounds__(kWalkWarps * 32) walk_emit_kernel(WalkArgs a) 
 
 // Emit pass for staged units: expand each unit's record into its queries' CSR/COO slots, one warp
 // per unit, window by window of kExpandWin chunks.  The window's candidate columns are gathered
-// into shared memory once (consecutive sorted indices: coalesced reads of the sort index), lanes
-// over (query, chunk) pairs expand their hit bits into a shared output table (source chunk and bit
-// of every output, in output order), and lanes over output positions write consecutive slots.  A
-// window of more than kExpandTab outputs is written query by query instead.
+// into shared memory once (consecutive sorted indices: coalesced reads of the sort index; each
+// lane finds its candidate's run by a rank in the window's run-start bitmap).  Lanes over
+// (query, chunk) pairs -- lane = query + nbp * g takes chunk g of each group of 32 / nbp chunks,
+// nbp the unit's query count rounded up to a power of two -- expand their hit bits into a shared
+// output table (query, chunk and bit of every output, in output order), and lanes over output
+// positions write consecutive slots.  A window of more than kExpandTab outputs is written query by
+// query instead.
 constexpr int kExpandWarps = 8;
 constexpr int kExpandWin = 16;    // chunks per window: 512 candidates
 constexpr int kExpandTab = 2048;  // outputs one table holds
@@ -1716,9 +1791,11 @@ struct ExpandSmem {
     int32_t col[kExpandWarps][kExpandWin * 32];    // output column of each candidate of the window
     uint32_t mask[kExpandWarps][kExpandWin * 32];  // the window's masks, [chunk][query]
     uint16_t tab[kExpandWarps][kExpandTab];        // (query << 9) | (chunk << 5) | bit, in output order
+    uint32_t rstart[kExpandWarps][kExpandWin];     // bit k of word c: a run starts at candidate 32 c + k
+    int32_t rrank[kExpandWarps][kExpandWin];       // runs starting before word c, minus one
     int32_t run_beg[kExpandWarps][32];
     int32_t run_pre[kExpandWarps][33];
-    int32_t qpre[kExpandWarps][33];                // exclusive output prefix over queries (this window)
+    int64_t qbase[kExpandWarps][32];               // output slot of table entry 0 of each query (this window)
     int64_t qoff[kExpandWarps][32];                // output position of each query's next hit
     int32_t qrow[kExpandWarps][32];
 };
@@ -1785,17 +1862,37 @@ __global__ void __launch_bounds__(kExpandWarps * 32, 3) expand_records_kernel(Ex
         }
         __syncwarp();
         const int32_t M = rpre[R];
-        int32_t cr = 0;  // run of this lane's candidate, moving forward only
+        // lane = q + nbp * g: query q, chunk g of each group of G chunks
+        const int lg = nb > 1 ? 32 - __clz(nb - 1) : 0;
+        const int nbp = 1 << lg, G = 32 >> lg;
+        const int q = lane & (nbp - 1), g = lane >> lg;
+        const bool qlane = q < nb;
         for (int32_t c0 = 0; c0 < nchunks; c0 += kExpandWin) {
             const int32_t nc = min(kExpandWin, nchunks - c0);
+            const int32_t wbase = c0 << 5;
+            // run of candidate wbase + k: the runs starting at or before it, minus one
+            if (lane < kExpandWin) sm.rstart[w][lane] = 0u;
+            __syncwarp();
+            const bool rl = lane < R;
+            const int32_t rs = rl ? rpre[lane] - wbase : -1;
+            const int32_t nbefore = __popc(__ballot_sync(0xffffffffu, rl && rs < 0));
+            if (rl && rs >= 0 && rs < (nc << 5)) atomicOr(&sm.rstart[w][rs >> 5], 1u << (rs & 31));
+            __syncwarp();
+            const int32_t wp = lane < kExpandWin ? __popc(sm.rstart[w][lane]) : 0;
+            const int32_t wpi = warp_inclusive_scan(wp);
+            if (lane < kExpandWin) sm.rrank[w][lane] = nbefore + wpi - wp - 1;
+            __syncwarp();
+            const uint32_t le = (2u << lane) - 1u;  // bits 0 .. lane
             for (int32_t cc = 0; cc < nc; ++cc) {
-                const int32_t k = ((c0 + cc) << 5) + lane;
+                const int32_t k = wbase + (cc << 5) + lane;
                 int32_t col = 0;
                 if (k < M) {
-                    while (rpre[cr + 1] <= k) ++cr;
-                    const int32_t j = rbeg[cr] + (k - rpre[cr]);
-                    const int32_t jl = TCR_GUARD(j, a.nr) ? __ldg(&a.rsidx[j]) : 0;
-                    col = a.ref_ids ? __ldg(&a.ref_ids[jl]) : jl - rshift;
+                    const int32_t cr = sm.rrank[w][cc] + __popc(sm.rstart[w][cc] & le);
+                    if (TCR_GUARD(cr, R)) {
+                        const int32_t j = rbeg[cr] + (k - rpre[cr]);
+                        const int32_t jl = TCR_GUARD(j, a.nr) ? __ldg(&a.rsidx[j]) : 0;
+                        col = a.ref_ids ? __ldg(&a.ref_ids[jl]) : jl - rshift;
+                    }
                 }
                 cols[(cc << 5) + lane] = col;
             }
@@ -1803,52 +1900,57 @@ __global__ void __launch_bounds__(kExpandWarps * 32, 3) expand_records_kernel(Ex
             const uint32_t* src = masks + (int64_t)c0 * nb;
             for (int32_t i = lane; i < nm; i += 32) mks[i] = __ldcs(&src[i]);
             __syncwarp();
+            // the window's outputs of each query, and their exclusive prefix over the queries
             int32_t tot = 0;
-            if (lane < nb)
-                for (int32_t cc = 0; cc < nc; ++cc) tot += __popc(mks[cc * nb + lane]);
-            const int32_t qinc = warp_inclusive_scan(tot);
-            sm.qpre[w][lane + 1] = qinc;
-            if (lane == 0) sm.qpre[w][0] = 0;
-            const int32_t n = __shfl_sync(0xffffffffu, qinc, 31);
+            if (qlane)
+                for (int32_t c = g; c < nc; c += G) tot += __popc(mks[c * nb + q]);
+            for (int sft = nbp; sft < 32; sft <<= 1) tot += __shfl_xor_sync(0xffffffffu, tot, sft);
+            const int32_t tv = (g == 0 && qlane) ? tot : 0;
+            const int32_t tinc = warp_inclusive_scan(tv);
+            const int32_t n = __shfl_sync(0xffffffffu, tinc, 31);
+            const int32_t qpre = __shfl_sync(0xffffffffu, tinc - tv, q);
             if (n <= kExpandTab) {
-                // lanes over (query, chunk) pairs in output order; each expands its few hit bits
-                int32_t carry = 0;
-                int pq = 0, pc = lane;  // pair (query, chunk) of p = base + lane, advanced without division
-                while (pc >= nc) { pc -= nc; ++pq; }
-                for (int32_t base = 0; base < nm; base += 32) {
-                    uint32_t m = base + lane < nm ? mks[pc * nb + pq] : 0u;
-                    const int32_t cnt = __popc(m);
-                    const int32_t inc = warp_inclusive_scan(cnt);
-                    int32_t k = carry + inc - cnt;
-                    carry += __shfl_sync(0xffffffffu, inc, 31);
-                    const int32_t tag = (pq << 9) | (pc << 5);
-                    while (m) {
-                        const int bit = __ffs(m) - 1;
-                        m &= m - 1;
-                        tab[k++] = (uint16_t)(tag | bit);
+                // each lane expands its (query, chunk) mask into the table, highest bit at the end
+                int32_t run = qpre;  // table slot of the query's next output
+                for (int32_t cc0 = 0; cc0 < nc; cc0 += G) {
+                    const int32_t c = cc0 + g;
+                    uint32_t m = (qlane && c < nc) ? mks[c * nb + q] : 0u;
+                    int32_t inc = __popc(m);
+                    for (int sft = nbp; sft < 32; sft <<= 1) {  // inclusive scan over g, per query
+                        const int32_t t = __shfl_up_sync(0xffffffffu, inc, sft);
+                        if (lane >= sft) inc += t;
                     }
-                    pc += 32;
-                    while (pc >= nc) { pc -= nc; ++pq; }
+                    const int32_t tq = __shfl_sync(0xffffffffu, inc, q + 32 - nbp);
+                    int32_t pos = run + inc;
+                    const uint32_t tag = ((uint32_t)q << 9) | ((uint32_t)c << 5);
+                    while (m) {
+                        const int bit = 31 - __clz(m);
+                        m ^= 1u << bit;
+                        tab[--pos] = (uint16_t)(tag | bit);
+                    }
+                    run += tq;
                 }
+                if (g == 0 && qlane) sm.qbase[w][q] = sm.qoff[w][q] - qpre;
                 __syncwarp();
+                const bool rows = a.row_out != nullptr;
 #pragma unroll 4
                 for (int32_t o = lane; o < n; o += 32) {
-                    const int32_t v = tab[o];
-                    const int q = v >> 9;
-                    const int64_t pos = sm.qoff[w][q] + (o - sm.qpre[w][q]);
+                    const uint32_t v = tab[o];
+                    const uint32_t vq = v >> 9;
+                    const int64_t pos = sm.qbase[w][vq] + o;
                     if (TCR_GUARD(pos, a.out_cap)) {
-                        __stcs(reinterpret_cast<long long*>(&a.col_out[pos]), (long long)cols[v & 0x1ff]);
-                        if (a.row_out) __stcs(reinterpret_cast<long long*>(&a.row_out[pos]), (long long)sm.qrow[w][q]);
+                        __stcs(reinterpret_cast<long long*>(&a.col_out[pos]), (long long)cols[v & 0x1ffu]);
+                        if (rows) __stcs(reinterpret_cast<long long*>(&a.row_out[pos]), (long long)sm.qrow[w][vq]);
                     }
                 }
             } else {
                 // many outputs: query by query, lanes over the window's chunks
-                for (int32_t q = 0; q < nb; ++q) {
-                    uint32_t m = lane < nc ? mks[lane * nb + q] : 0u;
+                for (int32_t qq = 0; qq < nb; ++qq) {
+                    uint32_t m = lane < nc ? mks[lane * nb + qq] : 0u;
                     const int32_t cnt = __popc(m);
                     const int32_t inc = warp_inclusive_scan(cnt);
-                    int64_t pos = sm.qoff[w][q] + (inc - cnt);
-                    const long long row = sm.qrow[w][q];
+                    int64_t pos = sm.qoff[w][qq] + (inc - cnt);
+                    const long long row = sm.qrow[w][qq];
                     while (m) {
                         const int bit = __ffs(m) - 1;
                         m &= m - 1;
@@ -1861,7 +1963,7 @@ __global__ void __launch_bounds__(kExpandWarps * 32, 3) expand_records_kernel(Ex
                 }
             }
             __syncwarp();
-            if (lane < nb) sm.qoff[w][lane] += tot;
+            if (g == 0 && qlane) sm.qoff[w][q] += tot;
             __syncwarp();
         }
     }
@@ -2008,7 +2110,20 @@ struct HostBatch {
     const int32_t* lin_hint = nullptr;  // incremental build: previous linear cell of every reference point
     int32_t* lin_out = nullptr;         // receives the linear cell of every sorted reference point
     int32_t* order_out = nullptr;       // receives the input index of every sorted reference point
+    int unit_cap = kDefaultUnitQueries;           // queries per work unit
+    int walk_bps = kDefaultWalkBlocksPerSM;       // resident walk blocks per SM
 };
+
+// The descriptors' tuning fields (0: default).
+static int take_tuning(HostBatch& b, int32_t unit_queries, int32_t walk_blocks_per_sm) {
+    if (unit_queries != 0 && unit_queries != 8 && unit_queries != 16 && unit_queries != 32)
+        return set_error(TCR_ERR_INVALID, "unit_queries must be 8, 16 or 32 (0: default 32)");
+    if (walk_blocks_per_sm < 0 || walk_blocks_per_sm > 64)
+        return set_error(TCR_ERR_INVALID, "walk_blocks_per_sm must be in [1, 64] (0: default 12)");
+    b.unit_cap = unit_queries ? unit_queries : kDefaultUnitQueries;
+    b.walk_bps = walk_blocks_per_sm ? walk_blocks_per_sm : kDefaultWalkBlocksPerSM;
+    return TCR_OK;
+}
 
 // Validation shared by both descriptors.  level 0: sizes only; 1: query phases (the reference
 // supports come from the structure); 2: structure build.
@@ -2104,6 +2219,7 @@ static int batch_of_desc(const tcr_search_desc* d, int level, HostBatch& b) {
     b.query_ids = d->query_ids;
     b.ref_ids = d->ref_ids;
     b.clouds.push_back(cp);
+    if ((rc = take_tuning(b, d->unit_queries, d->walk_blocks_per_sm))) return rc;
     return finish_batch(b, kSingleMapMin);
 }
 
@@ -2123,6 +2239,7 @@ static int batch_of(const tcr_batch_desc* bd, int level, HostBatch& b) {
     b.lin_out = bd->ref_lin_out;
     b.order_out = bd->ref_order_out;
     b.clouds.resize(bd->n_clouds);
+    if (int rc = take_tuning(b, bd->unit_queries, bd->walk_blocks_per_sm)) return rc;
     char who[48];
     for (int k = 0; k < bd->n_clouds; ++k) {
         const tcr_cloud_desc& c = bd->clouds[k];
@@ -2324,9 +2441,9 @@ static cudaError_t launch_walks(const HostBatch& b, WalkArgs a, dim3 grid, dim3 
 
 // Persistent walk grid: the blocks loop over units through an atomic counter, so the size only
 // sets the parallelism -- about two units per query group's worth of full units per warp.
-static unsigned walk_blocks(int64_t nq) {
-    const int64_t max_units = 2 * nq / g_unit_cap + 1;
-    return (unsigned)std::max<int64_t>(1, std::min<int64_t>((int64_t)num_sms() * g_walk_blocks_per_sm,
+static unsigned walk_blocks(const HostBatch& b, int64_t nq) {
+    const int64_t max_units = 2 * nq / b.unit_cap + 1;
+    return (unsigned)std::max<int64_t>(1, std::min<int64_t>((int64_t)num_sms() * b.walk_bps,
                                                             (max_units + kWalkWarps - 1) / kWalkWarps));
 }
 
@@ -2405,7 +2522,7 @@ static int count_impl(const HostBatch& b, const Structure& S, const Scratch& W, 
     const int64_t nq = b.nq;
     int rc = upload_table(b, W, st);
     if (rc) return rc;
-    const int unit_cap = g_unit_cap;
+    const int unit_cap = b.unit_cap;
     count_init_kernel<<<grid_for(std::max<int64_t>(C, nq), 256), 256, 0, st>>>(W, C, unit_cap, nq);
     note_launches(1);
     if (b.any_query_sup && nq > 0 && !b.same_sorted) {
@@ -2462,7 +2579,7 @@ static int count_impl(const HostBatch& b, const Structure& S, const Scratch& W, 
         a.stage = stage;
         a.stage_cap = stage_cap;
         prof_mark(TCR_PROFILE_COUNT_WALK, 0, st);
-        TCR_CUDA(launch_walks<CountLaunch>(b, a, dim3(walk_blocks(nq)), dim3(kWalkWarps * 32), 0, st));
+        TCR_CUDA(launch_walks<CountLaunch>(b, a, dim3(walk_blocks(b, nq)), dim3(kWalkWarps * 32), 0, st));
         prof_mark(TCR_PROFILE_COUNT_WALK, 1, st);
         stray_kernel<false><<<grid_for(nq, 128, num_sms() * 4), 128, 0, st>>>(a);
         note_launches(1);
@@ -2522,7 +2639,7 @@ static int emit_impl(const HostBatch& b, const Structure& S, const Scratch& W, c
         note_launches(1);
     }
     TCR_CUDA(cudaMemsetAsync(W.work, 0, sizeof(int32_t) * kWorkCounters, st));
-    TCR_CUDA(launch_walks<EmitLaunch>(b, a, dim3(walk_blocks(nq)), dim3(kWalkWarps * 32), 0, st));
+    TCR_CUDA(launch_walks<EmitLaunch>(b, a, dim3(walk_blocks(b, nq)), dim3(kWalkWarps * 32), 0, st));
     stray_kernel<true><<<grid_for(nq, 128, num_sms() * 4), 128, 0, st>>>(a);
     note_launches(1);
     return TCR_OK;
@@ -2632,16 +2749,6 @@ int tcr_debug_checks(int64_t* out3) {
     return TCR_OK;
 }
 #endif
-
-int tcr_set_tuning(int32_t unit_queries, int32_t walk_blocks_per_sm) {
-    if (unit_queries != 0 && unit_queries != 8 && unit_queries != 16 && unit_queries != 32)
-        return set_error(TCR_ERR_INVALID, "unit_queries must be 8, 16 or 32 (0: default 32)");
-    if (walk_blocks_per_sm < 0 || walk_blocks_per_sm > 64)
-        return set_error(TCR_ERR_INVALID, "walk_blocks_per_sm must be in [1, 64] (0: default 12)");
-    g_unit_cap = unit_queries ? unit_queries : 32;
-    g_walk_blocks_per_sm = walk_blocks_per_sm ? walk_blocks_per_sm : 12;
-    return TCR_OK;
-}
 
 int tcr_search_sizes(int64_t n_query, int64_t n_ref, int32_t dim, int64_t* structure_bytes, int64_t* scratch_bytes) {
     if (dim < 1 || dim > 3 || n_query < 0 || n_ref < 0) return set_error(TCR_ERR_INVALID, "invalid sizes");

@@ -26,10 +26,10 @@ import math
 import torch
 
 from . import _lib
+from . import context as _context
 from .search import _check_info, _ptr
 
 GROW = 1.0 + 1e-3  # covers cell-index rounding and the seam cell's width error
-_stage_per_query = [96.0]  # staging words per level-pair query of the previous search
 
 
 def _levels(h, H0, L):
@@ -146,7 +146,8 @@ def multilevel_search(xq, hq, xr, hr, lo, hi, mask, mode, fmt, max_levels=4):
         nqb = int(table["n_query"].sum())
         sbuf = torch.empty(s_bytes, dtype=torch.uint8, device=device)
         scratch = torch.empty(w_bytes, dtype=torch.uint8, device=device)
-        stage_cap = int(min(0x7fffffff, _stage_per_query[0] * 1.1 * nqb + 65536))
+        ctx = _context.current()
+        stage_cap = int(min(0x7fffffff, ctx.level_stage_per_query * 1.1 * nqb + 65536))
         stage = torch.empty(stage_cap, dtype=torch.int32, device=device)
         off_b = torch.empty(nqb + 1, dtype=torch.int64, device=device)
         cnt_b = torch.empty(nqb, dtype=torch.int64, device=device)
@@ -162,7 +163,7 @@ def multilevel_search(xq, hq, xr, hr, lo, hi, mask, mode, fmt, max_levels=4):
     total = int(offsets[-1])  # the one host synchronisation
     if pairs:
         _check_info(info)
-        _stage_per_query[0] = max(int(info[4]) / max(nqb, 1), 1.0)
+        ctx.level_stage_per_query = max(int(info[4]) / max(nqb, 1), 1.0)
     if fmt == "csr" and total > 0x7fffffff:
         raise ValueError(f"{total} pairs do not fit the int32 indptr of SparseCSR")
     col = torch.empty(total, dtype=torch.int64, device=device)

@@ -14,13 +14,9 @@ from typing import Optional
 import torch
 
 from . import _lib
+from . import context as _context
 
 _tls = threading.local()
-
-# Pairs and staging words per query of the previous search: they size the output and the staging
-# list of the next one.
-_pairs_per_query = [64.0]
-_stage_per_query = [64.0]
 
 
 def _info_buffer():
@@ -95,7 +91,7 @@ def make_desc(dim, mode, mask, lo, hi, L, xq, hq, xr, hr, self_search):
     d.query_sup = hq.data_ptr() if hq is not None and hq.numel() else None
     d.ref_pos = xr.data_ptr() if xr.numel() else None
     d.ref_sup = hr.data_ptr() if hr is not None and hr.numel() else None
-    return d
+    return _context.apply_tuning(d)
 
 
 class CompactHashMap:
@@ -287,8 +283,9 @@ def compact_search(xq, hq, xr, hr, domain_lo, domain_hi, mask, mode, L, fmt, sel
     info = _info_buffer()
     # One estimate sizes both the staging list and the output, so count and emit are enqueued
     # back to back and the host waits only once, at the end.
-    cap = int(min(0x7fffffff, _pairs_per_query[0] * 1.25 * nq + 4096))
-    stage_cap = int(min(0x7fffffff, _stage_per_query[0] * 1.1 * nq + 65536))
+    ctx = _context.current()
+    cap = int(min(0x7fffffff, ctx.pairs_per_query * 1.25 * nq + 4096))
+    stage_cap = int(min(0x7fffffff, ctx.stage_per_query * 1.1 * nq + 65536))
     stage = torch.empty(stage_cap, dtype=torch.int32, device=device)
     col = torch.empty(cap, dtype=torch.int64, device=device)
     row = torch.empty(cap, dtype=torch.int64, device=device) if fmt == "coo" else None
@@ -305,8 +302,8 @@ def compact_search(xq, hq, xr, hr, domain_lo, domain_hi, mask, mode, L, fmt, sel
     _check_info(info)
     total = int(info[0])
     if nq:
-        _pairs_per_query[0] = max(total / nq, 1.0)
-        _stage_per_query[0] = max(int(info[4]) / nq, 1.0)
+        ctx.pairs_per_query = max(total / nq, 1.0)
+        ctx.stage_per_query = max(int(info[4]) / nq, 1.0)
     if fmt == "csr" and total > 0x7fffffff:
         raise ValueError(f"{total} pairs do not fit the int32 indptr of SparseCSR")
     if total > cap:  # the estimate was short: emit again into an exact buffer (the count is kept)

@@ -26,7 +26,7 @@ import numpy as np
 import torch
 
 from . import _lib
-from . import search as _search
+from . import context as _context
 from .search import _check_info, _info_buffer, _ptr, make_desc
 
 
@@ -138,7 +138,8 @@ def compact_search_f64(xq, hq, xr, hr, lo, hi, mask, mode, L, fmt, self_search, 
         rowEntries = torch.empty(nq, dtype=torch.int64, device=device)
     info = _info_buffer()
     # the count walk stages each unit's hit masks for the emit (sized like the float32 search's)
-    stage_cap = int(min(0x7fffffff, _search._stage_per_query[0] * 1.1 * nq + 65536))
+    ctx = _context.current()
+    stage_cap = int(min(0x7fffffff, ctx.stage_per_query * 1.1 * nq + 65536))
     stage = torch.empty(stage_cap, dtype=torch.int32, device=device)
     _lib.check(lib.tcr_count_f64(ctypes.byref(desc), ctypes.byref(inputs), _ptr(sbuf), _ptr(scratch), w_bytes,
                                  _ptr(stage), stage_cap, _ptr(offsets), _ptr(indptr), _ptr(rowEntries),
@@ -147,7 +148,7 @@ def compact_search_f64(xq, hq, xr, hr, lo, hi, mask, mode, L, fmt, self_search, 
     _check_info(info)
     total = int(info[0])
     if nq:
-        _search._stage_per_query[0] = max(int(info[4]) / nq, 1.0)
+        ctx.stage_per_query = max(int(info[4]) / nq, 1.0)
     if fmt == "csr" and total > 0x7fffffff:
         raise ValueError(f"{total} pairs do not fit the int32 indptr of SparseCSR")
     col = torch.empty(max(total, 1), dtype=torch.int64, device=device)

@@ -31,6 +31,7 @@ from typing import Dict, List, Optional
 import numpy as np
 import torch
 
+from . import context as _context
 from .batched import BatchBuffers, cloud_table, run_batch
 from .search import _as_f32, _domain_host, _require_cuda
 from .util import DomainDescription, SparseCOO
@@ -134,6 +135,11 @@ class SearchServer:
         self._threads = []
         self.batches = 0
         self.batched_requests = 0
+        self.tuning = (0, 0)  # (queries per unit, walk blocks per SM) of the workers' searches; 0: default
+
+    def set_tuning(self, config):
+        """Tuning of the searches the workers make from now on (an Autotuner's `apply`)."""
+        self.tuning = (int(config[0]), int(config[1]))
 
     # -- setup ----------------------------------------------------------------------------
     def add_scene(self, scene: Scene) -> int:
@@ -242,6 +248,7 @@ class SearchServer:
             torch.cuda.set_device(self.device)
             stream = torch.cuda.Stream(self.device)
             bufs = {d: BatchBuffers(self.device) for d in (1, 2, 3)}
+            ctx = _context.SearchContext()  # this worker's size estimates
         except BaseException as ex:  # no worker: fail what waits instead of leaving it hanging
             with self._cv:
                 while self._pending:
@@ -260,10 +267,12 @@ class SearchServer:
                 if not batch:
                     return
             try:
-                for dim in (1, 2, 3):
-                    group = [r for r in batch if self.scenes[r.scene].dim == dim]
-                    if group:
-                        self._run(group, dim, stream, bufs[dim])
+                ctx.unit_queries, ctx.walk_blocks_per_sm = self.tuning
+                with _context.use(ctx):
+                    for dim in (1, 2, 3):
+                        group = [r for r in batch if self.scenes[r.scene].dim == dim]
+                        if group:
+                            self._run(group, dim, stream, bufs[dim])
             except BaseException as ex:  # the requests report it; the server keeps serving
                 for r in batch:
                     r.error = ex
