@@ -48,6 +48,8 @@ def parse():
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-batched", action="store_true", help="skip the batched-form measurement")
+    ap.add_argument("--details", default="bench_details.json",
+                    help="file that receives the full measurement (the printed line keeps a summary of each form)")
     ap.add_argument("--profile-searches", type=int, default=0,
                     help="only run this many eager searches of the workload (a small case for ncu captures)")
     ap.add_argument("--profile-scatter", type=int, default=0,
@@ -702,6 +704,47 @@ def tcr_launches():
     return int(_lib.load().tcr_kernel_launches())
 
 
+def bench_fixed_support(dev, flush, steps=5):
+    """One support for every point (supportOverride): the 1M-point workload's positions with the
+    mean support, symmetric CSR, searched once with the supports given as an array (the two-support
+    symmetric walk) and once with supportOverride (the fixed-radius form: the gather walk); the
+    same CSR both ways."""
+    import torch
+
+    import torchcompactradius_b200 as tcr
+    pos, sup = make_workload()
+    x = pos.to(dev)
+    hval = float(sup.mean())
+    hs = torch.full((x.shape[0],), hval, device=dev)
+    dom = tcr.DomainDescription(torch.full((3,), -1.0), torch.full((3,), 1.0), torch.zeros(3, dtype=torch.bool), 3)
+    stream = torch.cuda.current_stream(dev)
+
+    def run(fixed):
+        if fixed:
+            return tcr.radiusSearch(tcr.PointCloud(x, None), None, supportOverride=hval, mode="symmetric",
+                                    domain=dom, algorithm="compact", format="csr")
+        return tcr.radiusSearch(tcr.PointCloud(x, hs), None, mode="symmetric", domain=dom, algorithm="compact",
+                                format="csr")
+
+    out = {}
+    for fixed in (False, True):
+        adj = run(fixed)
+        ms = []
+        for k in range(steps):
+            flush.fill_(k & 0xff)
+            s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            s.record(stream)
+            adj = run(fixed)
+            e.record(stream)
+            e.synchronize()
+            ms.append(s.elapsed_time(e))
+        out["fixed" if fixed else "array"] = (statistics.median(ms), adj)
+    (ta, a), (tf, f) = out["array"], out["fixed"]
+    return {"workload": f"3d_1m positions, one support {hval:.6g} for every point, symmetric CSR",
+            "pairs": int(f.indices.numel()), "supports_array_ms": ta, "support_override_ms": tf,
+            "speedup": ta / tf, "same_csr": bool(torch.equal(a.indices, f.indices) and torch.equal(a.indptr, f.indptr))}
+
+
 def bench_f64(dev, flush, steps=3, cpu=True):
     """The 1M-point workload in float64 (positions, supports and domain): the reference's double
     search, symmetric CSR, timed per search with events (L2 flushed), and the reference's own double
@@ -728,7 +771,7 @@ def bench_f64(dev, flush, steps=3, cpu=True):
     pairs = int(adj.indices.numel())
     res = {"workload": "3d_1m_uniform_symmetric_csr in float64 (positions, supports, domain)", "pairs": pairs,
            "ms_per_search": statistics.median(ms), "value": pairs / (statistics.median(ms) / 1e3), "unit": "pairs/s",
-           "note": "one thread per query, every stencil candidate tested in double"}
+           "note": "the float32 walk over float32 copies; pairs within the widened rounding band decided in double"}
     if cpu:
         try:
             from oracle import ref_pipeline
@@ -967,6 +1010,7 @@ def run_b200(args):
         line["adaptive"] = bench_adaptive(dev, flush)
         line["scatter"] = bench_scatter(dev, flush)
         line["f64"] = bench_f64(dev, flush, cpu=rank == 0 and not args.no_cpu_baseline)
+        line["fixed_support"] = bench_fixed_support(dev, flush)
         del flush
         line["served"] = bench_served(dev)
     if world > 1:
@@ -980,8 +1024,64 @@ def run_b200(args):
             cb["note"] = f"reference operators unavailable: {ex}"
         line["cpu_baseline"] = cb
     if rank == 0:
-        print(json.dumps(line))
+        print(json.dumps(summarize(line, args.details)))
     return 0
+
+
+def _pick(d, *keys):
+    return {k: d[k] for k in keys if isinstance(d, dict) and k in d}
+
+
+def summarize(line, details_path):
+    """The printed line: the headline keys in full and a summary of every other form; the full
+    record goes to `details_path` (the line names it)."""
+    out = dict(line)
+    try:
+        with open(details_path, "w") as f:
+            json.dump(line, f, indent=1)
+        out["details"] = os.path.abspath(details_path)
+    except OSError as ex:
+        out["details"] = f"not written: {ex}"
+    if "tuning" in out:
+        out["tuning"] = out["tuning"].get("chosen", out["tuning"])
+    b = line.get("batched")
+    if b:
+        out["batched"] = dict(_pick(b, "value", "unit", "ms_per_step", "p99_ms", "speedup_vs_per_call"),
+                              clouds=b.get("clouds"), per_call_pairs_match=b.get("per_call", {}).get("pairs_match"),
+                              e2e=_pick(b.get("e2e", {}), "value", "unit"),
+                              cpu_baseline=_pick(b.get("cpu_baseline", {}), "value", "unit", "cores", "kind"))
+    g = line.get("graphs")
+    if g:
+        out["graphs"] = {"small_graph_p50_ms": g.get("small", {}).get("graph_p50_ms"),
+                         "small_eager_p50_ms": g.get("small", {}).get("eager_p50_ms"),
+                         "big_graph_replay_ms": g.get("big", {}).get("graph_replay_ms")}
+    a = line.get("adaptive")
+    if a:
+        out["adaptive"] = {"mlm_ms": a.get("mlm", {}).get("ms_per_search"),
+                           "compact_ms": a.get("compact", {}).get("ms_per_search"),
+                           "pairs": a.get("mlm", {}).get("pairs"), "same_pair_set": a.get("same_pair_set"),
+                           "speedup_mlm_vs_compact": a.get("speedup_mlm_vs_compact")}
+    sc = line.get("scatter")
+    if sc:
+        out["scatter"] = dict(_pick(sc, "ms_per_call", "value", "unit", "repeatable"),
+                              roofline_frac=sc.get("roofline", {}).get("frac"),
+                              cpu_bit_identical=sc.get("cpu_baseline", {}).get("bit_identical"))
+    f = line.get("f64")
+    if f:
+        out["f64"] = dict(_pick(f, "ms_per_search", "value", "unit", "pairs"),
+                          pairs_match=f.get("cpu_baseline", {}).get("pairs_match"),
+                          indptr_match=f.get("cpu_baseline", {}).get("indptr_match"))
+    fs = line.get("fixed_support")
+    if fs:
+        out["fixed_support"] = _pick(fs, "supports_array_ms", "support_override_ms", "speedup", "same_csr")
+    sv = line.get("served")
+    if sv:
+        out["served"] = {"speedup_vs_per_call": sv.get("speedup_vs_per_call"),
+                         "served_capacity": _pick(sv.get("served_capacity", {}), "value", "unit", "mean_batch"),
+                         "served": _pick(sv.get("served", {}), "value", "p50_ms", "p99_ms", "requests"),
+                         "per_call": _pick(sv.get("per_call", {}), "value", "p50_ms", "p99_ms"),
+                         "tuning": sv.get("tuning", {}).get("chosen")}
+    return out
 
 
 def profile_searches(n):

@@ -196,8 +196,7 @@ int tcr_build_structure(const tcr_search_desc* d, void* structure, int64_t struc
  * offsets: device int64 [n_query+1] (exclusive scan, offsets[n_query] = total pairs).
  * indptr_out (device int32 [n_query+1]) and row_entries_out (device int64 [n_query]) are the
  * SparseCSR fields of util.py:321-358 and may be NULL.  info_out (host, 8 x int64, may be NULL)
- * receives, asynchronously on `stream`: {total pairs, clouds without a valid grid (-1: a bounded
- * wait of a device-wide scan or sort gave up and nothing of the search is valid), queries walked serially,
+ * receives, asynchronously on `stream`: {total pairs, clouds without a valid grid, queries walked serially,
  * exact-only mode, staging words the units asked for, units left for tcr_emit to re-test, units
  * re-tested with exact decisions because a pair lay within the fast test's rounding band, and
  * for a batch built with a linear-cell hint the points its incremental re-sort sorted (-1: it fell
@@ -240,17 +239,20 @@ int tcr_batch_emit(const tcr_batch_desc* b, const void* structure, void* scratch
  * search time (a host that gives the search a fixed arena at start-up and forbids cudaMalloc
  * afterwards, e.g. because cudaMalloc can synchronise the device inside a real-time loop, or a
  * plugin host whose allocator the search cannot reach).  The structure and scratch live in a
- * 32 MiB file-scope device array that every GPU loading this library holds until exit, which
- * bounds a search to about 180K points (the exact limit is the byte size of structure plus
- * scratch; larger searches are rejected with TCR_ERR_INVALID before any device work).
+ * 32 MiB file-scope device array that every GPU loading this library holds until exit.  A search
+ * fits when its structure plus scratch bytes (tcr_search_sizes) do not exceed the array; larger
+ * searches are rejected with TCR_ERR_INVALID before any device work, naming the bytes they need.
+ * What is left of the array after structure and scratch is the staging list of tcr_count (units
+ * whose records do not fit it are tested again by the emit).
  * The caller passes its inputs in `d` and its outputs: offsets (device int64 [n_query+1]),
  * optional indptr_out / row_entries_out as in tcr_count, row_out (NULL for CSR) and col_out of
  * pair_capacity entries.  The call synchronises `stream` once to learn the pair count
  * (*total_out); if it exceeds pair_capacity nothing is emitted and TCR_ERR_INVALID is returned,
  * so the caller can retry with a larger output.
- * The first call on a device looks the array up with cudaGetSymbolAddress; make that first call
- * before any stream capture.  All calls share the one array: calls whose work overlaps on the GPU
- * (other streams, other host threads) race and must be serialised by the caller. */
+ * The call synchronises `stream` (between the count and the emit), so it can never run inside a
+ * stream capture or a CUDA graph; callers that need graphs use tcr_build_structure / tcr_count /
+ * tcr_emit with their own buffers.  All calls share the one array: calls whose work overlaps on
+ * the GPU (other streams, other host threads) race and must be serialised by the caller. */
 int tcr_search_noalloc(const tcr_search_desc* d, int64_t* offsets, int32_t* indptr_out, int64_t* row_entries_out,
                        int64_t* row_out, int64_t* col_out, int64_t pair_capacity, int64_t* total_out, void* stream);
 

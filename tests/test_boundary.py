@@ -212,3 +212,36 @@ def test_scatter_index_broadcast_matches_reference_rule():
     assert torch.equal(b[2, :, 3], torch.arange(5))
     full = torch.zeros(3, 5, 4, dtype=torch.int64)
     assert broadcast(full, src, 1).data_ptr() == full.data_ptr()
+
+
+def test_noalloc_accepts_exactly_what_its_static_array_holds():
+    """tcr_search_noalloc rejects, before any device work, every search whose structure plus
+    scratch (tcr_search_sizes) exceed its 32 MiB array, naming the bytes; the largest self-search
+    below the limit is sized within it."""
+    from torchcompactradius_b200 import _lib
+    lib = _lib.load()
+    limit = 32 << 20
+    for dim in (1, 2, 3):
+        lo, hi = 1, 1 << 22
+        while hi - lo > 1:  # largest n whose self-search fits
+            mid = (lo + hi) // 2
+            s, w = _lib.search_sizes(mid, mid, dim)
+            lo, hi = (mid, hi) if s + w <= limit else (lo, mid)
+        n = hi
+        s, w = _lib.search_sizes(n, n, dim)
+        assert s + w > limit
+        d = _lib.SearchDesc()
+        d.dim, d.mode, d.self_search, d.hash_map_length = dim, 0, 1, 4096
+        d.n_query = d.n_ref = n
+        for k in range(3):
+            d.domain_max[k] = 1.0
+        d.query_pos = d.ref_pos = d.query_sup = d.ref_sup = 256  # never dereferenced: rejected first
+        total = ctypes.c_int64(-1)
+        col = ctypes.c_void_p(512)
+        off = ctypes.c_void_p(768)
+        rc = lib.tcr_search_noalloc(ctypes.byref(d), off, None, None, None, col, 1, ctypes.byref(total), None)
+        msg = lib.tcr_last_error()
+        assert rc == -1 and total.value == -1
+        assert b"static" in msg and str(s + w).encode() in msg
+        s1, w1 = _lib.search_sizes(lo, lo, dim)
+        assert s1 + w1 <= limit and lo > 50000

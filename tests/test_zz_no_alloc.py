@@ -129,3 +129,28 @@ def test_noalloc_rejects_clouds_beyond_its_static_scratch():
     from torchcompactradius_b200 import _lib
     assert rc == -1 and total == -1
     assert b"static" in _lib.load().tcr_last_error()
+
+
+def test_noalloc_with_no_queries_writes_no_pairs():
+    from torchcompactradius_b200 import _lib
+    x, h, lo, hi, p = _case(34, 3, 5000, [False] * 3, 0.08)
+    d = _desc(x, h, lo, hi, p, "gather")
+    d.self_search = 0
+    d.n_query = 0
+    d.query_pos = d.query_sup = None
+    rc, total, off, ip, re, row, col = _noalloc(d, "coo", 4)
+    assert rc == 0, _lib.load().tcr_last_error()
+    assert total == 0
+    assert int(off[0]) == 0 and int(ip[0]) == 0
+    assert bool((col == -7).all()) and bool((row == -7).all())
+
+
+def test_noalloc_without_a_valid_grid_reports_it_and_writes_no_pairs():
+    from torchcompactradius_b200 import _lib
+    x = torch.rand(2000, 2, device="cuda")
+    h = torch.full((2000,), 1.5, device="cuda")  # support above the periodic extent: no cell grid
+    d = _desc(x, h, [0.0, 0.0], [1.0, 1.0], [True, True], "gather")
+    rc, total, _, _, _, _, col = _noalloc(d, "csr", 8)
+    assert rc == -1 and b"no valid cell grid" in _lib.load().tcr_last_error()
+    assert total == 0
+    assert bool((col == -7).all())

@@ -155,6 +155,76 @@ def run_batch(table, mode, self_search, fmt, device, local_index=True, query_ids
                 counts=counts, total=total, info=info.clone())
 
 
+class PendingBatch:
+    """A batched search enqueued on a stream and not waited for (``enqueue_batch``).  It owns every
+    buffer its kernels use until ``finish()``, which waits for ``event`` (recorded after the emit),
+    checks the device's info block and, when the output estimate was short, emits again into exact
+    buffers -- the count, offsets and staging list are kept, so only the emit runs twice."""
+
+    def __init__(self, **kw):
+        self.__dict__.update(kw)
+
+    def finish(self):
+        self.event.synchronize()
+        info = self.info
+        _check_device_fault(info)
+        if int(info[1]) != 0:
+            raise ValueError(f"{int(info[1])} cloud(s) have no valid cell grid for their domain and support")
+        total = int(info[0])
+        if total > self.cap:
+            lib = _lib.load()
+            self.col = torch.empty(total, dtype=torch.int64, device=self.device)
+            self.row = torch.empty(total, dtype=torch.int64, device=self.device) if self.fmt == "coo" else None
+            sptr = ctypes.c_void_p(self.stream.cuda_stream)
+            _lib.check(lib.tcr_batch_emit(ctypes.byref(self.desc), _ptr(self.structure), _ptr(self.scratch),
+                                          self.scratch.numel(), _ptr(self.stage), _ptr(self.offsets), _ptr(self.row),
+                                          _ptr(self.col), total, sptr), "tcr_batch_emit")
+            self.stream.synchronize()
+        self.total = total
+        return total
+
+
+def enqueue_batch(table, mode, self_search, fmt, device, stream, cap, stage_cap, local_index=True, query_ids=None,
+                  ref_ids=None, lin_hint=None, lin_out=None, order_out=None, base_index=None):
+    """Enqueues build, count and emit of one batch on `stream` into buffers of its own and returns a
+    ``PendingBatch`` without waiting: `cap` output pairs and `stage_cap` staging words are the
+    caller's estimates.  `base_index` (int64 device tensor, optional): query indices whose offsets
+    are copied to pinned host memory after the count (``PendingBatch.offsets_host``), so a caller
+    can slice per-cloud results with no device read of its own."""
+    lib = _lib.load()
+    table = np.ascontiguousarray(table)
+    b = batch_desc(table, mode, self_search, local_index, query_ids, ref_ids, lin_hint, lin_out, order_out)
+    s_bytes, w_bytes = _lib.batch_sizes(b)
+    nq = int(table["n_query"].sum())
+    cap, stage_cap = int(min(0x7fffffff, max(cap, 1))), int(min(0x7fffffff, max(stage_cap, 1)))
+    sptr = ctypes.c_void_p(stream.cuda_stream)
+    with torch.cuda.stream(stream):
+        structure = torch.empty(max(s_bytes, 1), dtype=torch.uint8, device=device)
+        scratch = torch.empty(max(w_bytes, 1), dtype=torch.uint8, device=device)
+        stage = torch.empty(stage_cap, dtype=torch.int32, device=device)
+        offsets = torch.empty(nq + 1, dtype=torch.int64, device=device)
+        col = torch.empty(cap, dtype=torch.int64, device=device)
+        row = torch.empty(cap, dtype=torch.int64, device=device) if fmt == "coo" else None
+        info = torch.zeros(8, dtype=torch.int64, pin_memory=True)
+        _lib.check(lib.tcr_batch_build_structure(ctypes.byref(b), _ptr(structure), s_bytes, _ptr(scratch), w_bytes,
+                                                 sptr), "tcr_batch_build_structure")
+        _lib.check(lib.tcr_batch_count(ctypes.byref(b), _ptr(structure), _ptr(scratch), w_bytes, _ptr(stage),
+                                       stage_cap, _ptr(offsets), None, None, ctypes.c_void_p(info.data_ptr()), sptr),
+                   "tcr_batch_count")
+        offsets_host = None
+        if base_index is not None:
+            offsets_host = torch.empty(base_index.numel(), dtype=torch.int64, pin_memory=True)
+            offsets_host.copy_(offsets.index_select(0, base_index), non_blocking=True)
+        _lib.check(lib.tcr_batch_emit(ctypes.byref(b), _ptr(structure), _ptr(scratch), w_bytes, _ptr(stage),
+                                      _ptr(offsets), _ptr(row), _ptr(col), cap, sptr), "tcr_batch_emit")
+        event = torch.cuda.Event()
+        event.record(stream)
+    return PendingBatch(desc=b, table=table, query_ids=query_ids, ref_ids=ref_ids, structure=structure,
+                        scratch=scratch, stage=stage, offsets=offsets, col=col, row=row, info=info,
+                        offsets_host=offsets_host, cap=cap, fmt=fmt, device=device, stream=stream, event=event,
+                        total=None)
+
+
 class BatchedAdjacency:
     """Adjacency of a batched search: one CSR (or COO) over the queries of all clouds in order,
     and per-cloud views ``adj[k]`` -- the ``SparseCSR`` / ``SparseCOO`` that ``radiusSearch``

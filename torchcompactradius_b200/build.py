@@ -21,6 +21,41 @@ def _nvcc():
     return "nvcc"
 
 
+OPS_LIB = "libtcr_torch_ops.so"
+OPS_SRC = "tcr_torch_ops.cpp"
+
+
+def build_ops(force=False, verbose=False):
+    """Builds the TORCH_LIBRARY operator layer (tcr_torch_ops.cpp, linked to libtcr_b200.so) into
+    the package directory; returns its path."""
+    dst = os.path.join(HERE, OPS_LIB)
+    deps = [os.path.join(CSRC, OPS_SRC), os.path.join(REPO, "include", "tcr_b200.h"), os.path.join(HERE, "libtcr_b200.so")]
+    if not force and os.path.exists(dst) and all(os.path.getmtime(d) <= os.path.getmtime(dst) for d in deps[:2]):
+        return dst
+    import shutil
+
+    from torch.utils import cpp_extension
+    bdir = os.path.join(HERE, "_build", "ops")
+    os.makedirs(bdir, exist_ok=True)
+    cmd_env = os.environ.copy()
+    # The system g++ links libstdc++ dynamically, the one copy torch uses; a toolchain whose
+    # library path holds only the static archive would give this library a second, uninitialised
+    # copy of the C++ runtime (its stream and locale state), so the system compiler is used.
+    if os.path.exists("/usr/bin/g++"):
+        os.environ["CXX"] = "/usr/bin/g++"
+    cpp_extension.load(name="tcr_torch_ops", sources=[os.path.join(CSRC, OPS_SRC)],
+                       extra_include_paths=[os.path.join(REPO, "include")],
+                       extra_cflags=["-O2", "-std=c++17"],
+                       extra_ldflags=["-L" + HERE, "-ltcr_b200",
+                                      # $$ reaches the linker as one $ through ninja, quotes keep the shell off it
+                                      "'-Wl,-rpath,$$ORIGIN'", "'-Wl,-rpath,$$ORIGIN/../..'"],
+                       with_cuda=True, is_python_module=False, build_directory=bdir, verbose=verbose)
+    os.environ.clear()
+    os.environ.update(cmd_env)
+    shutil.copy2(os.path.join(bdir, "tcr_torch_ops.so"), dst)
+    return dst
+
+
 def build(force=False, verbose=False):
     """Builds every library whose sources are newer than the .so; returns the paths."""
     out = []
@@ -40,3 +75,5 @@ def build(force=False, verbose=False):
 
 if __name__ == "__main__":
     print(build(force="--force" in sys.argv, verbose=True))
+    if "--ops" in sys.argv:
+        print(build_ops(force="--force" in sys.argv, verbose=True))

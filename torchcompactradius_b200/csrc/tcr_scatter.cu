@@ -707,7 +707,7 @@ int64_t carve_work(const Plan& p, char* base, Work& w) {
         w.vals[1] = c.take<int32_t>(p.M);
         const int64_t nh = sort_hist_elems(p.M);
         w.hist = c.take<int32_t>(nh);
-        w.tile_sums = c.take<int32_t>(scan_tiles(nh));
+        w.tile_sums = c.take<int32_t>(kBins);  // the sort's digit totals
     }
     return c.off;
 }

@@ -185,7 +185,7 @@ static Scratch carve_scratch(void* buf, int64_t nq, int64_t nr, int64_t C, bool 
     s.vals[0] = c.take<int32_t>(nmax);
     s.vals[1] = c.take<int32_t>(nmax);
     s.hist = c.take<int32_t>(sort_hist_elems(nmax));
-    s.tile_sums = c.take<int32_t>(scan_tiles(sort_hist_elems(nmax)));
+    s.tile_sums = c.take<int32_t>(kBins);  // the sort's digit totals
     s.scan_tiles64 = c.take<int64_t>(scan_tiles(nmax + 1));
     s.scan_tiles32 = c.take<int32_t>(scan_tiles(nmax + 1));
     const int64_t q = std::max<int64_t>(nq, 1);
@@ -1787,6 +1787,7 @@ __global__ void __launch_bounds__(kWalkWarps * 32) walk_emit_kernel(WalkArgs a) 
 constexpr int kExpandWarps = 8;
 constexpr int kExpandWin = 16;    // chunks per window: 512 candidates
 constexpr int kExpandTab = 2048;  // outputs one table holds
+constexpr int kExpandBatch = 8;   // global loads a lane issues before it waits for the first
 struct ExpandSmem {
     int32_t col[kExpandWarps][kExpandWin * 32];    // output column of each candidate of the window
     uint32_t mask[kExpandWarps][kExpandWin * 32];  // the window's masks, [chunk][query]
@@ -1834,17 +1835,22 @@ __global__ void __launch_bounds__(kExpandWarps * 32, 3) expand_records_kernel(Ex
     uint16_t* __restrict__ tab = sm.tab[w];
     int64_t u = (int64_t)blockIdx.x * kExpandWarps + w;
     int32_t r0n = u < nu ? a.rec[u] : -1;
+    int32_t t0n = u < nu ? a.unit_t0[u] : 0;
     for (; u < nu; u += warps) {
-        const int32_t r0 = r0n;
-        if (u + warps < nu) r0n = a.rec[u + warps];  // the next unit's record, ahead of its use
+        const int32_t r0 = r0n, t0 = t0n;
+        if (u + warps < nu) {  // the next unit's record and first query, ahead of their use
+            r0n = a.rec[u + warps];
+            t0n = a.unit_t0[u + warps];
+        }
         if (r0 < 0) continue;  // no candidates, or re-tested by the emit walk
         if (!TCR_GUARD(r0 + 3, a.stage_cap)) continue;
         const int32_t* rec = a.stage + r0;
+        // the unit's queries (lane < 32 covers every unit size) load beside the record header
+        const int32_t qrow_l = TCR_GUARD(t0 + lane, a.nq) ? a.qsidx[t0 + lane] : -1;
         const int32_t nchunks = rec[0], R = rec[1], nb = rec[2];
         if (!TCR_GUARD(R, 28) || !TCR_GUARD(nb - 1, 32) || !TCR_GUARD(r0 + record_words(R, nchunks, nb) - 1, a.stage_cap))
             continue;
         const uint32_t* masks = reinterpret_cast<const uint32_t*>(rec + kRecHeader + 2 * R + 1);
-        const int32_t t0 = a.unit_t0[u];
         int32_t rshift = 0, qshift = 0;
         if (a.local_index) {
             const CloudParams& cp = a.table[a.num_clouds == 1 ? 0 : a.group_cloud[a.unit_group[u]]];
@@ -1853,12 +1859,9 @@ __global__ void __launch_bounds__(kExpandWarps * 32, 3) expand_records_kernel(Ex
         }
         if (lane < R) rbeg[lane] = rec[kRecHeader + lane];
         if (lane <= R) rpre[lane] = rec[kRecHeader + R + lane];
-        if (lane < nb && TCR_GUARD(t0 + lane, a.nq)) {
-            const int32_t row = a.qsidx[t0 + lane];
-            if (TCR_GUARD(row, a.nq)) {
-                sm.qrow[w][lane] = a.query_ids ? a.query_ids[row] : row - qshift;
-                sm.qoff[w][lane] = a.offsets[row];
-            }
+        if (lane < nb && TCR_GUARD(qrow_l, a.nq)) {
+            sm.qrow[w][lane] = a.query_ids ? a.query_ids[qrow_l] : qrow_l - qshift;
+            sm.qoff[w][lane] = a.offsets[qrow_l];
         }
         __syncwarp();
         const int32_t M = rpre[R];
@@ -1882,23 +1885,50 @@ __global__ void __launch_bounds__(kExpandWarps * 32, 3) expand_records_kernel(Ex
             const int32_t wpi = warp_inclusive_scan(wp);
             if (lane < kExpandWin) sm.rrank[w][lane] = nbefore + wpi - wp - 1;
             __syncwarp();
-            const uint32_t le = (2u << lane) - 1u;  // bits 0 .. lane
-            for (int32_t cc = 0; cc < nc; ++cc) {
-                const int32_t k = wbase + (cc << 5) + lane;
-                int32_t col = 0;
-                if (k < M) {
-                    const int32_t cr = sm.rrank[w][cc] + __popc(sm.rstart[w][cc] & le);
-                    if (TCR_GUARD(cr, R)) {
-                        const int32_t j = rbeg[cr] + (k - rpre[cr]);
-                        const int32_t jl = TCR_GUARD(j, a.nr) ? __ldg(&a.rsidx[j]) : 0;
-                        col = a.ref_ids ? __ldg(&a.ref_ids[jl]) : jl - rshift;
-                    }
-                }
-                cols[(cc << 5) + lane] = col;
-            }
+            // the window's masks and candidate columns, the loads of each batch issued together so
+            // that their latencies overlap (one load waited for at a time left the warps idle)
             const int32_t nm = nc * nb;
             const uint32_t* src = masks + (int64_t)c0 * nb;
-            for (int32_t i = lane; i < nm; i += 32) mks[i] = __ldcs(&src[i]);
+            for (int32_t i0 = 0; i0 < nm; i0 += 32 * kExpandBatch) {
+                uint32_t v[kExpandBatch];
+#pragma unroll
+                for (int i = 0; i < kExpandBatch; ++i) {
+                    const int32_t ii = i0 + (i << 5) + lane;
+                    v[i] = ii < nm ? __ldcs(&src[ii]) : 0u;
+                }
+#pragma unroll
+                for (int i = 0; i < kExpandBatch; ++i) {
+                    const int32_t ii = i0 + (i << 5) + lane;
+                    if (ii < nm) mks[ii] = v[i];
+                }
+            }
+            const uint32_t le = (2u << lane) - 1u;  // bits 0 .. lane
+            for (int32_t cc0 = 0; cc0 < nc; cc0 += kExpandBatch) {
+                int32_t jl[kExpandBatch];
+                bool ok[kExpandBatch];
+#pragma unroll
+                for (int i = 0; i < kExpandBatch; ++i) {
+                    const int32_t cc = cc0 + i;
+                    const int32_t k = wbase + (cc << 5) + lane;
+                    jl[i] = 0;
+                    ok[i] = false;
+                    if (cc < nc && k < M) {
+                        const int32_t cr = sm.rrank[w][cc] + __popc(sm.rstart[w][cc] & le);
+                        if (TCR_GUARD(cr, R)) {
+                            const int32_t j = rbeg[cr] + (k - rpre[cr]);
+                            ok[i] = true;
+                            if (TCR_GUARD(j, a.nr)) jl[i] = __ldg(&a.rsidx[j]);
+                        }
+                    }
+                }
+                int32_t col[kExpandBatch];
+#pragma unroll
+                for (int i = 0; i < kExpandBatch; ++i)
+                    col[i] = !ok[i] ? 0 : (a.ref_ids ? __ldg(&a.ref_ids[jl[i]]) : jl[i] - rshift);
+#pragma unroll
+                for (int i = 0; i < kExpandBatch; ++i)
+                    if (cc0 + i < nc) cols[((cc0 + i) << 5) + lane] = col[i];
+            }
             __syncwarp();
             // the window's outputs of each query, and their exclusive prefix over the queries
             int32_t tot = 0;
@@ -2938,6 +2968,7 @@ extern "C" int tcr_search_noalloc(const tcr_search_desc* d, int64_t* offsets, in
                                   int64_t* row_entries_out, int64_t* row_out, int64_t* col_out,
                                   int64_t pair_capacity, int64_t* total_out, void* stream) {
     using namespace tcr;
+    NvtxRange nvtx_("tcr_search_noalloc");
     HostBatch b;
     int rc = batch_of_desc(d, 2, b);
     if (rc) return rc;
@@ -2947,9 +2978,9 @@ extern "C" int tcr_search_noalloc(const tcr_search_desc* d, int64_t* offsets, in
     batch_sizes(b, &s_bytes, &w_bytes);
     if (s_bytes + w_bytes > kTcrStaticScratchBytes)
         return set_error(TCR_ERR_INVALID,
-                         "tcr_search_noalloc: %lld query and %lld reference points need %lld bytes of scratch, "
-                         "more than the static %lld bytes (about 180K points); use tcr_build_structure/"
-                         "tcr_count/tcr_emit with caller-allocated buffers",
+                         "tcr_search_noalloc: %lld query and %lld reference points need %lld bytes of structure "
+                         "and scratch, more than the static %lld bytes; use tcr_build_structure/tcr_count/tcr_emit "
+                         "with caller-allocated buffers",
                          (long long)d->n_query, (long long)d->n_ref, (long long)(s_bytes + w_bytes),
                          (long long)kTcrStaticScratchBytes);
     void* base = nullptr;
@@ -2957,12 +2988,18 @@ extern "C" int tcr_search_noalloc(const tcr_search_desc* d, int64_t* offsets, in
     if (rc) return rc;
     void* structure = base;
     void* scratch = static_cast<char*>(base) + s_bytes;
+    // The rest of the array is the staging list: units whose records fit are expanded by the emit
+    // without being tested again.
+    const int64_t stage_off = align256(s_bytes + w_bytes);
+    const int64_t stage_words = std::min<int64_t>((kTcrStaticScratchBytes - stage_off) / 4, 0x7fffffff);
+    int32_t* stage = stage_words > 0 ? reinterpret_cast<int32_t*>(static_cast<char*>(base) + stage_off) : nullptr;
     // Every kernel below initialises what it reads (counters, map, sort state), so the contents a
     // previous call left in the array do not matter.
     rc = tcr_build_structure(d, structure, s_bytes, scratch, w_bytes, stream);
     if (rc) return rc;
     int64_t info[8] = {0, 0, 0, 0, 0, 0, 0, 0};
-    rc = tcr_count(d, structure, scratch, w_bytes, nullptr, 0, offsets, indptr_out, row_entries_out, info, stream);
+    rc = tcr_count(d, structure, scratch, w_bytes, stage, stage ? stage_words : 0, offsets, indptr_out,
+                   row_entries_out, info, stream);
     if (rc) return rc;
     TCR_CUDA(cudaStreamSynchronize((cudaStream_t)stream));
     if (total_out) *total_out = info[0];
@@ -2971,5 +3008,5 @@ extern "C" int tcr_search_noalloc(const tcr_search_desc* d, int64_t* offsets, in
         return set_error(TCR_ERR_INVALID, "tcr_search_noalloc: %lld pairs do not fit the %lld-entry output",
                          (long long)info[0], (long long)pair_capacity);
     if (info[0] == 0) return TCR_OK;
-    return tcr_emit(d, structure, scratch, w_bytes, nullptr, offsets, row_out, col_out, pair_capacity, stream);
+    return tcr_emit(d, structure, scratch, w_bytes, stage, offsets, row_out, col_out, pair_capacity, stream);
 }

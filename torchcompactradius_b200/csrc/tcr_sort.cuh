@@ -1,7 +1,7 @@
 // tcr_sort.cuh -- stable LSD radix sort of (key, int32 value) pairs, 32- or 64-bit keys.
 //
-// Per 8-bit digit: a tile histogram kernel, a device scan of the digit-major histogram and a
-// stable scatter.  Inside a tile the scatter ranks keys with warp match/ballot so equal digits
+// Per 8-bit digit: a tile histogram kernel, a per-digit scan of the tiles' counts and a stable
+// scatter.  Inside a tile the scatter ranks keys with warp match/ballot so equal digits
 // keep their input order; tiles are concatenated in order, so the whole sort is stable.  A pass
 // whose digit is the same for every key is skipped on the device without a host round trip:
 // digits above the highest bit in which two keys differ (from the key range the producer
@@ -19,6 +19,7 @@ constexpr int kSortThreads = 256;
 constexpr int kSortItems = 8;
 constexpr int kSortTile = kSortThreads * kSortItems;  // 2048 keys per tile
 constexpr int kBins = 256;
+static_assert(kSortThreads == kBins, "the scatter scans one digit per thread");
 
 template <typename K>
 struct SortStateT {
@@ -96,12 +97,16 @@ __global__ void __launch_bounds__(kSortThreads) radix_hist_kernel(const K* keys0
 }
 
 // Stable scatter of one tile.  Warp w owns keys [w*256, w*256+256) of the tile, processed in 8
-// rounds of 32 consecutive keys, so (warp, round, lane) order is the input order.
+// rounds of 32 consecutive keys, so (warp, round, lane) order is the input order.  The tile is
+// first ordered by digit in shared memory (stable), then written out by consecutive threads over
+// that order: the keys of one digit land in consecutive output slots, so the stores coalesce into
+// runs instead of one sector per key.
 template <typename K>
 __global__ void __launch_bounds__(kSortThreads) radix_scatter_kernel(K* keys0, K* keys1, int32_t* vals0,
                                                                      int32_t* vals1, int64_t n, int shift, int pass,
                                                                      int64_t ntiles, SortStateT<K>* st,
-                                                                     const int32_t* hist_scanned) {
+                                                                     const int32_t* hist_scanned,
+                                                                     const int32_t* digit_total) {
     const int s = st->sel[pass];
     if (!pass_runs(st, shift, pass)) {
         if (blockIdx.x == 0 && threadIdx.x == 0) st->sel[pass + 1] = s;
@@ -114,12 +119,24 @@ __global__ void __launch_bounds__(kSortThreads) radix_scatter_kernel(K* keys0, K
     int32_t* vout = s ? vals0 : vals1;
     constexpr int NW = kSortThreads / 32;
     __shared__ int32_t warp_hist[NW][kBins];
-    __shared__ int32_t tile_base[kBins];
+    __shared__ int32_t tile_base[kBins];   // first output slot of each digit of this tile
+    __shared__ int32_t digit_start[kBins + 1];  // first slot of each digit in the tile's digit order
+    __shared__ K sk[kSortTile];
+    __shared__ int32_t sv[kSortTile];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     for (int i = threadIdx.x; i < NW * kBins; i += kSortThreads) (&warp_hist[0][0])[i] = 0;
-    for (int d = threadIdx.x; d < kBins; d += kSortThreads) tile_base[d] = hist_scanned[(int64_t)d * ntiles + blockIdx.x];
+    {
+        // first slot of digit d in the output: the keys of smaller digits, then this digit's keys in
+        // earlier tiles (one digit per thread)
+        __shared__ int32_t base_sm[kSortThreads / 32 + 1];
+        int32_t total;
+        const int d = threadIdx.x;
+        const int32_t db = block_exclusive_scan<int32_t, kSortThreads>(digit_total[d], base_sm, total);
+        tile_base[d] = db + hist_scanned[(int64_t)d * ntiles + blockIdx.x];
+    }
     __syncthreads();
-    const int64_t base = (int64_t)blockIdx.x * kSortTile + (int64_t)warp * (kSortItems * 32);
+    const int64_t tile0 = (int64_t)blockIdx.x * kSortTile;
+    const int64_t base = tile0 + (int64_t)warp * (kSortItems * 32);
     const unsigned lt = (1u << lane) - 1u;
     K key[kSortItems];
     int32_t val[kSortItems];
@@ -130,6 +147,11 @@ __global__ void __launch_bounds__(kSortThreads) radix_scatter_kernel(K* keys0, K
         bool valid = i < n;
         key[r] = valid ? kin[i] : (K)0;
         val[r] = valid ? vin[i] : 0;
+    }
+#pragma unroll
+    for (int r = 0; r < kSortItems; ++r) {
+        int64_t i = base + r * 32 + lane;
+        bool valid = i < n;
         uint32_t dig = valid ? (uint32_t)((key[r] >> shift) & 0xff) : 0x100u;  // invalid lanes: own group
         unsigned peers = __match_any_sync(0xffffffffu, dig);
         int before = __popc(peers & lt);
@@ -140,15 +162,26 @@ __global__ void __launch_bounds__(kSortThreads) radix_scatter_kernel(K* keys0, K
         rank[r] = run + before;
     }
     __syncthreads();
-    // exclusive scan over warps for each digit
-    for (int d = threadIdx.x; d < kBins; d += kSortThreads) {
+    // per digit: exclusive scan over warps; the digit's total, scanned over digits, is its start
+    // in the tile's digit order
+    int32_t dtot = 0;
+    const int d0 = threadIdx.x;  // kSortThreads == kBins: one digit per thread
+    {
         int acc = 0;
 #pragma unroll
         for (int w = 0; w < NW; ++w) {
-            int c = warp_hist[w][d];
-            warp_hist[w][d] = acc;
+            int c = warp_hist[w][d0];
+            warp_hist[w][d0] = acc;
             acc += c;
         }
+        dtot = acc;
+    }
+    {
+        __shared__ int32_t scan_sm[kSortThreads / 32 + 1];
+        int32_t total;
+        const int32_t ex = block_exclusive_scan<int32_t, kSortThreads>(dtot, scan_sm, total);
+        digit_start[d0] = ex;
+        if (d0 == 0) digit_start[kBins] = total;
     }
     __syncthreads();
 #pragma unroll
@@ -156,68 +189,51 @@ __global__ void __launch_bounds__(kSortThreads) radix_scatter_kernel(K* keys0, K
         int64_t i = base + r * 32 + lane;
         if (i < n) {
             int dig = (int)((key[r] >> shift) & 0xff);
-            int64_t pos = (int64_t)tile_base[dig] + warp_hist[warp][dig] + rank[r];
-            kout[pos] = key[r];
-            vout[pos] = val[r];
+            const int loc = digit_start[dig] + warp_hist[warp][dig] + rank[r];
+            sk[loc] = key[r];
+            sv[loc] = val[r];
         }
+    }
+    __syncthreads();
+    const int tn = digit_start[kBins];
+    for (int i = threadIdx.x; i < tn; i += kSortThreads) {
+        const K k = sk[i];
+        const int dig = (int)((k >> shift) & 0xff);
+        const int64_t pos = (int64_t)tile_base[dig] + (i - digit_start[dig]);
+        kout[pos] = k;
+        vout[pos] = sv[i];
     }
     if (blockIdx.x == 0 && threadIdx.x == 0) st->sel[pass + 1] = s ^ 1;
 }
 
-// Scan kernels for the histogram, gated on the pass running.
+// Per digit (one block each): exclusive scan of the digit's tile counts in place, and the
+// digit's total; the scatter adds the totals of the smaller digits.  Gated on the pass running.
 template <typename K>
-__global__ void __launch_bounds__(kScanThreads) hist_scan_reduce(const int32_t* h, int64_t n, int32_t* tile_sums,
+__global__ void __launch_bounds__(kScanThreads) hist_scan_digits(int32_t* hist, int64_t ntiles, int32_t* digit_total,
                                                                  const SortStateT<K>* st, int shift, int pass) {
     if (!pass_runs(st, shift, pass)) return;
     __shared__ int32_t sm[kScanThreads / 32 + 1];
-    const int64_t base = (int64_t)blockIdx.x * kScanTile;
-    int32_t s = 0;
-#pragma unroll
-    for (int k = 0; k < kScanItems; ++k) {
-        int64_t i = base + (int64_t)k * kScanThreads + threadIdx.x;
-        if (i < n) s += h[i];
-    }
-    int32_t total;
-    block_exclusive_scan<int32_t, kScanThreads>(s, sm, total);
-    if (threadIdx.x == 0) tile_sums[blockIdx.x] = total;
-}
-template <typename K>
-__global__ void __launch_bounds__(1024) hist_scan_tiles(int32_t* tile_sums, int64_t ntiles, const SortStateT<K>* st,
-                                                        int shift, int pass) {
-    if (!pass_runs(st, shift, pass)) return;
-    __shared__ int32_t sm[1024 / 32 + 1];
+    int32_t* row = hist + (int64_t)blockIdx.x * ntiles;
     int32_t carry = 0;
-    for (int64_t b = 0; b < ntiles; b += 1024) {
-        int64_t i = b + threadIdx.x;
-        int32_t v = i < ntiles ? tile_sums[i] : 0;
+    for (int64_t b = 0; b < ntiles; b += kScanTile) {
+        const int64_t i0 = b + (int64_t)threadIdx.x * kScanItems;
+        int32_t v[kScanItems];
+        int32_t sum = 0;
+#pragma unroll
+        for (int k = 0; k < kScanItems; ++k) {
+            v[k] = i0 + k < ntiles ? row[i0 + k] : 0;
+            sum += v[k];
+        }
         int32_t total;
-        int32_t ex = block_exclusive_scan<int32_t, 1024>(v, sm, total);
-        if (i < ntiles) tile_sums[i] = ex + carry;
+        int32_t ex = block_exclusive_scan<int32_t, kScanThreads>(sum, sm, total) + carry;
+#pragma unroll
+        for (int k = 0; k < kScanItems; ++k) {
+            if (i0 + k < ntiles) row[i0 + k] = ex;
+            ex += v[k];
+        }
         carry += total;
     }
-}
-template <typename K>
-__global__ void __launch_bounds__(kScanThreads) hist_scan_apply(int32_t* h, int64_t n, const int32_t* tile_sums,
-                                                                const SortStateT<K>* st, int shift, int pass) {
-    if (!pass_runs(st, shift, pass)) return;
-    __shared__ int32_t sm[kScanThreads / 32 + 1];
-    const int64_t base = (int64_t)blockIdx.x * kScanTile + (int64_t)threadIdx.x * kScanItems;
-    int32_t v[kScanItems];
-    int32_t s = 0;
-#pragma unroll
-    for (int k = 0; k < kScanItems; ++k) {
-        int64_t i = base + k;
-        v[k] = i < n ? h[i] : 0;
-        s += v[k];
-    }
-    int32_t total;
-    int32_t ex = block_exclusive_scan<int32_t, kScanThreads>(s, sm, total) + tile_sums[blockIdx.x];
-#pragma unroll
-    for (int k = 0; k < kScanItems; ++k) {
-        int64_t i = base + k;
-        if (i < n) h[i] = ex;
-        ex += v[k];
-    }
+    if (threadIdx.x == 0) digit_total[blockIdx.x] = carry;
 }
 
 template <typename K>
@@ -225,7 +241,7 @@ struct SortWorkspaceT {
     K* keys[2];
     int32_t* vals[2];
     int32_t* hist;          // kBins * ntiles
-    int32_t* tile_sums;     // scan_tiles(kBins * ntiles)
+    int32_t* tile_sums;     // kBins digit totals of the running pass
     SortStateT<K>* state;   // device
 };
 
@@ -239,18 +255,14 @@ template <typename K>
 inline cudaError_t radix_sort_pairs(const SortWorkspaceT<K>& w, int64_t n, cudaStream_t st) {
     if (n <= 0) return cudaSuccess;
     const int64_t nt = sort_tiles(n);
-    const int64_t nh = (int64_t)kBins * nt;
-    const int64_t nht = scan_tiles(nh);
     for (int p = 0; p < key_passes<K>(); ++p) {
         const int shift = 8 * p;
         radix_hist_kernel<K><<<(unsigned)nt, kSortThreads, 0, st>>>(w.keys[0], w.keys[1], n, shift, p, nt, w.state,
                                                                     w.hist);
-        hist_scan_reduce<K><<<(unsigned)nht, kScanThreads, 0, st>>>(w.hist, nh, w.tile_sums, w.state, shift, p);
-        hist_scan_tiles<K><<<1, 1024, 0, st>>>(w.tile_sums, nht, w.state, shift, p);
-        hist_scan_apply<K><<<(unsigned)nht, kScanThreads, 0, st>>>(w.hist, nh, w.tile_sums, w.state, shift, p);
+        hist_scan_digits<K><<<kBins, kScanThreads, 0, st>>>(w.hist, nt, w.tile_sums, w.state, shift, p);
         radix_scatter_kernel<K><<<(unsigned)nt, kSortThreads, 0, st>>>(w.keys[0], w.keys[1], w.vals[0], w.vals[1], n,
-                                                                      shift, p, nt, w.state, w.hist);
-        note_launches(5);
+                                                                      shift, p, nt, w.state, w.hist, w.tile_sums);
+        note_launches(3);
     }
     return cudaGetLastError();
 }

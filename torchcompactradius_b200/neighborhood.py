@@ -102,7 +102,12 @@ def radiusSearch(queryPointCloud: PointCloud, referencePointCloud: Optional[Poin
             out = multilevel_search(xq, hq, xr, hr, lo, hi, mask, mode, format)
             ds = None  # neighborhood.py:260-263: the multi-level path returns no reusable structure
         else:
-            out, ds = compact_search(xq, hq, xr, hr, lo, hi, mask, mode, hashMapLength, format, same,
+            # One support h for every point: each mode's threshold is h itself (symmetric:
+            # fl(h/2 + h/2) = h, superSymmetric: max(h, h) = h), so the fixed-radius search runs the
+            # gather walk, whose test is d^2 - h^2 with the query's share precomputed -- the same
+            # pairs with fewer operations per test than the two-support modes.
+            walk_mode = "gather" if supportOverride is not None else mode
+            out, ds = compact_search(xq, hq, xr, hr, lo, hi, mask, walk_mode, hashMapLength, format, same,
                                      return_structure=returnStructure, ref_pos_user=rpos,
                                      ref_sup_user=referencePointCloud.supports, fixed_support=supportOverride)
         if in_device.type != "cuda":

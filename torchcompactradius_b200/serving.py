@@ -10,11 +10,18 @@ displacement to its points) and asks for its adjacency.  The server
   (``tcr_batch_desc.ref_lin_hint``) instead of rebuilding from scratch;
 * admits pending requests in arrival order while their estimated device memory fits the HBM
   budget and their scene has no request in flight (a scene's requests run in order);
-* runs each admitted group as one batched search (``tcr_batch_*``: one set of launches for all
-  its scenes) on one of ``slots`` worker streams, so a group admitted while another is still on
-  the GPU runs beside it: requests that arrive during a search are admitted as soon as a slot and
-  memory free up (continuous batching), not after the queue drains.  The host work of a group is
-  a fixed number of vectorised operations over the arena, whatever the number of scenes in it.
+* admits pending requests in arrival order while the device bytes their searches need -- the
+  structure and scratch sizes ``tcr_batch_sizes`` reports for the scene, its staging list and its
+  output at the pair count of its last search -- fit the HBM budget, and their scene has no
+  request waiting to be enqueued (a scene's requests run in order);
+* enqueues each admitted group as one batched search (``tcr_batch_*``: one set of launches for
+  all its scenes) on one of ``slots`` worker streams and does not wait for it: the worker goes
+  straight back to admission, so groups are enqueued while earlier ones run (continuous
+  batching).  A completion thread waits for each group's event, slices the per-scene results with
+  offsets the device copied to pinned memory, and completes the requests; nothing on the worker
+  reads device memory.  A scene's next request waits on the stream for its previous search's
+  arena update (an event), not on the host.  The host work of a group is a fixed number of
+  vectorised operations over the arena, whatever the number of scenes in it.
 
 Results are in the scene's user numbering (``SparseCOO`` rows and columns are the indices the
 scene was given with; rows come grouped in the scene's cell order), ready for use on the default
@@ -31,15 +38,19 @@ from typing import Dict, List, Optional
 import numpy as np
 import torch
 
+import queue
+
+from . import _lib
 from . import context as _context
-from .batched import BatchBuffers, cloud_table, run_batch
+from .batched import batch_desc, cloud_table, enqueue_batch
 from .search import _as_f32, _domain_host, _require_cuda
 from .util import DomainDescription, SparseCOO
 
-# Device bytes one search needs per point and per expected pair (structure, scratch with the
-# incremental re-sort, staging list and int64 COO output), for admission.
-BYTES_PER_POINT = 420
-BYTES_PER_PAIR = 22
+# Device bytes of a search beyond the library's structure and scratch: per point the arena
+# indices of the group (int64 slot, shift), the user ids, the cell hint and the new cell order
+# (int32 each); per staging word 4 bytes; per pair two int64 (COO row and column).
+WORK_BYTES_PER_POINT = 32
+STAGE_WORDS_PER_POINT = 64
 
 
 class Scene:
@@ -58,9 +69,35 @@ class Scene:
         self.lo, self.hi, self.mask = _domain_host(domain, self.dim)
         self.hashMapLength = int(hashMapLength)
         self.expected_neighbours = float(expected_neighbours)
+        self.pairs = self.n * self.expected_neighbours  # pair count of the last search (estimate before one)
+        self._lib_bytes = None
+
+    def library_bytes(self) -> int:
+        """Structure + scratch bytes of this scene's search with the incremental re-sort, as
+        ``tcr_batch_sizes`` reports them (host-only; no device work)."""
+        if self._lib_bytes is None:
+            t = cloud_table(1)
+            t["dim"][0] = self.dim
+            t["n_query"][0] = t["n_ref"][0] = self.n
+            hint = _FakePtr()  # a hint enlarges the scratch; sizing reads no pointer
+            b = batch_desc(t, "gather", True, lin_hint=hint)
+            s, w = _lib.batch_sizes(b)
+            self._lib_bytes = int(s + w)
+        return self._lib_bytes
 
     def bytes_estimate(self) -> int:
-        return int(self.n * (BYTES_PER_POINT + BYTES_PER_PAIR * self.expected_neighbours))
+        """Device bytes one search of this scene needs: library structure and scratch, work arrays,
+        staging list and COO output at the last search's pair count (plus 10%)."""
+        return int(self.library_bytes() + self.n * (WORK_BYTES_PER_POINT + 4 * STAGE_WORDS_PER_POINT)
+                   + 16 * 1.1 * self.pairs + 65536)
+
+
+class _FakePtr:
+    """Stands in for a device tensor in a descriptor that is only sized (data_ptr is never read)."""
+
+    @staticmethod
+    def data_ptr():
+        return 256
 
 
 class Request:
@@ -133,6 +170,9 @@ class SearchServer:
         self._cv = threading.Condition()
         self._running = False
         self._threads = []
+        self._completer = None
+        self._done = queue.Queue()
+        self._last_event = {}  # scene -> event after the arena update of its last enqueued search
         self.batches = 0
         self.batched_requests = 0
         self.tuning = (0, 0)  # (queries per unit, walk blocks per SM) of the workers' searches; 0: default
@@ -180,6 +220,9 @@ class SearchServer:
         """A scene's current positions in user order (call while it has no request in flight)."""
         if not self._where:
             return self.scenes[scene].positions
+        ev = self._last_event.get(scene)
+        if ev is not None:
+            ev.synchronize()
         dim, j = self._where[scene]
         ar = self._arenas[dim]
         a, b = int(ar.base[j]), int(ar.base[j + 1])
@@ -193,6 +236,8 @@ class SearchServer:
                 return self
             self._build_arenas()
             self._running = True
+        self._completer = threading.Thread(target=self._complete, daemon=True)
+        self._completer.start()
         for slot in range(self.slots):
             t = threading.Thread(target=self._worker, args=(slot,), daemon=True)
             t.start()
@@ -206,6 +251,10 @@ class SearchServer:
         for t in self._threads:
             t.join()
         self._threads = []
+        if self._completer is not None:
+            self._done.put(None)  # after every enqueued group
+            self._completer.join()
+            self._completer = None
 
     def __enter__(self):
         return self.start()
@@ -235,6 +284,7 @@ class SearchServer:
                 keep.append(r)
                 blocked.add(r.scene)  # later requests of the scene wait behind this one
                 continue
+            r._bytes = need
             batch.append(r)
             scenes.add(r.scene)
             self._in_use += need
@@ -243,18 +293,26 @@ class SearchServer:
         self._busy |= scenes
         return batch
 
+    def _fail(self, reqs, ex):
+        with self._cv:
+            for r in reqs:
+                self._in_use -= getattr(r, "_bytes", 0)
+                r.error = ex
+                r.finish = time.perf_counter()
+            self._cv.notify_all()
+        for r in reqs:
+            r._done.set()
+
     def _worker(self, slot):
         try:
             torch.cuda.set_device(self.device)
             stream = torch.cuda.Stream(self.device)
-            bufs = {d: BatchBuffers(self.device) for d in (1, 2, 3)}
-            ctx = _context.SearchContext()  # this worker's size estimates
+            ctx = _context.SearchContext()  # this worker's staging estimate
         except BaseException as ex:  # no worker: fail what waits instead of leaving it hanging
             with self._cv:
-                while self._pending:
-                    r = self._pending.popleft()
-                    r.error = ex
-                    r._done.set()
+                reqs = list(self._pending)
+                self._pending.clear()
+            self._fail(reqs, ex)
             return
         while True:
             with self._cv:
@@ -266,40 +324,33 @@ class SearchServer:
                     self._cv.wait(0.05)
                 if not batch:
                     return
+            launched = []
             try:
                 ctx.unit_queries, ctx.walk_blocks_per_sm = self.tuning
                 with _context.use(ctx):
                     for dim in (1, 2, 3):
                         group = [r for r in batch if self.scenes[r.scene].dim == dim]
                         if group:
-                            self._run(group, dim, stream, bufs[dim])
+                            self._done.put(self._launch(group, dim, stream, ctx))
+                            launched += group
             except BaseException as ex:  # the requests report it; the server keeps serving
-                for r in batch:
-                    r.error = ex
+                self._fail([r for r in batch if r not in launched], ex)
             finally:
-                now = time.perf_counter()
+                # the scenes' next requests may be enqueued now: their device work waits for this
+                # group's arena update on the stream (_last_event), not on the host
                 with self._cv:
                     for r in batch:
                         self._busy.discard(r.scene)
-                        self._in_use -= self.scenes[r.scene].bytes_estimate()
-                        r.finish = now
-                    self.batches += 1
-                    self.batched_requests += len(batch)
                     self._cv.notify_all()
-                for r in batch:
-                    if r.on_done is not None:
-                        try:
-                            r.on_done(r)
-                        except BaseException as ex:
-                            r.error = ex
-                    r._done.set()
 
-    def _run(self, group, dim, stream, bufs):
-        """One batched search over the scenes of `group` (all of dimension dim)."""
+    def _launch(self, group, dim, stream, ctx):
+        """Enqueues one batched search over the scenes of `group` (all of dimension dim) and the
+        arena update after it; returns what the completion thread needs."""
         dev = self.device
         ar = self._arenas[dim]
+        now = time.perf_counter()
         for r in group:
-            r.admitted = time.perf_counter()
+            r.admitted = now
         js = np.array([self._where[r.scene][1] for r in group], dtype=np.int64)
         n = ar.base[js + 1] - ar.base[js]
         bb = np.zeros(len(js) + 1, dtype=np.int64)  # batch bases
@@ -308,15 +359,25 @@ class SearchServer:
         table = np.ascontiguousarray(self._tables[dim][js])
         user = torch.cuda.default_stream(dev)
         stream.wait_stream(user)  # explicit displacements made on the caller's stream are ready
+        for r in group:
+            ev = self._last_event.get(r.scene)
+            if ev is not None:
+                stream.wait_event(ev)  # the scene's previous search has updated its arena segment
+        jit = np.array([r.jitter or 0.0 for r in group], dtype=np.float32)
+        # the group's per-scene values in one pinned block, copied without waiting for the stream
+        # (a copy from pageable memory would wait for the stream's earlier groups)
+        host = torch.from_numpy(np.concatenate([n, ar.base[js] - bb[:-1], bb, jit.view(np.int32).astype(np.int64)]))
+        host = host.pin_memory()
+        G = len(group)
         with torch.cuda.stream(stream):
+            vals = host.to(dev, non_blocking=True)
+            ns, base_shift, bb_dev = vals[:G], vals[G:2 * G], vals[2 * G:3 * G + 1]
             # arena index of every batch slot: arena base of its scene + its offset in the scene
             # (expanded from per-scene values on the device)
-            ns = torch.as_tensor(n, device=dev)
-            shift = torch.repeat_interleave(torch.as_tensor(ar.base[js] - bb[:-1], device=dev), ns, output_size=T)
+            shift = torch.repeat_interleave(base_shift, ns, output_size=T)
             dst = torch.arange(T, device=dev) + shift
-            jit = np.array([r.jitter or 0.0 for r in group], dtype=np.float32)
             if jit.any():
-                sig = torch.repeat_interleave(torch.as_tensor(jit, device=dev), ns, output_size=T)
+                sig = torch.repeat_interleave(vals[3 * G + 1:].to(torch.int32).view(torch.float32), ns, output_size=T)
                 ar.pos.index_add_(0, dst, torch.randn(T, dim, device=dev) * sig[:, None])
             for k, r in enumerate(group):
                 if r.displacement is not None:
@@ -325,24 +386,65 @@ class SearchServer:
                     ar.pos[a:b] += d.index_select(0, ar.ids[a:b].long())
             ids = ar.ids.index_select(0, dst)
             hint = ar.lin.index_select(0, dst)
-            lin_out = bufs.get("lin_out", T, torch.int32)
-            order_out = bufs.get("order_out", T, torch.int32)
-            out = run_batch(table, self.mode, True, "coo", dev, local_index=False, query_ids=ids, ref_ids=ids,
-                            buffers=bufs, stream=stream, lin_hint=hint, lin_out=lin_out, order_out=order_out,
-                            fresh_outputs=True)
-            for t in (out["row"], out["col"]):
-                t.record_stream(user)  # results are read on the default stream
+            lin_out = torch.empty(T, dtype=torch.int32, device=dev)
+            order_out = torch.empty(T, dtype=torch.int32, device=dev)
+            cap = int(1.1 * sum(self.scenes[r.scene].pairs for r in group)) + 4096
+            stage_cap = int(ctx.batch_stage_per_query * 1.1 * T) + 65536
+            pend = enqueue_batch(table, self.mode, True, "coo", dev, stream, cap, stage_cap, local_index=False,
+                                 query_ids=ids, ref_ids=ids, lin_hint=hint, lin_out=lin_out, order_out=order_out,
+                                 base_index=bb_dev)
             # keep every scene in its new cell order (the next search re-sorts incrementally)
             src = order_out.long() + shift
             ar.pos.index_copy_(0, dst, ar.pos.index_select(0, src))
             ar.sup.index_copy_(0, dst, ar.sup.index_select(0, src))
             ar.ids.index_copy_(0, dst, ar.ids.index_select(0, src))
             ar.lin.index_copy_(0, dst, lin_out)
-            offs = out["offsets"].index_select(0, torch.as_tensor(bb, device=dev)).cpu().tolist()
-            for k, r in enumerate(group):
-                m = int(n[k])
-                r.result = SparseCOO(out["row"][offs[k]:offs[k + 1]], out["col"][offs[k]:offs[k + 1]], m, m)
-            stream.synchronize()
+            ev = torch.cuda.Event()
+            ev.record(stream)
+        for r in group:
+            self._last_event[r.scene] = ev
+        pend.keep = (host, vals, shift, dst, ids, hint, lin_out, order_out, src)
+        return group, n, pend, ctx
+
+    def _complete(self):
+        """Waits for each enqueued group in order and completes its requests."""
+        user = torch.cuda.default_stream(self.device)
+        while True:
+            item = self._done.get()
+            if item is None:
+                return
+            group, n, pend, ctx = item
+            try:
+                total = pend.finish()
+                offs = pend.offsets_host.tolist()
+                for t in (pend.row, pend.col):
+                    t.record_stream(user)  # results are read on the default stream
+                for k, r in enumerate(group):
+                    m = int(n[k])
+                    a, b = offs[k], offs[k + 1]
+                    r.result = SparseCOO(pend.row[a:b], pend.col[a:b], m, m)
+                    self.scenes[r.scene].pairs = b - a
+                if len(n):
+                    ctx.batch_stage_per_query = max(int(pend.info[4]) / max(int(n.sum()), 1), 1.0)
+                del total
+            except BaseException as ex:  # the requests report it; the server keeps serving
+                for r in group:
+                    r.error = ex
+            now = time.perf_counter()
+            with self._cv:
+                for r in group:
+                    self._in_use -= getattr(r, "_bytes", 0)
+                    r.finish = now
+                self.batches += 1
+                self.batched_requests += len(group)
+                self._cv.notify_all()
+            for r in group:
+                if r.on_done is not None:
+                    try:
+                        r.on_done(r)
+                    except BaseException as ex:
+                        r.error = ex
+                r._done.set()
 
     # -- convenience ----------------------------------------------------------------------
     def search(self, scene: int, displacement: Optional[torch.Tensor] = None, timeout=None,
