@@ -887,8 +887,16 @@ def run_b200(args):
     # the walks' run-time parameters, picked on this workload (no result depends on them)
     tuner = Autotuner(reps=3)
     tuned = tuner.tune(lambda: device_step(), key="headline")
-    tuning = {"chosen": {"queries_per_unit": tuned[0], "walk_blocks_per_sm": tuned[1]},
-              "ms_per_search": {f"{c[0]}q/{c[1]}b": round(v, 4) for c, v in tuner.timings["headline"].items()}}
+    # the cell-size multiplier, on the eager single search it applies to (kept only if it finds the
+    # same pairs); the graph-replayed headline keeps the reference's cell
+    from torchcompactradius_b200 import context as tcr_context
+    scale = tuner.tune_cell_scale(
+        lambda: tcr.radiusSearch(tcr.PointCloud(pos_d, sup_d), None, mode="symmetric", domain=dom,
+                                 algorithm="compact", format="csr"), key="headline")
+    tuning = {"chosen": {"queries_per_unit": tuned[0], "walk_blocks_per_sm": tuned[1], "cell_scale": scale},
+              "ms_per_search": {f"{c[0]}q/{c[1]}b": round(v, 4) for c, v in tuner.timings["headline"].items()},
+              "eager_ms_per_cell_scale": {str(m): round(v, 4) for m, v in tuner.scale_timings["headline"].items()}}
+    tcr_context.current().cell_scale = 1.0
 
     # ---- phases of the eager path (public API) ------------------------------------------------
     _lib.check(lib.tcr_profile_kernels(1), "tcr_profile_kernels")

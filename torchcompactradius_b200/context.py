@@ -3,8 +3,11 @@
 A ``SearchContext`` holds what one caller's searches share and no other caller sees:
 
 * the tuning -- queries per work unit of the walks (32, 16 or 8) and resident walk blocks per SM
-  (0 keeps the engine's default).  Neither changes a result; both travel to the engine in each
-  call's descriptor (``tcr_search_desc`` / ``tcr_batch_desc``), so the engine keeps no tuning state;
+  (0 keeps the engine's default), which travel to the engine in each call's descriptor
+  (``tcr_search_desc`` / ``tcr_batch_desc``), so the engine keeps no tuning state; and the cell-size
+  multiplier of single searches (1: the reference's cell; m > 1: cells m times the largest
+  threshold on the exact clamped grid -- the same pair set whenever every point lies inside the
+  domain on its non-periodic dimensions).  None of them changes such a result;
 * the output and staging-list sizes per query learnt from the previous search, which size the
   buffers of the next one (a short estimate costs a second emit, never a wrong result).
 
@@ -22,6 +25,7 @@ from dataclasses import dataclass
 class SearchContext:
     unit_queries: int = 0        # queries per work unit: 32, 16 or 8 (0: default 32)
     walk_blocks_per_sm: int = 0  # resident walk blocks per SM, 1..64 (0: default 12)
+    cell_scale: float = 1.0      # cell-size multiplier of single searches (1: the reference's cell)
     pairs_per_query: float = 64.0        # single searches: output pairs per query last time
     stage_per_query: float = 64.0        # single searches: staging words per query last time
     batch_pairs_per_query: float = 64.0  # batched searches

@@ -1289,15 +1289,26 @@ __device__ __forceinline__ float pair_residual(const WrapCtx& wc, const float4& 
 }
 
 // Warp-wide 32 x 32 bit transpose: lane j holds row j (bit k = entry (j, k)); lane k receives
-// column k (bit j = entry (j, k)).  Five butterfly stages swap ever smaller off-diagonal blocks.
+// column k (bit j = entry (j, k)).  Five butterfly stages swap ever smaller off-diagonal blocks
+// with the partner lane (lane ^ s): the 16- and 8-bit stages are one byte permutation of the own
+// and the partner's row each; in the 4-, 2- and 1-bit stages a lane keeps its own bits under a
+// lane-dependent mask and takes the partner's row rotated into place (right by s in the upper
+// lane of a pair, left by s in the lower one) under the complement.  The per-lane selectors,
+// masks and rotations depend on the lane only, so a loop over chunks computes them once.
 __device__ __forceinline__ uint32_t warp_transpose32(uint32_t x, int lane) {
-#pragma unroll
-    for (int s = 16; s >= 1; s >>= 1) {
-        const uint32_t m = s == 16 ? 0x0000ffffu : (s == 8 ? 0x00ff00ffu : (s == 4 ? 0x0f0f0f0fu
-                                                                                 : (s == 2 ? 0x33333333u : 0x55555555u)));
-        const uint32_t y = __shfl_xor_sync(0xffffffffu, x, s);
-        x = (lane & s) ? ((x & ~m) | ((y & ~m) >> s)) : ((x & m) | ((y & m) << s));
-    }
+    const uint32_t sel16 = (lane & 16) ? 0x3276u : 0x5410u;
+    const uint32_t sel8 = (lane & 8) ? 0x3715u : 0x6240u;
+    const uint32_t keep4 = (lane & 4) ? 0xf0f0f0f0u : 0x0f0f0f0fu, rot4 = (lane & 4) ? 4u : 28u;
+    const uint32_t keep2 = (lane & 2) ? 0xccccccccu : 0x33333333u, rot2 = (lane & 2) ? 2u : 30u;
+    const uint32_t keep1 = (lane & 1) ? 0xaaaaaaaau : 0x55555555u, rot1 = (lane & 1) ? 1u : 31u;
+    x = __byte_perm(x, __shfl_xor_sync(0xffffffffu, x, 16), sel16);
+    x = __byte_perm(x, __shfl_xor_sync(0xffffffffu, x, 8), sel8);
+    uint32_t y = __shfl_xor_sync(0xffffffffu, x, 4);
+    x = (x & keep4) | (__funnelshift_r(y, y, rot4) & ~keep4);
+    y = __shfl_xor_sync(0xffffffffu, x, 2);
+    x = (x & keep2) | (__funnelshift_r(y, y, rot2) & ~keep2);
+    y = __shfl_xor_sync(0xffffffffu, x, 1);
+    x = (x & keep1) | (__funnelshift_r(y, y, rot1) & ~keep1);
     return x;
 }
 
@@ -1422,6 +1433,14 @@ __device__ __forceinline__ void count_unit(const WalkArgs& a, WalkSmem& sm, int3
     const int32_t t0 = a.unit_t0[unit];
     const int32_t nb = min(*a.unit_cap, a.group_start[grp + 1] - t0);
     const int32_t gc[3] = {a.group_coords[3 * grp], a.group_coords[3 * grp + 1], a.group_coords[3 * grp + 2]};
+    // the unit's queries, loaded before the stencil look-ups so that both latencies overlap
+    const bool qlane = lane < nb && TCR_IN(t0 + lane, a.nq_total);
+    float4 qv = nan4;
+    int32_t qorig = 0;
+    if (qlane) {
+        qv = a.qsorted[t0 + lane];
+        qorig = a.qsidx[t0 + lane];
+    }
     int32_t beg = 0, cnt = 0;
     if (lane < S) stencil_lookup(a, u, gc, lane, beg, cnt);
     const bool shift_mode = PERIODIC && u.shift_ok;
@@ -1462,14 +1481,10 @@ __device__ __forceinline__ void count_unit(const WalkArgs& a, WalkSmem& sm, int3
         sm.shift[w][2][rid] = sh[2];
     }
     if (lane == 0) sm.run_pre[w][R] = M;
-    // the unit's queries
+    // the unit's queries: a query whose own cell differs from the group's leaves for the serial path
     bool active = false;
-    int32_t qorig = 0;
-    float4 qv = nan4;
-    if (lane < nb && TCR_IN(t0 + lane, a.nq_total)) {
+    if (qlane) {
         const int32_t t = t0 + lane;
-        qv = a.qsorted[t];
-        qorig = a.qsidx[t];
         active = TCR_IN(qorig, a.nq_total);
         if (active && (!a.no_stray_check || u.out_of_grid)) {
             int32_t qc[3];
@@ -1638,10 +1653,22 @@ __global__ void __launch_bounds__(kWalkWarps * 32, PERIODIC ? kWalkMinBlocksPeri
     const int32_t nunits = *a.num_units;
     int32_t* counter = &a.work[a.class_filter >= 0 ? 2 + a.class_filter : 0];
     int cur = -1;
+    const bool filter = a.class_filter >= 0;
+    int32_t claim = 0;
+    if (lane == 0) claim = atomicAdd(counter, filter ? 32 : 1);
     for (;;) {
-        int32_t base;
-        uint32_t todo = next_units(a, counter, nullptr, nunits, lane, base);
+        const int32_t base = __shfl_sync(0xffffffffu, claim, 0);
         if (base >= nunits) break;
+        uint32_t todo = 1u;
+        if (filter) {  // a chunk of 32 consecutive units; the units of other classes are dropped
+            bool mine = false;
+            if (base + lane < nunits) mine = cloud_class(a.table[a.group_cloud[a.unit_group[base + lane]]]) ==
+                                             a.class_filter;
+            todo = __ballot_sync(0xffffffffu, mine);
+        }
+        // the next claim is issued before this one's units run and read after them, so the
+        // atomic's latency overlaps their work
+        if (lane == 0) claim = atomicAdd(counter, filter ? 32 : 1);
         while (todo) {
             const int32_t unit = base + (__ffs(todo) - 1);
             todo &= todo - 1;

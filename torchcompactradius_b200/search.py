@@ -239,6 +239,26 @@ def _check_info(info):
                          "domain extent, or a support/domain value is not finite)")
 
 
+def _scaled_cells(desc, scale, mode, hq, hr, lo, hi, mask, dim):
+    """Cells `scale` times the largest threshold a pair can have (on periodic dimensions a whole
+    number of cells spans the domain), searched on the clamped grid, which finds exactly the pairs
+    with dist < thr for any cell at least that large.  The largest support is read from the device
+    (one synchronisation)."""
+    if scale < 1.0:
+        raise ValueError("the cell-size multiplier must be >= 1")
+    from .multilevel import GROW, cell_sizes
+    parts = [t for t, use in ((hq, mode != "scatter"), (hr, mode != "gather")) if use and t is not None and t.numel()]
+    if not parts:
+        return
+    hmax = float(torch.stack([t.max() for t in parts]).max())
+    if not (hmax > 0 and hmax < float("inf")):
+        return
+    cells = cell_sizes(scale * hmax * GROW, lo, hi, mask, dim)
+    for d in range(3):
+        desc.hcell[d] = cells[d] if d < dim else 1.0
+    desc.clamped_grid = 1
+
+
 def compact_search(xq, hq, xr, hr, domain_lo, domain_hi, mask, mode, L, fmt, self_search, return_structure=False,
                    structure: Optional[CompactHashMap] = None, ref_pos_user=None, ref_sup_user=None,
                    fixed_support=None, events=None):
@@ -255,6 +275,9 @@ def compact_search(xq, hq, xr, hr, domain_lo, domain_hi, mask, mode, L, fmt, sel
     stream = torch.cuda.current_stream(device)
     sptr = ctypes.c_void_p(stream.cuda_stream)
     desc = make_desc(dim, mode, mask, domain_lo, domain_hi, L, xq, hq, xr, hr, self_search)
+    scale = float(_context.current().cell_scale)
+    if scale != 1.0 and structure is None and not return_structure:
+        _scaled_cells(desc, scale, mode, hq, hr, domain_lo, domain_hi, mask, dim)
     s_bytes, w_bytes = _lib.search_sizes(nq, nr, dim)
     scratch = torch.empty(w_bytes, dtype=torch.uint8, device=device)
     def mark(name, end=False):
