@@ -1242,8 +1242,21 @@ struct WalkSmem {
     int32_t run_beg[kWalkWarps][32];
     int32_t run_pre[kWalkWarps][33];
     float shift[kWalkWarps][3][32];  // per run: +-ext on the dimensions its cells lie across a seam
+    float4 ring[kWalkWarps][3][32];  // candidate chunks in flight (cp.async), one slot per lane
     UnitCtx u[kWalkWarps];
 };
+
+// cp.async of 16 bytes from global to shared memory, its commit and wait (the copies of one
+// thread land in program order of their groups; a thread reads back only what it copied itself).
+__device__ __forceinline__ void cp_async16(void* smem, const void* gmem) {
+    const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(s), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() {
+    asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory");
+}
 
 // Candidate k of the unit (prefix pre[0..S]): returns its sorted index.
 __device__ __forceinline__ int32_t cand_index(const int32_t* pre, const int32_t* beg, int S, int32_t k) {
@@ -1559,11 +1572,41 @@ __device__ __forceinline__ void count_unit(const WalkArgs& a, WalkSmem& sm, int3
     const float4* qsm = sm.q[w];
     uint32_t count = 0;
     bool unc = false;
-    int32_t jn;
-    float4 nxt = fetch(lane, jn);
+    // The fast pass streams candidate chunks into a three-slot ring in shared memory by cp.async,
+    // two chunks ahead of their use, so the loads' latency hides behind two chunks of tests
+    // without holding registers.  Lanes past the unit's candidates get NaN (never a hit).
+    float4* ring = &sm.ring[w][0][0];
+    auto issue = [&](int32_t c, int slot) {
+        const int32_t k = (c << 5) + lane;
+        float4* dst = ring + slot * 32 + lane;
+        bool copied = false;
+        if (k < M) {
+            while (rpre[cr + 1] <= k) ++cr;
+            const int32_t j = rbeg[cr] + (k - rpre[cr]);
+            if (TCR_GUARD(j, a.nr_total)) {
+                cp_async16(dst, &rs[j]);
+                copied = true;
+            }
+        }
+        if (!copied) *dst = nan4;
+        cp_async_commit();
+        return cr;
+    };
+    int32_t cra = issue(0, 0);  // runs of the candidates of chunks c and c + 1 (seam shifts)
+    int32_t crb = issue(1, 1);
+    int slot = 0;
     for (int32_t c = 0; c < nchunks; ++c) {
-        const float4 cv = nxt;
-        nxt = fetch(((c + 1) << 5) + lane, jn);  // the next chunk's candidate, ahead of its use
+        const int32_t crc = issue(c + 2, slot == 0 ? 2 : slot - 1);
+        cp_async_wait<2>();  // chunk c has landed
+        float4 cv = ring[slot * 32 + lane];
+        if (PERIODIC && shifting) {
+            cv.x += sm.shift[w][0][cra];
+            if (DIM > 1) cv.y += sm.shift[w][1][cra];
+            if (DIM > 2) cv.z += sm.shift[w][2][cra];
+        }
+        cra = crb;
+        crb = crc;
+        slot = slot == 2 ? 0 : slot + 1;
         const float cw = cand_share<MODE>(cv.w);
         const float t = cand_tmax<MODE>(cw, qmax);
         float band = exact_all ? inf : kBandEps * t * t;
@@ -1594,8 +1637,8 @@ __device__ __forceinline__ void count_unit(const WalkArgs& a, WalkSmem& sm, int3
         shifting = false;
         cr = 0;
         count = 0;
-        int32_t jc;
-        nxt = fetch(lane, jn);
+        int32_t jc, jn;
+        float4 nxt = fetch(lane, jn);
         for (int32_t c = 0; c < nchunks; ++c) {
             const float4 cv = nxt;
             jc = jn;
@@ -1861,20 +1904,34 @@ __global__ void __launch_bounds__(kExpandWarps * 32, 3) expand_records_kernel(Ex
     uint32_t* __restrict__ mks = sm.mask[w];
     uint16_t* __restrict__ tab = sm.tab[w];
     int64_t u = (int64_t)blockIdx.x * kExpandWarps + w;
-    int32_t r0n = u < nu ? a.rec[u] : -1;
-    int32_t t0n = u < nu ? a.unit_t0[u] : 0;
+    // A unit's record offset and first query are read two iterations before it runs, its record
+    // header (lanes 0..2) and query rows (lane < 32 covers every unit size) one iteration before,
+    // so a unit starts with its header at hand instead of two dependent round trips.
+    auto header = [&](int32_t r0) -> int32_t {
+        return (r0 >= 0 && lane < 3 && TCR_GUARD(r0 + 3, a.stage_cap)) ? a.stage[r0 + lane] : 0;
+    };
+    auto qrows = [&](int64_t v, int32_t t0) -> int32_t {
+        return (v < nu && TCR_GUARD(t0 + lane, a.nq)) ? a.qsidx[t0 + lane] : -1;
+    };
+    int32_t r0a = u < nu ? a.rec[u] : -1, t0a = u < nu ? a.unit_t0[u] : 0;
+    int32_t r0b = u + warps < nu ? a.rec[u + warps] : -1, t0b = u + warps < nu ? a.unit_t0[u + warps] : 0;
+    int32_t ha = header(r0a), qa = qrows(u, t0a);
     for (; u < nu; u += warps) {
-        const int32_t r0 = r0n, t0 = t0n;
-        if (u + warps < nu) {  // the next unit's record and first query, ahead of their use
-            r0n = a.rec[u + warps];
-            t0n = a.unit_t0[u + warps];
+        const int32_t r0 = r0a, hw = ha, qrow_l = qa;
+        ha = header(r0b);
+        qa = qrows(u + warps, t0b);
+        r0a = r0b;
+        t0a = t0b;
+        r0b = -1;
+        if (u + 2 * warps < nu) {
+            r0b = a.rec[u + 2 * warps];
+            t0b = a.unit_t0[u + 2 * warps];
         }
         if (r0 < 0) continue;  // no candidates, or re-tested by the emit walk
         if (!TCR_GUARD(r0 + 3, a.stage_cap)) continue;
         const int32_t* rec = a.stage + r0;
-        // the unit's queries (lane < 32 covers every unit size) load beside the record header
-        const int32_t qrow_l = TCR_GUARD(t0 + lane, a.nq) ? a.qsidx[t0 + lane] : -1;
-        const int32_t nchunks = rec[0], R = rec[1], nb = rec[2];
+        const int32_t nchunks = __shfl_sync(0xffffffffu, hw, 0), R = __shfl_sync(0xffffffffu, hw, 1),
+                      nb = __shfl_sync(0xffffffffu, hw, 2);
         if (!TCR_GUARD(R, 28) || !TCR_GUARD(nb - 1, 32) || !TCR_GUARD(r0 + record_words(R, nchunks, nb) - 1, a.stage_cap))
             continue;
         const uint32_t* masks = reinterpret_cast<const uint32_t*>(rec + kRecHeader + 2 * R + 1);
@@ -1900,6 +1957,15 @@ __global__ void __launch_bounds__(kExpandWarps * 32, 3) expand_records_kernel(Ex
         for (int32_t c0 = 0; c0 < nchunks; c0 += kExpandWin) {
             const int32_t nc = min(kExpandWin, nchunks - c0);
             const int32_t wbase = c0 << 5;
+            // the window's masks: the first batch loads ahead of the run bitmap
+            const int32_t nm = nc * nb;
+            const uint32_t* src = masks + (int64_t)c0 * nb;
+            uint32_t v[kExpandBatch];
+#pragma unroll
+            for (int i = 0; i < kExpandBatch; ++i) {
+                const int32_t ii = (i << 5) + lane;
+                v[i] = ii < nm ? __ldcs(&src[ii]) : 0u;
+            }
             // run of candidate wbase + k: the runs starting at or before it, minus one
             if (lane < kExpandWin) sm.rstart[w][lane] = 0u;
             __syncwarp();
@@ -1914,14 +1980,13 @@ __global__ void __launch_bounds__(kExpandWarps * 32, 3) expand_records_kernel(Ex
             __syncwarp();
             // the window's masks and candidate columns, the loads of each batch issued together so
             // that their latencies overlap (one load waited for at a time left the warps idle)
-            const int32_t nm = nc * nb;
-            const uint32_t* src = masks + (int64_t)c0 * nb;
             for (int32_t i0 = 0; i0 < nm; i0 += 32 * kExpandBatch) {
-                uint32_t v[kExpandBatch];
+                if (i0 > 0) {
 #pragma unroll
-                for (int i = 0; i < kExpandBatch; ++i) {
-                    const int32_t ii = i0 + (i << 5) + lane;
-                    v[i] = ii < nm ? __ldcs(&src[ii]) : 0u;
+                    for (int i = 0; i < kExpandBatch; ++i) {
+                        const int32_t ii = i0 + (i << 5) + lane;
+                        v[i] = ii < nm ? __ldcs(&src[ii]) : 0u;
+                    }
                 }
 #pragma unroll
                 for (int i = 0; i < kExpandBatch; ++i) {
