@@ -397,11 +397,15 @@ def make_served_workload(seed=5, n_scenes=64, rate=2000.0, seconds=1.0):
     return scenes, arrivals
 
 
+HBM_BUDGET = 120e9  # the served form's admission budget: two thirds of a B200's 180 GB
+
+
 def bench_served(dev, seconds=1.0, slots=2):
     """The served form: requests arrive on a Poisson trace; each jitters its scene by
     N(0, (0.05 h)^2) per coordinate and searches it (gather, COO).  The search server (resident
-    scenes, incremental re-sort, HBM-budget admission, continuous batching on two streams) and the
-    per-call path (one radiusSearch per request, in arrival order) replay the same trace;
+    scenes, incremental re-sort, HBM-budget admission, continuous batching with groups enqueued
+    without host waits) and the per-call path (one radiusSearch per request, in arrival order)
+    replay the same trace;
     latency = completion - arrival, host clock."""
     import torch
 
@@ -417,7 +421,7 @@ def bench_served(dev, seconds=1.0, slots=2):
         return v[min(len(v) - 1, int(q * len(v)))]
 
     # ---- served -------------------------------------------------------------------------
-    srv = SearchServer(dev, mode="gather", hbm_budget=40e9, slots=slots)
+    srv = SearchServer(dev, mode="gather", hbm_budget=HBM_BUDGET, slots=slots)
     for x, h in scenes:
         srv.add_scene(Scene(x.to(dev), torch.full((x.shape[0],), h, device=dev), dom, expected_neighbours=50))
     with srv:
@@ -490,7 +494,7 @@ def bench_served(dev, seconds=1.0, slots=2):
                 "note": "falls behind the arrivals, so value is its capacity"}
     return {"workload": f"64 persistent 3D scenes, sizes log-uniform [1e3, 1e6] (seed 5), periodic [-1,1]^3, "
                         f"50 neighbours, gather, COO; Poisson arrivals 2000/s for {seconds:g} s, each request "
-                        f"jitters its scene by N(0, (0.05 h)^2); 40 GB admission budget, {slots} worker streams",
+                        f"jitters its scene by N(0, (0.05 h)^2); {HBM_BUDGET / 1e9:g} GB admission budget, {slots} worker stream(s)",
             "points": int(sum(x.shape[0] for x, h in scenes)),
             "tuning": {"chosen": {"queries_per_unit": tuned[0], "walk_blocks_per_sm": tuned[1]},
                        "ms_per_batch_of_all_scenes": {f"{c[0]}q/{c[1]}b": round(v, 3)

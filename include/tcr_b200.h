@@ -197,8 +197,9 @@ int tcr_build_structure(const tcr_search_desc* d, void* structure, int64_t struc
  * indptr_out (device int32 [n_query+1]) and row_entries_out (device int64 [n_query]) are the
  * SparseCSR fields of util.py:321-358 and may be NULL.  info_out (host, 8 x int64, may be NULL)
  * receives, asynchronously on `stream`: {total pairs, clouds without a valid grid, queries walked serially,
- * exact-only mode, staging words the units asked for, units left for tcr_emit to re-test, units
- * re-tested with exact decisions because a pair lay within the fast test's rounding band, and
+ * exact-only mode, staging words the units asked for, units left for tcr_emit to re-test, chunks
+ * (32 candidates of a unit) tested again with exact decisions because a pair lay within the fast
+ * test's rounding band, and
  * for a batch built with a linear-cell hint the points its incremental re-sort sorted (-1: it fell
  * back to the full sort; -2: no hint)};
  * a caller sizes the next search's staging list from entry 4. */

@@ -80,27 +80,46 @@ __global__ void __launch_bounds__(1024) scan_tiles_kernel(T* tile_sums, int64_t 
     if (threadIdx.x == 0 && grand_total) *grand_total = carry;
 }
 
-// Pass 3: per-tile exclusive scan; Out(i, exclusive_prefix, value) consumes each element.
-// Elements are processed in blocked order (thread t owns kScanItems consecutive elements).
+// Pass 3: per-tile exclusive scan; Out(i, exclusive_prefix, value) consumes each element.  The
+// tile's values are read and its results consumed in striped order (element base + k * threads +
+// thread), so that the producer's loads and the consumer's stores coalesce; in between they pass
+// through shared memory to the blocked order (kScanItems consecutive elements per thread) the
+// scan works in.  A padded index keeps the blocked reads free of bank conflicts.
+__device__ __forceinline__ int scan_pad(int i) { return i + (i >> 5); }
+
 template <typename T, typename In, typename Out>
 __global__ void __launch_bounds__(kScanThreads) scan_apply_kernel(In in, Out out, int64_t n, const T* tile_sums) {
     __shared__ T sm[kScanThreads / 32 + 1];
-    const int64_t base = (int64_t)blockIdx.x * kScanTile + (int64_t)threadIdx.x * kScanItems;
+    __shared__ T sval[kScanTile + kScanTile / 32];
+    __shared__ T sex[kScanTile + kScanTile / 32];
+    const int64_t base = (int64_t)blockIdx.x * kScanTile;
+#pragma unroll
+    for (int k = 0; k < kScanItems; ++k) {
+        const int j = k * kScanThreads + threadIdx.x;
+        const int64_t i = base + j;
+        sval[scan_pad(j)] = i < n ? in(i) : T(0);
+    }
+    __syncthreads();
     T v[kScanItems];
     T s = 0;
 #pragma unroll
     for (int k = 0; k < kScanItems; ++k) {
-        int64_t i = base + k;
-        v[k] = i < n ? in(i) : T(0);
+        v[k] = sval[scan_pad(threadIdx.x * kScanItems + k)];
         s += v[k];
     }
     T total;
     T ex = block_exclusive_scan<T, kScanThreads>(s, sm, total) + tile_sums[blockIdx.x];
 #pragma unroll
     for (int k = 0; k < kScanItems; ++k) {
-        int64_t i = base + k;
-        if (i < n) out(i, ex, v[k]);
+        sex[scan_pad(threadIdx.x * kScanItems + k)] = ex;
         ex += v[k];
+    }
+    __syncthreads();
+#pragma unroll
+    for (int k = 0; k < kScanItems; ++k) {
+        const int j = k * kScanThreads + threadIdx.x;
+        const int64_t i = base + j;
+        if (i < n) out(i, sex[scan_pad(j)], sval[scan_pad(j)]);
     }
 }
 

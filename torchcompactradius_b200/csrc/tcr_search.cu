@@ -1371,7 +1371,7 @@ __device__ __forceinline__ uint32_t chunk_hits_x2(const float4* __restrict__ qp,
     const float2 ncx = make_float2(-cv.x, -cv.x), ncy = make_float2(-cv.y, -cv.y), ncz = make_float2(-cv.z, -cv.z);
     const float2 ncw = make_float2(-cv.w, -cv.w), pcw = make_float2(cv.w, cv.w);
     uint32_t hit = 0;
-    for (int p = (K4 >> 1) - 2; p >= 0; p -= 2) {
+    for (int p = (K4 >> 1) - 2; p >= 0; p -= 2) {  // two query pairs per iteration (K4 a multiple of 4)
 #pragma unroll
         for (int i = 1; i >= 0; --i) {
             const float4 a = qp[2 * (p + i)];
@@ -1547,22 +1547,6 @@ __device__ __forceinline__ void count_unit(const WalkArgs& a, WalkSmem& sm, int3
     const int32_t* rbeg = sm.run_beg[w];
     const float4* __restrict__ rs = a.rsorted;
     int32_t cr = 0;
-    bool shifting = shift_mode;  // the fast pass tests shifted candidates, the exact pass the originals
-    auto fetch = [&](int32_t k, int32_t& j) {
-        float4 v = nan4;
-        j = 0;
-        if (k < M) {
-            while (rpre[cr + 1] <= k) ++cr;
-            j = rbeg[cr] + (k - rpre[cr]);
-            if (TCR_GUARD(j, a.nr_total)) v = __ldg(&rs[j]);
-            if (PERIODIC && shifting) {
-                v.x += sm.shift[w][0][cr];
-                if (DIM > 1) v.y += sm.shift[w][1][cr];
-                if (DIM > 2) v.z += sm.shift[w][2][cr];
-            }
-        }
-        return v;
-    };
     const WrapCtx wc = wrap_ctx(u.periodic_mask, u.ext);
     const float qmax = u.qmax;
     const bool exact_all = u.exact_all != 0;
@@ -1571,7 +1555,6 @@ __device__ __forceinline__ void count_unit(const WalkArgs& a, WalkSmem& sm, int3
     const int K4 = (nb + 3) & ~3;
     const float4* qsm = sm.q[w];
     uint32_t count = 0;
-    bool unc = false;
     // The fast pass streams candidate chunks into a three-slot ring in shared memory by cp.async,
     // two chunks ahead of their use, so the loads' latency hides behind two chunks of tests
     // without holding registers.  Lanes past the unit's candidates get NaN (never a hit).
@@ -1599,10 +1582,11 @@ __device__ __forceinline__ void count_unit(const WalkArgs& a, WalkSmem& sm, int3
         const int32_t crc = issue(c + 2, slot == 0 ? 2 : slot - 1);
         cp_async_wait<2>();  // chunk c has landed
         float4 cv = ring[slot * 32 + lane];
-        if (PERIODIC && shifting) {
-            cv.x += sm.shift[w][0][cra];
-            if (DIM > 1) cv.y += sm.shift[w][1][cra];
-            if (DIM > 2) cv.z += sm.shift[w][2][cra];
+        const int32_t crn = cra;  // run of this chunk's candidate
+        if (PERIODIC && shift_mode) {  // the fast test takes seam candidates shifted
+            cv.x += sm.shift[w][0][crn];
+            if (DIM > 1) cv.y += sm.shift[w][1][crn];
+            if (DIM > 2) cv.z += sm.shift[w][2][crn];
         }
         cra = crb;
         crb = crc;
@@ -1612,46 +1596,39 @@ __device__ __forceinline__ void count_unit(const WalkArgs& a, WalkSmem& sm, int3
         float band = exact_all ? inf : kBandEps * t * t;
         // float64 inputs: the band also covers the rounding of the coordinates to float32
         if (fe > 0.0f) band += fmaf(2.0f * 1.7320508f * t, fe, 3.0f * fe * fe);
+        const float band_exact = band;
         // shifted candidates: the band also covers the shift's rounding (|d2 error| <= 2 T delta + delta^2)
         if (seam) band += fmaf(2.0f * t, dl, dl * dl);
         uint32_t hit;
+        bool inband = false;  // some pair of this lane's candidate lies within the band
         if (MODE != kSuperSymmetric && (!PERIODIC || shift_mode)) {
             float umin = inf;
             hit = chunk_hits_x2<DIM, MODE>(sm.qp[w], K4, cv, cw, umin);
-            unc |= umin <= band;
+            inband = umin <= band;
         } else if (shift_mode) {
-            hit = chunk_hits<DIM, false, MODE>(wc, qsm, K4, cv, cw, band, unc);
+            hit = chunk_hits<DIM, false, MODE>(wc, qsm, K4, cv, cw, band, inband);
         } else {
-            hit = chunk_hits<DIM, PERIODIC, MODE>(wc, qsm, K4, cv, cw, band, unc);
+            hit = chunk_hits<DIM, PERIODIC, MODE>(wc, qsm, K4, cv, cw, band, inband);
+        }
+        if (__any_sync(0xffffffffu, inband)) {
+            // some pair of the chunk lies within the band: the chunk again, every pair in the band
+            // decided by the reference's exact test on the original (unshifted) candidates
+            if (lane == 0) atomicAdd(a.num_exact, 1);
+            const int32_t k = (c << 5) + lane;
+            float4 v0 = nan4;
+            int32_t j = 0;
+            if (k < M) {
+                j = rbeg[crn] + (k - rpre[crn]);
+                if (TCR_GUARD(j, a.nr_total)) v0 = __ldg(&rs[j]);
+            }
+            hit = chunk_hits_exact<DIM, MODE>(unit_exact_ctx(u, MODE), qsm, sm.qh[w], sm.qid[w], K4, v0, j,
+                                              band_exact, a.f64);
         }
         const uint32_t m = warp_transpose32(hit, lane);
         if (lane < nb) {
             count += __popc(m);
             if (stage && TCR_IN((int64_t)(msk - reinterpret_cast<uint32_t*>(a.stage)) + c * nb + lane, a.stage_cap))
                 msk[c * nb + lane] = m;
-        }
-    }
-    if (__any_sync(0xffffffffu, unc)) {  // some pair lies in the band: walk again with exact decisions
-        if (lane == 0) atomicAdd(a.num_exact, 1);
-        const ExactCtx xc = unit_exact_ctx(u, MODE);
-        shifting = false;
-        cr = 0;
-        count = 0;
-        int32_t jc, jn;
-        float4 nxt = fetch(lane, jn);
-        for (int32_t c = 0; c < nchunks; ++c) {
-            const float4 cv = nxt;
-            jc = jn;
-            nxt = fetch(((c + 1) << 5) + lane, jn);
-            const float t = cand_tmax<MODE>(cand_share<MODE>(cv.w), qmax);
-            float band = exact_all ? inf : kBandEps * t * t;
-            if (fe > 0.0f) band += fmaf(2.0f * 1.7320508f * t, fe, 3.0f * fe * fe);
-            const uint32_t m = warp_transpose32(
-                chunk_hits_exact<DIM, MODE>(xc, qsm, sm.qh[w], sm.qid[w], K4, cv, jc, band, a.f64), lane);
-            if (lane < nb) {
-                count += __popc(m);
-                if (stage) msk[c * nb + lane] = m;
-            }
         }
     }
     if (active) a.counts[qorig] = (int32_t)count;
@@ -1822,6 +1799,7 @@ __global__ void __launch_bounds__(kWalkWarps * 32) walk_emit_kernel(WalkArgs a) 
     __shared__ EmitSmem sm;
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
     const int32_t nlist = *a.num_list;
+    if (nlist == 0) return;  // every unit was staged: no claim atomics at all
     int32_t* counter = a.class_filter >= 0 ? &a.work[8 + a.class_filter] : &a.work[1];
     int cur = -1;
     for (;;) {
@@ -1845,6 +1823,13 @@ __global__ void __launch_bounds__(kWalkWarps * 32) walk_emit_kernel(WalkArgs a) 
     }
 }
 
+// Position of the highest set bit of a non-zero word (one bfind).
+__device__ __forceinline__ uint32_t top_set_bit(uint32_t m) {
+    uint32_t b;
+    asm("bfind.u32 %0, %1;" : "=r"(b) : "r"(m));
+    return b;
+}
+
 // Emit pass for staged units: expand each unit's record into its queries' CSR/COO slots, one warp
 // per unit, window by window of kExpandWin chunks.  The window's candidate columns are gathered
 // into shared memory once (consecutive sorted indices: coalesced reads of the sort index; each
@@ -1856,17 +1841,16 @@ __global__ void __launch_bounds__(kWalkWarps * 32) walk_emit_kernel(WalkArgs a) 
 // query instead.
 constexpr int kExpandWarps = 8;
 constexpr int kExpandWin = 16;    // chunks per window: 512 candidates
-constexpr int kExpandTab = 2048;  // outputs one table holds
+constexpr int kExpandTab = 1920;  // outputs one table holds (four blocks of eight warps fit an SM)
 constexpr int kExpandBatch = 8;   // global loads a lane issues before it waits for the first
 struct ExpandSmem {
     int32_t col[kExpandWarps][kExpandWin * 32];    // output column of each candidate of the window
-    uint32_t mask[kExpandWarps][kExpandWin * 32];  // the window's masks, [chunk][query]
     uint16_t tab[kExpandWarps][kExpandTab];        // (query << 9) | (chunk << 5) | bit, in output order
     uint32_t rstart[kExpandWarps][kExpandWin];     // bit k of word c: a run starts at candidate 32 c + k
     int32_t rrank[kExpandWarps][kExpandWin];       // runs starting before word c, minus one
     int32_t run_beg[kExpandWarps][32];
     int32_t run_pre[kExpandWarps][33];
-    int64_t qbase[kExpandWarps][32];               // output slot of table entry 0 of each query (this window)
+    long long* qcol[kExpandWarps][32];             // column output of table entry 0 of each query (this window)
     int64_t qoff[kExpandWarps][32];                // output position of each query's next hit
     int32_t qrow[kExpandWarps][32];
 };
@@ -1892,7 +1876,7 @@ struct ExpandArgs {
     int64_t stage_cap, nq, nr;  // bounds of the checked build
 };
 
-__global__ void __launch_bounds__(kExpandWarps * 32, 3) expand_records_kernel(ExpandArgs a) {
+__global__ void __launch_bounds__(kExpandWarps * 32, 4) expand_records_kernel(ExpandArgs a) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     ExpandSmem& sm = *reinterpret_cast<ExpandSmem*>(smem_raw);
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
@@ -1901,7 +1885,6 @@ __global__ void __launch_bounds__(kExpandWarps * 32, 3) expand_records_kernel(Ex
     int32_t* __restrict__ rbeg = sm.run_beg[w];
     int32_t* __restrict__ rpre = sm.run_pre[w];
     int32_t* __restrict__ cols = sm.col[w];
-    uint32_t* __restrict__ mks = sm.mask[w];
     uint16_t* __restrict__ tab = sm.tab[w];
     int64_t u = (int64_t)blockIdx.x * kExpandWarps + w;
     // A unit's record offset and first query are read two iterations before it runs, its record
@@ -1957,14 +1940,15 @@ __global__ void __launch_bounds__(kExpandWarps * 32, 3) expand_records_kernel(Ex
         for (int32_t c0 = 0; c0 < nchunks; c0 += kExpandWin) {
             const int32_t nc = min(kExpandWin, nchunks - c0);
             const int32_t wbase = c0 << 5;
-            // the window's masks: the first batch loads ahead of the run bitmap
-            const int32_t nm = nc * nb;
+            // the window's masks, in registers: lane (q, g) holds the masks of chunks g, g + G, ...
+            // (G = 1 when the unit has more than 16 queries), all loaded at the window's start;
+            // consecutive lanes read consecutive words
             const uint32_t* src = masks + (int64_t)c0 * nb;
-            uint32_t v[kExpandBatch];
+            uint32_t mv[kExpandWin];
 #pragma unroll
-            for (int i = 0; i < kExpandBatch; ++i) {
-                const int32_t ii = (i << 5) + lane;
-                v[i] = ii < nm ? __ldcs(&src[ii]) : 0u;
+            for (int t = 0; t < kExpandWin; ++t) {
+                const int32_t c = g + G * t;
+                mv[t] = (qlane && c < nc) ? __ldcs(&src[c * nb + q]) : 0u;
             }
             // run of candidate wbase + k: the runs starting at or before it, minus one
             if (lane < kExpandWin) sm.rstart[w][lane] = 0u;
@@ -1978,22 +1962,8 @@ __global__ void __launch_bounds__(kExpandWarps * 32, 3) expand_records_kernel(Ex
             const int32_t wpi = warp_inclusive_scan(wp);
             if (lane < kExpandWin) sm.rrank[w][lane] = nbefore + wpi - wp - 1;
             __syncwarp();
-            // the window's masks and candidate columns, the loads of each batch issued together so
-            // that their latencies overlap (one load waited for at a time left the warps idle)
-            for (int32_t i0 = 0; i0 < nm; i0 += 32 * kExpandBatch) {
-                if (i0 > 0) {
-#pragma unroll
-                    for (int i = 0; i < kExpandBatch; ++i) {
-                        const int32_t ii = i0 + (i << 5) + lane;
-                        v[i] = ii < nm ? __ldcs(&src[ii]) : 0u;
-                    }
-                }
-#pragma unroll
-                for (int i = 0; i < kExpandBatch; ++i) {
-                    const int32_t ii = i0 + (i << 5) + lane;
-                    if (ii < nm) mks[ii] = v[i];
-                }
-            }
+            // the window's candidate columns, the loads of each batch issued together so that their
+            // latencies overlap (one load waited for at a time left the warps idle)
             const uint32_t le = (2u << lane) - 1u;  // bits 0 .. lane
             for (int32_t cc0 = 0; cc0 < nc; cc0 += kExpandBatch) {
                 int32_t jl[kExpandBatch];
@@ -2024,8 +1994,8 @@ __global__ void __launch_bounds__(kExpandWarps * 32, 3) expand_records_kernel(Ex
             __syncwarp();
             // the window's outputs of each query, and their exclusive prefix over the queries
             int32_t tot = 0;
-            if (qlane)
-                for (int32_t c = g; c < nc; c += G) tot += __popc(mks[c * nb + q]);
+#pragma unroll
+            for (int t = 0; t < kExpandWin; ++t) tot += __popc(mv[t]);
             for (int sft = nbp; sft < 32; sft <<= 1) tot += __shfl_xor_sync(0xffffffffu, tot, sft);
             const int32_t tv = (g == 0 && qlane) ? tot : 0;
             const int32_t tinc = warp_inclusive_scan(tv);
@@ -2034,9 +2004,11 @@ __global__ void __launch_bounds__(kExpandWarps * 32, 3) expand_records_kernel(Ex
             if (n <= kExpandTab) {
                 // each lane expands its (query, chunk) mask into the table, highest bit at the end
                 int32_t run = qpre;  // table slot of the query's next output
-                for (int32_t cc0 = 0; cc0 < nc; cc0 += G) {
-                    const int32_t c = cc0 + g;
-                    uint32_t m = (qlane && c < nc) ? mks[c * nb + q] : 0u;
+#pragma unroll
+                for (int t = 0; t < kExpandWin; ++t) {
+                    if (G * t >= nc) break;
+                    const int32_t c = G * t + g;
+                    uint32_t m = mv[t];
                     int32_t inc = __popc(m);
                     for (int sft = nbp; sft < 32; sft <<= 1) {  // inclusive scan over g, per query
                         const int32_t t = __shfl_up_sync(0xffffffffu, inc, sft);
@@ -2046,29 +2018,44 @@ __global__ void __launch_bounds__(kExpandWarps * 32, 3) expand_records_kernel(Ex
                     int32_t pos = run + inc;
                     const uint32_t tag = ((uint32_t)q << 9) | ((uint32_t)c << 5);
                     while (m) {
-                        const int bit = 31 - __clz(m);
+                        const uint32_t bit = top_set_bit(m);
                         m ^= 1u << bit;
                         tab[--pos] = (uint16_t)(tag | bit);
                     }
                     run += tq;
                 }
-                if (g == 0 && qlane) sm.qbase[w][q] = sm.qoff[w][q] - qpre;
+                // per query: the output slot of its table entry 0, and whether all of the window's
+                // outputs fit the output buffer (then the column-only loop writes without checks)
+                bool fits = true;
+                if (g == 0 && qlane) {
+                    sm.qcol[w][q] = reinterpret_cast<long long*>(a.col_out) + (sm.qoff[w][q] - qpre);
+                    fits = sm.qoff[w][q] + tot <= a.out_cap;
+                }
+                fits = __all_sync(0xffffffffu, fits);
                 __syncwarp();
                 const bool rows = a.row_out != nullptr;
+                if (fits && !rows) {
 #pragma unroll 4
-                for (int32_t o = lane; o < n; o += 32) {
-                    const uint32_t v = tab[o];
-                    const uint32_t vq = v >> 9;
-                    const int64_t pos = sm.qbase[w][vq] + o;
-                    if (TCR_GUARD(pos, a.out_cap)) {
-                        __stcs(reinterpret_cast<long long*>(&a.col_out[pos]), (long long)cols[v & 0x1ffu]);
-                        if (rows) __stcs(reinterpret_cast<long long*>(&a.row_out[pos]), (long long)sm.qrow[w][vq]);
+                    for (int32_t o = lane; o < n; o += 32) {
+                        const uint32_t v = tab[o];
+                        __stcs(sm.qcol[w][v >> 9] + o, (long long)cols[v & 0x1ffu]);
+                    }
+                } else {
+#pragma unroll 4
+                    for (int32_t o = lane; o < n; o += 32) {
+                        const uint32_t v = tab[o];
+                        const uint32_t vq = v >> 9;
+                        const int64_t pos = (sm.qcol[w][vq] - reinterpret_cast<long long*>(a.col_out)) + o;
+                        if (TCR_GUARD(pos, a.out_cap)) {
+                            __stcs(reinterpret_cast<long long*>(&a.col_out[pos]), (long long)cols[v & 0x1ffu]);
+                            if (rows) __stcs(reinterpret_cast<long long*>(&a.row_out[pos]), (long long)sm.qrow[w][vq]);
+                        }
                     }
                 }
             } else {
                 // many outputs: query by query, lanes over the window's chunks
                 for (int32_t qq = 0; qq < nb; ++qq) {
-                    uint32_t m = lane < nc ? mks[lane * nb + qq] : 0u;
+                    uint32_t m = lane < nc ? __ldcs(&src[lane * nb + qq]) : 0u;
                     const int32_t cnt = __popc(m);
                     const int32_t inc = warp_inclusive_scan(cnt);
                     int64_t pos = sm.qoff[w][qq] + (inc - cnt);
@@ -2596,9 +2583,10 @@ static int build_impl(const HostBatch& b, const Structure& S, const Scratch& W, 
     TCR_CUDA(cudaMemsetAsync(S.map, 0xff, sizeof(unsigned long long) * S.map_total, st));
     if (nr > 0) {
         const bool inc = b.lin_hint != nullptr;
-        pack_points_kernel<K><<<grid_for(nr, 256), 256, 0, st>>>(W.table, S.grid, W.ref_prefix, C, nr, 0, 2, 1, W.pack,
-                                                                 sw.keys[0], sw.vals[0], sw.state,
-                                                                 inc ? b.lin_hint : nullptr, inc ? W.stay : nullptr);
+        // few blocks: each ends with one atomic on the key range, so thousands of them would queue
+        pack_points_kernel<K><<<grid_for(nr, 256, num_sms() * 4), 256, 0, st>>>(
+            W.table, S.grid, W.ref_prefix, C, nr, 0, 2, 1, W.pack, sw.keys[0], sw.vals[0], sw.state,
+            inc ? b.lin_hint : nullptr, inc ? W.stay : nullptr);
         note_launches(1);
         if (inc) {
             SortWorkspaceT<K> mw = sw;
@@ -2677,8 +2665,8 @@ static int count_impl(const HostBatch& b, const Structure& S, const Scratch& W, 
             const SortWorkspaceT<K> sw = sort_workspace<K>(W);
             sort_state_init_kernel<K><<<1, 1, 0, st>>>(sw.state);
             note_launches(1);
-            pack_points_kernel<K><<<grid_for(nq, 256), 256, 0, st>>>(W.table, S.grid, W.query_prefix, C, nq, 1, 1, 0,
-                                                                     W.pack, sw.keys[0], sw.vals[0], sw.state);
+            pack_points_kernel<K><<<grid_for(nq, 256, num_sms() * 4), 256, 0, st>>>(
+                W.table, S.grid, W.query_prefix, C, nq, 1, 1, 0, W.pack, sw.keys[0], sw.vals[0], sw.state);
             note_launches(1);
             TCR_CUDA(radix_sort_pairs<K>(sw, nq, st));
             gather_sorted_kernel<K><<<grid_for(nq, 256), 256, 0, st>>>(W.pack, sw.vals[0], sw.vals[1], sw.state, nq,

@@ -50,7 +50,7 @@ from .util import DomainDescription, SparseCOO
 # indices of the group (int64 slot, shift), the user ids, the cell hint and the new cell order
 # (int32 each); per staging word 4 bytes; per pair two int64 (COO row and column).
 WORK_BYTES_PER_POINT = 32
-STAGE_WORDS_PER_POINT = 64
+STAGE_WORDS_PER_POINT = 24  # dense 3D clouds (50 neighbours) stage about 15 record words per point
 
 
 class Scene:
