@@ -100,6 +100,41 @@ def config(pairs):
             "l2": "flushed between timed steps (256 MiB device write)", "parallelism": "replicas"}
 
 
+def gpu_local_cpus(index):
+    """The CPUs NVML reports as local to CUDA device `index` (read-only query), or None."""
+    try:
+        import pynvml
+        import torch
+        pynvml.nvmlInit()
+        p = torch.cuda.get_device_properties(index)
+        bus = f"{p.pci_domain_id:08x}:{p.pci_bus_id:02x}:{p.pci_device_id:02x}.0"
+        words = pynvml.nvmlDeviceGetCpuAffinity(pynvml.nvmlDeviceGetHandleByPciBusId(bus), (os.cpu_count() + 63) // 64)
+        cpus = {64 * i + b for i, word in enumerate(words) for b in range(64) if (word >> b) & 1}
+        return (cpus & os.sched_getaffinity(0)) or None
+    except Exception:
+        return None
+
+
+class near_gpu:
+    """Runs the block on the CPUs local to the GPU, so that pinned host buffers allocated inside it
+    come from the GPU's NUMA node (host<->device copies from the far node run at a fraction of the
+    link's speed); restores the affinity afterwards."""
+
+    def __init__(self, index):
+        self.cpus = gpu_local_cpus(index)
+        self.old = None
+
+    def __enter__(self):
+        if self.cpus:
+            self.old = os.sched_getaffinity(0)
+            os.sched_setaffinity(0, self.cpus)
+        return self
+
+    def __exit__(self, *exc):
+        if self.old is not None:
+            os.sched_setaffinity(0, self.old)
+
+
 def measured_peak():
     p = os.path.join(REPO, "MEASURED_PEAKS.json")
     try:
@@ -274,8 +309,9 @@ def bench_batched(dev, stream, flush, steps, warmup, with_cpu):
     clouds = make_batched_workload()
     C = len(clouds)
     parts = {2: [c for c in clouds if c["dim"] == 2], 3: [c for c in clouds if c["dim"] == 3]}
-    host = {d: (torch.cat([c["x"] for c in parts[d]]).pin_memory(), torch.cat([c["h"] for c in parts[d]]).pin_memory())
-            for d in (2, 3)}
+    with near_gpu(dev.index):
+        host = {d: (torch.cat([c["x"] for c in parts[d]]).pin_memory(),
+                    torch.cat([c["h"] for c in parts[d]]).pin_memory()) for d in (2, 3)}
     devx = {d: (host[d][0].to(dev), host[d][1].to(dev)) for d in (2, 3)}
     table = batched.cloud_table(C)
     off = {2: 0, 3: 0}
@@ -339,8 +375,9 @@ def bench_batched(dev, stream, flush, steps, warmup, with_cpu):
     per_call_value = tot * len(pc_ms) / (sum(pc_ms) / 1e3)
 
     # end to end: inputs from pinned host memory, batched search, CSR back to pinned host memory
-    out_idx = torch.empty(pairs, dtype=torch.int64, pin_memory=True)
-    out_ptr = torch.empty(n_points + 1, dtype=torch.int32, pin_memory=True)
+    with near_gpu(dev.index):
+        out_idx = torch.empty(pairs, dtype=torch.int64, pin_memory=True)
+        out_ptr = torch.empty(n_points + 1, dtype=torch.int32, pin_memory=True)
     e2e_ms = []
     for k in range(max(3, min(steps, 10))):
         flush.fill_(k & 0xff)
@@ -872,7 +909,8 @@ def run_b200(args):
     max_over_ranks = ranks.max
 
     pos_h, sup_h = make_workload()
-    pos_pin, sup_pin = pos_h.pin_memory(), sup_h.pin_memory()
+    with near_gpu(local):
+        pos_pin, sup_pin = pos_h.pin_memory(), sup_h.pin_memory()
     pos_d, sup_d = pos_h.to(dev), sup_h.to(dev)
     dom = tcr.DomainDescription(torch.tensor([-1.0] * 3), torch.tensor([1.0] * 3), torch.tensor([False] * 3), 3)
     lib = _lib.load()
@@ -955,9 +993,10 @@ def run_b200(args):
 
     # ---- end to end through the public API (pinned host in, host out) ----------------------
     nq = N_POINTS
-    out_idx = torch.empty(pairs, dtype=torch.int64, pin_memory=True)
-    out_ptr = torch.empty(nq + 1, dtype=torch.int32, pin_memory=True)
-    out_ent = torch.empty(nq, dtype=torch.int64, pin_memory=True)
+    with near_gpu(local) as near:
+        out_idx = torch.empty(pairs, dtype=torch.int64, pin_memory=True)
+        out_ptr = torch.empty(nq + 1, dtype=torch.int32, pin_memory=True)
+        out_ent = torch.empty(nq, dtype=torch.int64, pin_memory=True)
     e2e_ms = []
     barrier()
     for k in range(max(3, min(args.steps, 30))):
@@ -974,6 +1013,16 @@ def run_b200(args):
         e.record(stream)
         e.synchronize()
         e2e_ms.append(s.elapsed_time(e))
+    # the device->host copy of the column indices alone: the link's share of the step
+    d2h = []
+    for _ in range(3):
+        s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        s.record(stream)
+        out_idx.copy_(adj.indices, non_blocking=True)
+        e.record(stream)
+        e.synchronize()
+        d2h.append(s.elapsed_time(e))
+    d2h_gbs = 8 * pairs / (statistics.median(d2h) / 1e3) / 1e9
     barrier()
     e2e_total = max_over_ranks(sum(e2e_ms))
     e2e_value = pairs * len(e2e_ms) * world / (e2e_total / 1e3)
@@ -1009,7 +1058,9 @@ def run_b200(args):
                             "frac": search_bytes / search_s / 1e9 / peak, "peak_kind": peak_kind},
         "e2e": {"value": e2e_value, "unit": "pairs/s", "h2d_bytes_per_step": 16 * N_POINTS,
                 "d2h_bytes_per_step": 8 * pairs + 4 * (N_POINTS + 1) + 8 * N_POINTS,
-                "ms_per_step": e2e_total / len(e2e_ms), "output_checked": bool(ok)},
+                "ms_per_step": e2e_total / len(e2e_ms), "output_checked": bool(ok),
+                "d2h_indices_GBps": d2h_gbs,
+                "host_buffers": "pinned, allocated on the GPU's NUMA node" if near.cpus else "pinned"},
         "gpu_launches": int(launches),
         "clocks": clocks,
         "tuning": tuning,

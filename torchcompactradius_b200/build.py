@@ -34,24 +34,27 @@ def build_ops(force=False, verbose=False):
         return dst
     import shutil
 
-    from torch.utils import cpp_extension
     bdir = os.path.join(HERE, "_build", "ops")
     os.makedirs(bdir, exist_ok=True)
-    cmd_env = os.environ.copy()
+    env = os.environ.copy()
     # The system g++ links libstdc++ dynamically, the one copy torch uses; a toolchain whose
     # library path holds only the static archive would give this library a second, uninitialised
     # copy of the C++ runtime (its stream and locale state), so the system compiler is used.
     if os.path.exists("/usr/bin/g++"):
-        os.environ["CXX"] = "/usr/bin/g++"
-    cpp_extension.load(name="tcr_torch_ops", sources=[os.path.join(CSRC, OPS_SRC)],
-                       extra_include_paths=[os.path.join(REPO, "include")],
-                       extra_cflags=["-O2", "-std=c++17"],
-                       extra_ldflags=["-L" + HERE, "-ltcr_b200",
-                                      # $$ reaches the linker as one $ through ninja, quotes keep the shell off it
-                                      "'-Wl,-rpath,$$ORIGIN'", "'-Wl,-rpath,$$ORIGIN/../..'"],
-                       with_cuda=True, is_python_module=False, build_directory=bdir, verbose=verbose)
-    os.environ.clear()
-    os.environ.update(cmd_env)
+        env["CXX"] = "/usr/bin/g++"
+    # torch's extension builder loads what it built into the calling process; it runs in a child
+    # so that this process registers the operators once, from the package copy (ops.load).
+    script = f"""
+from torch.utils import cpp_extension
+cpp_extension.load(name="tcr_torch_ops", sources=[{os.path.join(CSRC, OPS_SRC)!r}],
+                   extra_include_paths=[{os.path.join(REPO, "include")!r}],
+                   extra_cflags=["-O2", "-std=c++17"],
+                   extra_ldflags=["-L" + {HERE!r}, "-ltcr_b200",
+                                  # $$ reaches the linker as one $ through ninja, quotes keep the shell off it
+                                  "'-Wl,-rpath,$$ORIGIN'", "'-Wl,-rpath,$$ORIGIN/../..'"],
+                   with_cuda=True, is_python_module=False, build_directory={bdir!r}, verbose={bool(verbose)!r})
+"""
+    subprocess.check_call([sys.executable, "-c", script], env=env)
     shutil.copy2(os.path.join(bdir, "tcr_torch_ops.so"), dst)
     return dst
 

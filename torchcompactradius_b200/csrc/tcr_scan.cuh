@@ -1,8 +1,10 @@
 // tcr_scan.cuh -- device-wide exclusive prefix sums built from a block scan.
 //
-// Three launches: per-tile reduction, a single-CTA scan of the tile totals, and a per-tile scan
-// that adds the tile's prefix.  Input and output are functors so that producers (flags, counts)
-// and consumers (cell tables, offsets) fuse into the scan instead of round-tripping through HBM.
+// A per-tile reduction, then a per-tile scan that adds the tile's prefix.  Up to kScanDirectTiles
+// tiles, each tile sums the totals of the tiles before it itself (at most 16 KB of reads, from L2);
+// above that a single-CTA scan of the tile totals runs in between.  No block waits for another.
+// Input and output are functors so that producers (flags, counts) and consumers (cell tables,
+// offsets) fuse into the scan instead of round-tripping through HBM.
 #pragma once
 #include <cstdint>
 #include <cuda_runtime.h>
@@ -14,6 +16,7 @@ namespace tcr {
 constexpr int kScanThreads = 256;
 constexpr int kScanItems = 8;
 constexpr int kScanTile = kScanThreads * kScanItems;
+constexpr int64_t kScanDirectTiles = 2048;  // 4M elements
 
 template <typename T>
 __device__ __forceinline__ T warp_inclusive_scan(T v) {
@@ -87,8 +90,11 @@ __global__ void __launch_bounds__(1024) scan_tiles_kernel(T* tile_sums, int64_t 
 // scan works in.  A padded index keeps the blocked reads free of bank conflicts.
 __device__ __forceinline__ int scan_pad(int i) { return i + (i >> 5); }
 
-template <typename T, typename In, typename Out>
-__global__ void __launch_bounds__(kScanThreads) scan_apply_kernel(In in, Out out, int64_t n, const T* tile_sums) {
+// DIRECT: tile_sums holds the tiles' own totals; the tile's prefix is their sum over the tiles
+// before it, and the last tile stores the grand total.  Otherwise tile_sums holds the prefixes.
+template <typename T, bool DIRECT, typename In, typename Out>
+__global__ void __launch_bounds__(kScanThreads) scan_apply_kernel(In in, Out out, int64_t n, const T* tile_sums,
+                                                                  T* grand_total) {
     __shared__ T sm[kScanThreads / 32 + 1];
     __shared__ T sval[kScanTile + kScanTile / 32];
     __shared__ T sex[kScanTile + kScanTile / 32];
@@ -99,7 +105,15 @@ __global__ void __launch_bounds__(kScanThreads) scan_apply_kernel(In in, Out out
         const int64_t i = base + j;
         sval[scan_pad(j)] = i < n ? in(i) : T(0);
     }
-    __syncthreads();
+    T prefix;
+    if (DIRECT) {
+        T acc = 0;
+        for (int64_t t = threadIdx.x; t < (int64_t)blockIdx.x; t += kScanThreads) acc += tile_sums[t];
+        block_exclusive_scan<T, kScanThreads>(acc, sm, prefix);  // (its barriers also publish sval)
+    } else {
+        prefix = tile_sums[blockIdx.x];
+        __syncthreads();
+    }
     T v[kScanItems];
     T s = 0;
 #pragma unroll
@@ -108,7 +122,8 @@ __global__ void __launch_bounds__(kScanThreads) scan_apply_kernel(In in, Out out
         s += v[k];
     }
     T total;
-    T ex = block_exclusive_scan<T, kScanThreads>(s, sm, total) + tile_sums[blockIdx.x];
+    T ex = block_exclusive_scan<T, kScanThreads>(s, sm, total) + prefix;
+    if (DIRECT && grand_total && blockIdx.x == gridDim.x - 1 && threadIdx.x == 0) *grand_total = prefix + total;
 #pragma unroll
     for (int k = 0; k < kScanItems; ++k) {
         sex[scan_pad(threadIdx.x * kScanItems + k)] = ex;
@@ -134,8 +149,13 @@ cudaError_t device_exclusive_scan(In in, Out out, int64_t n, T* tile_sums, T* gr
         return cudaSuccess;
     }
     scan_reduce_kernel<T><<<(unsigned)nt, kScanThreads, 0, st>>>(in, n, tile_sums);
+    if (nt <= kScanDirectTiles) {
+        scan_apply_kernel<T, true><<<(unsigned)nt, kScanThreads, 0, st>>>(in, out, n, tile_sums, grand_total);
+        note_launches(2);
+        return cudaGetLastError();
+    }
     scan_tiles_kernel<T><<<1, 1024, 0, st>>>(tile_sums, nt, grand_total);
-    scan_apply_kernel<T><<<(unsigned)nt, kScanThreads, 0, st>>>(in, out, n, tile_sums);
+    scan_apply_kernel<T, false><<<(unsigned)nt, kScanThreads, 0, st>>>(in, out, n, tile_sums, nullptr);
     note_launches(3);
     return cudaGetLastError();
 }

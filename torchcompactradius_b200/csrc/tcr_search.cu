@@ -688,8 +688,7 @@ struct CellOut {
     int32_t* cell_cloud;
     unsigned long long* map;
     int32_t n_points;
-    __device__ void operator()(int64_t i, int32_t ex, int32_t flag) const {
-        if (!flag || !TCR_IN(ex, n_points)) return;
+    __device__ void write(int64_t i, int32_t ex) const {
         const K* k = st->sel[key_passes<K>()] ? keys1 : keys0;
         const K key = k[i];
         const int cloud = key_cloud(key);
@@ -712,6 +711,26 @@ struct CellOut {
         cell_bucket[ex] = (int32_t)bucket;
     }
 };
+
+// The run-start scan writes only where each cell begins; the cell records are then written by one
+// thread per cell (a run start is one element in 16 here, so doing that work inside the scan left
+// most lanes of every warp idle behind a long chain of dependent loads and the map insert).
+struct CellStartOut {
+    int32_t* cell_start;
+    int32_t n_points;
+    __device__ void operator()(int64_t i, int32_t ex, int32_t flag) const {
+        if (flag && TCR_IN(ex, n_points)) cell_start[ex] = (int32_t)i;
+    }
+};
+template <typename K>
+__global__ void cell_records_kernel(CellOut<K> co, const int32_t* __restrict__ num_cells, int64_t n) {
+    const int32_t nc = *num_cells;
+    if (blockIdx.x == 0 && threadIdx.x == 0) co.cell_start[nc] = (int32_t)n;  // end of the last cell
+    for (int32_t c = blockIdx.x * blockDim.x + threadIdx.x; c < nc; c += gridDim.x * blockDim.x) {
+        const int32_t i = co.cell_start[c];
+        if (TCR_GUARD(i, n)) co.write(i, c);
+    }
+}
 
 // lin_out (optional): the linear cell of each sorted point, the hint of the next incremental build;
 // order_out (optional): a copy of the sort index.
@@ -1242,7 +1261,7 @@ struct WalkSmem {
     int32_t run_beg[kWalkWarps][32];
     int32_t run_pre[kWalkWarps][33];
     float shift[kWalkWarps][3][32];  // per run: +-ext on the dimensions its cells lie across a seam
-    float4 ring[kWalkWarps][3][32];  // candidate chunks in flight (cp.async), one slot per lane
+    float4 ring[kWalkWarps][4][32];  // candidate chunks in flight (cp.async), one slot per lane
     UnitCtx u[kWalkWarps];
 };
 
@@ -1408,6 +1427,57 @@ __device__ __forceinline__ uint32_t chunk_hits_x2(const float4* __restrict__ qp,
     return hit;
 }
 
+// chunk_hits_x2 for the lane's candidates of two chunks at once: each query pair is read once for
+// both, and the two candidates' chains of operations are independent, so they overlap.
+template <int DIM, int MODE>
+__device__ __forceinline__ void chunk_hits_x2_two(const float4* __restrict__ qp, int K4, const float4& cv0,
+                                                  float cw0, const float4& cv1, float cw1, float& umin0,
+                                                  float& umin1, uint32_t& hit0, uint32_t& hit1) {
+    const float2 ax = make_float2(-cv0.x, -cv0.x), ay = make_float2(-cv0.y, -cv0.y), az = make_float2(-cv0.z, -cv0.z);
+    const float2 bx = make_float2(-cv1.x, -cv1.x), by = make_float2(-cv1.y, -cv1.y), bz = make_float2(-cv1.z, -cv1.z);
+    const float2 an = make_float2(-cv0.w, -cv0.w), ap = make_float2(cv0.w, cv0.w);
+    const float2 bn = make_float2(-cv1.w, -cv1.w), bp = make_float2(cv1.w, cv1.w);
+    uint32_t h0 = 0, h1 = 0;
+    for (int p = (K4 >> 1) - 1; p >= 0; --p) {
+        const float4 a = qp[2 * p];
+        const float4 b = qp[2 * p + 1];
+        const float2 qx = make_float2(a.x, a.y), qy = make_float2(a.z, a.w), qz = make_float2(b.x, b.y);
+        const float2 dx0 = __fadd2_rn(qx, ax), dx1 = __fadd2_rn(qx, bx);
+        float2 e0 = __fmul2_rn(dx0, dx0), e1 = __fmul2_rn(dx1, dx1);
+        if (DIM > 1) {
+            const float2 dy0 = __fadd2_rn(qy, ay), dy1 = __fadd2_rn(qy, by);
+            e0 = __ffma2_rn(dy0, dy0, e0);
+            e1 = __ffma2_rn(dy1, dy1, e1);
+        }
+        if (DIM > 2) {
+            const float2 dz0 = __fadd2_rn(qz, az), dz1 = __fadd2_rn(qz, bz);
+            e0 = __ffma2_rn(dz0, dz0, e0);
+            e1 = __ffma2_rn(dz1, dz1, e1);
+        }
+        float2 r0, r1;  // residuals of the query pair against each candidate
+        if (MODE == kGather) {
+            const float2 s = make_float2(b.z, b.w);
+            r0 = __fadd2_rn(e0, s);
+            r1 = __fadd2_rn(e1, s);
+        } else if (MODE == kScatter) {
+            r0 = __ffma2_rn(an, ap, e0);
+            r1 = __ffma2_rn(bn, bp, e1);
+        } else {
+            const float t00 = b.z + cw0, t01 = b.w + cw0, t10 = b.z + cw1, t11 = b.w + cw1;
+            r0 = make_float2(fmaf(-t00, t00, e0.x), fmaf(-t01, t01, e0.y));
+            r1 = make_float2(fmaf(-t10, t10, e1.x), fmaf(-t11, t11, e1.y));
+        }
+        h0 = __funnelshift_l(__float_as_uint(r0.y), h0, 1);
+        h0 = __funnelshift_l(__float_as_uint(r0.x), h0, 1);
+        h1 = __funnelshift_l(__float_as_uint(r1.y), h1, 1);
+        h1 = __funnelshift_l(__float_as_uint(r1.x), h1, 1);
+        umin0 = fminf(umin0, fminf(fabsf(r0.x), fabsf(r0.y)));
+        umin1 = fminf(umin1, fminf(fabsf(r1.x), fabsf(r1.y)));
+    }
+    hit0 = h0;
+    hit1 = h1;
+}
+
 // The same with every pair inside the band decided by the reference's exact test, on the original
 // (unshifted) candidate of sorted index j -- in double on the double arrays for float64 inputs;
 // rare units only, so out of line.
@@ -1555,13 +1625,14 @@ __device__ __forceinline__ void count_unit(const WalkArgs& a, WalkSmem& sm, int3
     const int K4 = (nb + 3) & ~3;
     const float4* qsm = sm.q[w];
     uint32_t count = 0;
-    // The fast pass streams candidate chunks into a three-slot ring in shared memory by cp.async,
-    // two chunks ahead of their use, so the loads' latency hides behind two chunks of tests
-    // without holding registers.  Lanes past the unit's candidates get NaN (never a hit).
+    // The fast pass takes the chunks two at a time (each lane tests its candidate of both against
+    // every query, reading each query pair once) and streams them into a four-slot ring in shared
+    // memory by cp.async, a pair of chunks ahead of its use, so the loads' latency hides behind the
+    // tests without holding registers.  Lanes past the unit's candidates get NaN (never a hit).
     float4* ring = &sm.ring[w][0][0];
-    auto issue = [&](int32_t c, int slot) {
+    auto issue = [&](int32_t c) {
         const int32_t k = (c << 5) + lane;
-        float4* dst = ring + slot * 32 + lane;
+        float4* dst = ring + (c & 3) * 32 + lane;
         bool copied = false;
         if (k < M) {
             while (rpre[cr + 1] <= k) ++cr;
@@ -1575,61 +1646,77 @@ __device__ __forceinline__ void count_unit(const WalkArgs& a, WalkSmem& sm, int3
         cp_async_commit();
         return cr;
     };
-    int32_t cra = issue(0, 0);  // runs of the candidates of chunks c and c + 1 (seam shifts)
-    int32_t crb = issue(1, 1);
-    int slot = 0;
-    for (int32_t c = 0; c < nchunks; ++c) {
-        const int32_t crc = issue(c + 2, slot == 0 ? 2 : slot - 1);
-        cp_async_wait<2>();  // chunk c has landed
-        float4 cv = ring[slot * 32 + lane];
-        const int32_t crn = cra;  // run of this chunk's candidate
-        if (PERIODIC && shift_mode) {  // the fast test takes seam candidates shifted
+    // one landed chunk: the candidate (shifted across a seam for the fast test) and its bands
+    auto take = [&](int32_t c, int32_t crn, float4& cv, float& cw, float& band, float& band_exact) {
+        cv = ring[(c & 3) * 32 + lane];
+        if (PERIODIC && shift_mode) {
             cv.x += sm.shift[w][0][crn];
             if (DIM > 1) cv.y += sm.shift[w][1][crn];
             if (DIM > 2) cv.z += sm.shift[w][2][crn];
         }
-        cra = crb;
-        crb = crc;
-        slot = slot == 2 ? 0 : slot + 1;
-        const float cw = cand_share<MODE>(cv.w);
+        cw = cand_share<MODE>(cv.w);
         const float t = cand_tmax<MODE>(cw, qmax);
-        float band = exact_all ? inf : kBandEps * t * t;
+        band = exact_all ? inf : kBandEps * t * t;
         // float64 inputs: the band also covers the rounding of the coordinates to float32
         if (fe > 0.0f) band += fmaf(2.0f * 1.7320508f * t, fe, 3.0f * fe * fe);
-        const float band_exact = band;
+        band_exact = band;
         // shifted candidates: the band also covers the shift's rounding (|d2 error| <= 2 T delta + delta^2)
         if (seam) band += fmaf(2.0f * t, dl, dl * dl);
-        uint32_t hit;
-        bool inband = false;  // some pair of this lane's candidate lies within the band
-        if (MODE != kSuperSymmetric && (!PERIODIC || shift_mode)) {
-            float umin = inf;
-            hit = chunk_hits_x2<DIM, MODE>(sm.qp[w], K4, cv, cw, umin);
-            inband = umin <= band;
-        } else if (shift_mode) {
-            hit = chunk_hits<DIM, false, MODE>(wc, qsm, K4, cv, cw, band, inband);
-        } else {
-            hit = chunk_hits<DIM, PERIODIC, MODE>(wc, qsm, K4, cv, cw, band, inband);
+    };
+    // some pair of a chunk lies within the band: the chunk again, every pair in the band decided by
+    // the reference's exact test on the original (unshifted) candidates
+    auto exact = [&](int32_t c, int32_t crn, float band_exact) {
+        if (lane == 0) atomicAdd(a.num_exact, 1);
+        const int32_t k = (c << 5) + lane;
+        float4 v0 = nan4;
+        int32_t j = 0;
+        if (k < M) {
+            j = rbeg[crn] + (k - rpre[crn]);
+            if (TCR_GUARD(j, a.nr_total)) v0 = __ldg(&rs[j]);
         }
-        if (__any_sync(0xffffffffu, inband)) {
-            // some pair of the chunk lies within the band: the chunk again, every pair in the band
-            // decided by the reference's exact test on the original (unshifted) candidates
-            if (lane == 0) atomicAdd(a.num_exact, 1);
-            const int32_t k = (c << 5) + lane;
-            float4 v0 = nan4;
-            int32_t j = 0;
-            if (k < M) {
-                j = rbeg[crn] + (k - rpre[crn]);
-                if (TCR_GUARD(j, a.nr_total)) v0 = __ldg(&rs[j]);
-            }
-            hit = chunk_hits_exact<DIM, MODE>(unit_exact_ctx(u, MODE), qsm, sm.qh[w], sm.qid[w], K4, v0, j,
-                                              band_exact, a.f64);
-        }
-        const uint32_t m = warp_transpose32(hit, lane);
+        return chunk_hits_exact<DIM, MODE>(unit_exact_ctx(u, MODE), qsm, sm.qh[w], sm.qid[w], K4, v0, j, band_exact,
+                                           a.f64);
+    };
+    auto store = [&](int32_t c, uint32_t m) {
         if (lane < nb) {
             count += __popc(m);
             if (stage && TCR_IN((int64_t)(msk - reinterpret_cast<uint32_t*>(a.stage)) + c * nb + lane, a.stage_cap))
                 msk[c * nb + lane] = m;
         }
+    };
+    int32_t cr0 = issue(0);  // runs of the candidates of chunks c and c + 1 (seam shifts)
+    int32_t cr1 = issue(1);
+    for (int32_t c = 0; c < nchunks; c += 2) {
+        const int32_t cr2 = issue(c + 2), cr3 = issue(c + 3);
+        cp_async_wait<2>();  // chunks c and c + 1 have landed
+        const bool two = c + 1 < nchunks;  // (past the last chunk the ring holds NaN: no hits)
+        float4 cv0, cv1;
+        float cw0, cw1, band0, band1, bx0, bx1;
+        take(c, cr0, cv0, cw0, band0, bx0);
+        take(c + 1, cr1, cv1, cw1, band1, bx1);
+        uint32_t hit0, hit1 = 0;
+        bool in0 = false, in1 = false;  // some pair of this lane's candidate lies within the band
+        if (MODE != kSuperSymmetric && (!PERIODIC || shift_mode)) {
+            float umin0 = inf, umin1 = inf;
+            chunk_hits_x2_two<DIM, MODE>(sm.qp[w], K4, cv0, cw0, cv1, cw1, umin0, umin1, hit0, hit1);
+            in0 = umin0 <= band0;
+            in1 = umin1 <= band1;
+        } else if (shift_mode) {
+            hit0 = chunk_hits<DIM, false, MODE>(wc, qsm, K4, cv0, cw0, band0, in0);
+            if (two) hit1 = chunk_hits<DIM, false, MODE>(wc, qsm, K4, cv1, cw1, band1, in1);
+        } else {
+            hit0 = chunk_hits<DIM, PERIODIC, MODE>(wc, qsm, K4, cv0, cw0, band0, in0);
+            if (two) hit1 = chunk_hits<DIM, PERIODIC, MODE>(wc, qsm, K4, cv1, cw1, band1, in1);
+        }
+        if (__any_sync(0xffffffffu, in0)) hit0 = exact(c, cr0, bx0);
+        if (two && __any_sync(0xffffffffu, in1)) hit1 = exact(c + 1, cr1, bx1);
+        // the two transposes are independent, so their shuffle chains overlap
+        const uint32_t m0 = warp_transpose32(hit0, lane);
+        const uint32_t m1 = warp_transpose32(hit1, lane);
+        store(c, m0);
+        if (two) store(c + 1, m1);
+        cr0 = cr2;
+        cr1 = cr3;
     }
     if (active) a.counts[qorig] = (int32_t)count;
     if (lane == 0 && !stage && TCR_IN(unit, a.nq_total)) {
@@ -2039,6 +2126,16 @@ __global__ void __launch_bounds__(kExpandWarps * 32, 4) expand_records_kernel(Ex
                     for (int32_t o = lane; o < n; o += 32) {
                         const uint32_t v = tab[o];
                         __stcs(sm.qcol[w][v >> 9] + o, (long long)cols[v & 0x1ffu]);
+                    }
+                } else if (fits) {  // COO: the row of an output sits at the same slot of row_out
+                    const int64_t rd = ((intptr_t)a.row_out - (intptr_t)a.col_out) / 8;  // both int64-aligned
+#pragma unroll 4
+                    for (int32_t o = lane; o < n; o += 32) {
+                        const uint32_t v = tab[o];
+                        const uint32_t vq = v >> 9;
+                        long long* p = sm.qcol[w][vq] + o;
+                        __stcs(p, (long long)cols[v & 0x1ffu]);
+                        __stcs(p + rd, (long long)sm.qrow[w][vq]);
                     }
                 } else {
 #pragma unroll 4
@@ -2567,13 +2664,13 @@ static int build_impl(const HostBatch& b, const Structure& S, const Scratch& W, 
     note_launches(1);
     // computeGridSupport: which supports set hMax depends on the mode
     if (b.any_ref_sup && nr > 0) {
-        support_stats_kernel<<<grid_for(nr, 256, num_sms() * 8), 256, 0, st>>>(
+        support_stats_kernel<<<grid_for(nr, 256, num_sms() * 4), 256, 0, st>>>(
             W.table, W.ref_prefix, C, nr, 0, reinterpret_cast<char*>(S.grid) + offsetof(GridParams, ref_stats),
             (int64_t)sizeof(GridParams));
         note_launches(1);
     }
     if (b.any_query_sup && nq > 0 && !b.same_sorted) {
-        support_stats_kernel<<<grid_for(nq, 256, num_sms() * 8), 256, 0, st>>>(
+        support_stats_kernel<<<grid_for(nq, 256, num_sms() * 4), 256, 0, st>>>(
             W.table, W.query_prefix, C, nq, 1,
             reinterpret_cast<char*>(S.grid) + offsetof(GridParams, build_query_stats), (int64_t)sizeof(GridParams));
         note_launches(1);
@@ -2613,12 +2710,15 @@ static int build_impl(const HostBatch& b, const Structure& S, const Scratch& W, 
                                                                    S.rsorted, S.rsidx, sw.keys[0], sw.keys[1],
                                                                    b.lin_out, b.order_out);
         note_launches(1);
+        RunFlagIn<K> fi{sw.keys[0], sw.keys[1], sw.state};
+        TCR_CUDA(device_exclusive_scan<int32_t>(fi, CellStartOut{S.cell_start, (int32_t)nr}, nr, W.scan_tiles32,
+                                                S.num_cells, st));
         CellOut<K> co{W.table, S.grid, sw.keys[0], sw.keys[1], sw.state, S.rsorted, S.cell_start, S.cell_lin,
                       S.cell_coords, S.cell_bucket, S.cell_cloud, S.map, (int32_t)nr};
-        RunFlagIn<K> fi{sw.keys[0], sw.keys[1], sw.state};
-        TCR_CUDA(device_exclusive_scan<int32_t>(fi, co, nr, W.scan_tiles32, S.num_cells, st));
+        cell_records_kernel<K><<<grid_for(nr, 256, num_sms() * 8), 256, 0, st>>>(co, S.num_cells, nr);
+    } else {
+        finish_cells_kernel<<<1, 1, 0, st>>>(S.cell_start, S.num_cells, nr);
     }
-    finish_cells_kernel<<<1, 1, 0, st>>>(S.cell_start, S.num_cells, nr);
     note_launches(1);
     TCR_CUDA(cudaGetLastError());
     return TCR_OK;
@@ -2636,7 +2736,7 @@ static int count_impl(const HostBatch& b, const Structure& S, const Scratch& W, 
     count_init_kernel<<<grid_for(std::max<int64_t>(C, nq), 256), 256, 0, st>>>(W, C, unit_cap, nq);
     note_launches(1);
     if (b.any_query_sup && nq > 0 && !b.same_sorted) {
-        support_stats_kernel<<<grid_for(nq, 256, num_sms() * 8), 256, 0, st>>>(
+        support_stats_kernel<<<grid_for(nq, 256, num_sms() * 4), 256, 0, st>>>(
             W.table, W.query_prefix, C, nq, 1, reinterpret_cast<char*>(W.qparams) + offsetof(QueryParams, stats),
             (int64_t)sizeof(QueryParams));
         note_launches(1);
