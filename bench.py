@@ -434,7 +434,8 @@ def make_served_workload(seed=5, n_scenes=64, rate=2000.0, seconds=1.0):
     return scenes, arrivals
 
 
-HBM_BUDGET = 120e9  # the served form's admission budget: two thirds of a B200's 180 GB
+HBM_BUDGET = 40e9  # the served form's admission budget: about three groups of all 64 scenes in flight;
+# larger budgets let the torch allocator's cache fill the 180 GB and stall on a free-and-retry
 
 
 def bench_served(dev, seconds=1.0, slots=2):
@@ -452,6 +453,8 @@ def bench_served(dev, seconds=1.0, slots=2):
 
     scenes, arrivals = make_served_workload(seconds=seconds)
     dom = tcr.DomainDescription(torch.full((3,), -1.0), torch.full((3,), 1.0), torch.tensor([True] * 3), 3)
+    torch.cuda.synchronize()
+    torch.cuda.empty_cache()  # both forms start from an empty allocator cache
 
     def pct(v, q):
         v = sorted(v)
@@ -510,6 +513,8 @@ def bench_served(dev, seconds=1.0, slots=2):
 
     # ---- per call (the same engine tuning as the server) ---------------------------------
     from torchcompactradius_b200 import context
+    torch.cuda.synchronize()
+    torch.cuda.empty_cache()
     pos = [x.to(dev) for x, h in scenes]
     sup = [torch.full((x.shape[0],), h, device=dev) for x, h in scenes]
     with context.use(context.SearchContext(unit_queries=tuned[0], walk_blocks_per_sm=tuned[1])):

@@ -1229,13 +1229,15 @@ __device__ __forceinline__ void lean_test(const WrapCtx& wc, const float4& q, co
 
 constexpr int kWalkWarps = 4;
 // Resident blocks per SM the count walk is compiled for (registers <= 65536 / (128 * blocks)):
-// five (96 registers, no spills) on non-periodic clouds, four on periodic ones, whose wrap tests
-// need more registers.
+// eight (64 registers) on non-periodic clouds and seven (72) on periodic ones.  More resident
+// warps beat the spills they cost: on the 1M workload 8/7/6/5/4 blocks measured
+// 0.348/0.355/0.363/0.372/0.385 ms non-periodic, 8/7/6/5/4 blocks 0.414/0.403/0.426/0.436/0.467 ms
+// periodic.
 #ifndef TCR_WALK_MIN_BLOCKS
-#define TCR_WALK_MIN_BLOCKS 5
+#define TCR_WALK_MIN_BLOCKS 8
 #endif
 #ifndef TCR_WALK_MIN_BLOCKS_PERIODIC
-#define TCR_WALK_MIN_BLOCKS_PERIODIC 4
+#define TCR_WALK_MIN_BLOCKS_PERIODIC 7
 #endif
 constexpr int kWalkMinBlocks = TCR_WALK_MIN_BLOCKS;
 constexpr int kWalkMinBlocksPeriodic = TCR_WALK_MIN_BLOCKS_PERIODIC;
