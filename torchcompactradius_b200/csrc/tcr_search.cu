@@ -734,12 +734,35 @@ __global__ void cell_records_kernel(CellOut<K> co, const int32_t* __restrict__ n
 
 // lin_out (optional): the linear cell of each sorted point, the hint of the next incremental build;
 // order_out (optional): a copy of the sort index.
+// The build's consumer of its sort: the sorted points, their input indices and (for the serving
+// loop) each point's linear cell and input index, written as the sort's last pass places them.
+template <typename K>
+struct SortedPointsOut {
+    static constexpr bool kActive = true;
+    const float4* __restrict__ pack;
+    float4* __restrict__ sorted;
+    int32_t* __restrict__ sidx;
+    int32_t* __restrict__ lin_out;
+    int32_t* __restrict__ order_out;
+    int64_t n;
+    __device__ __forceinline__ void operator()(int64_t i, K key, int32_t p) const {
+        if (!TCR_IN(p, n)) return;
+        sorted[i] = pack[p];
+        sidx[i] = p;
+        if (lin_out) lin_out[i] = (int32_t)(key_low(key) ^ 0x80000000u);
+        if (order_out) order_out[i] = p;
+    }
+};
+
+// The same placement when the sort's last pass did not do it (no pass moved the points, or an
+// incremental build's merge ordered them).
 template <typename K>
 __global__ void gather_sorted_kernel(const float4* __restrict__ pack, const int32_t* vals0, const int32_t* vals1,
                                      const SortStateT<K>* st, int64_t n, float4* __restrict__ sorted,
                                      int32_t* __restrict__ sidx, const K* keys0 = nullptr, const K* keys1 = nullptr,
                                      int32_t* __restrict__ lin_out = nullptr,
                                      int32_t* __restrict__ order_out = nullptr) {
+    if (st->consumed) return;
     const int32_t* v = st->sel[key_passes<K>()] ? vals1 : vals0;
     const K* k = st->sel[key_passes<K>()] ? keys1 : keys0;
     const int64_t stride = (int64_t)gridDim.x * blockDim.x;
@@ -2707,7 +2730,7 @@ static int build_impl(const HostBatch& b, const Structure& S, const Scratch& W, 
                 mw.state, W.inc_count, nr, sw.keys[0], sw.vals[0]);
             note_launches(1);
         }
-        TCR_CUDA(radix_sort_pairs<K>(sw, nr, st));
+        TCR_CUDA(radix_sort_pairs<K>(sw, nr, st, SortedPointsOut<K>{W.pack, S.rsorted, S.rsidx, b.lin_out, b.order_out, nr}));
         gather_sorted_kernel<K><<<grid_for(nr, 256), 256, 0, st>>>(W.pack, sw.vals[0], sw.vals[1], sw.state, nr,
                                                                    S.rsorted, S.rsidx, sw.keys[0], sw.keys[1],
                                                                    b.lin_out, b.order_out);

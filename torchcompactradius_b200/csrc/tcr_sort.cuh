@@ -28,6 +28,7 @@ struct SortStateT {
     int32_t pad;
     int64_t n_dev;        // >= 0: sort only the first n_dev keys (a count known on the device only)
     uint32_t seen[8][8];  // per pass: bitmap of the digit values the histogram met
+    int32_t consumed;     // the last pass handed the sorted pairs to the caller's consumer
 };
 using SortState32 = SortStateT<uint32_t>;
 using SortState64 = SortStateT<unsigned long long>;
@@ -45,6 +46,7 @@ __device__ __forceinline__ void sort_state_reset(SortStateT<K>* st) {
     st->key_max = 0;
     st->sel[0] = 0;
     st->n_dev = -1;
+    st->consumed = 0;
     for (int p = 0; p < 8; ++p)
         for (int i = 0; i < 8; ++i) st->seen[p][i] = 0u;
 }
@@ -96,17 +98,27 @@ __global__ void __launch_bounds__(kSortThreads) radix_hist_kernel(const K* keys0
     }
 }
 
+// A consumer of the sorted pairs that takes nothing: every pass writes keys and values.
+struct NoSortConsumer {
+    static constexpr bool kActive = false;
+    template <typename K>
+    __device__ void operator()(int64_t, K, int32_t) const {}
+};
+
 // Stable scatter of one tile.  Warp w owns keys [w*R*32, (w+1)*R*32) of the tile (R = kSortItems),
 // processed in R rounds of 32 consecutive keys, so (warp, round, lane) order is the input order.  The tile is
 // first ordered by digit in shared memory (stable), then written out by consecutive threads over
 // that order: the keys of one digit land in consecutive output slots, so the stores coalesce into
 // runs instead of one sector per key.
-template <typename K>
+// With an active consumer, a pass above which no digit differs (the last one that can move keys)
+// hands the consumer each (slot, key, value) instead of writing the value -- the keys are still
+// written -- and sets st->consumed.
+template <typename K, typename Consumer>
 __global__ void __launch_bounds__(kSortThreads) radix_scatter_kernel(K* keys0, K* keys1, int32_t* vals0,
                                                                      int32_t* vals1, int64_t n, int shift, int pass,
                                                                      int64_t ntiles, SortStateT<K>* st,
                                                                      const int32_t* hist_scanned,
-                                                                     const int32_t* digit_total) {
+                                                                     const int32_t* digit_total, Consumer consume) {
     const int s = st->sel[pass];
     if (!pass_runs(st, shift, pass)) {
         if (blockIdx.x == 0 && threadIdx.x == 0) st->sel[pass + 1] = s;
@@ -196,14 +208,21 @@ __global__ void __launch_bounds__(kSortThreads) radix_scatter_kernel(K* keys0, K
     }
     __syncthreads();
     const int tn = digit_start[kBins];
+    const bool last = Consumer::kActive && !pass_needed(st, shift + 8);
     for (int i = threadIdx.x; i < tn; i += kSortThreads) {
         const K k = sk[i];
         const int dig = (int)((k >> shift) & 0xff);
         const int64_t pos = (int64_t)tile_base[dig] + (i - digit_start[dig]);
         kout[pos] = k;
-        vout[pos] = sv[i];
+        if (last)
+            consume(pos, k, sv[i]);
+        else
+            vout[pos] = sv[i];
     }
-    if (blockIdx.x == 0 && threadIdx.x == 0) st->sel[pass + 1] = s ^ 1;
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        st->sel[pass + 1] = s ^ 1;
+        if (last) st->consumed = 1;
+    }
 }
 
 // Per digit (one block each): exclusive scan of the digit's tile counts in place, and the
@@ -250,9 +269,11 @@ inline int64_t sort_hist_elems(int64_t n) { return (int64_t)kBins * sort_tiles(n
 
 // Sorts keys[sel0]/vals[sel0] (sel0 = state->sel[0], set by the producer, which also reduced the
 // key range and cleared the digit bitmaps), n keys or state->n_dev when that is set and smaller.  The result lives in buffer state->sel[key_passes<K>()]
-// after the call; consumers read the selector on the device.
-template <typename K>
-inline cudaError_t radix_sort_pairs(const SortWorkspaceT<K>& w, int64_t n, cudaStream_t st) {
+// after the call; consumers read the selector on the device.  An active `consume` takes the pairs
+// from the last pass that moves keys instead of the value buffer (st->consumed then reads 1).
+template <typename K, typename Consumer = NoSortConsumer>
+inline cudaError_t radix_sort_pairs(const SortWorkspaceT<K>& w, int64_t n, cudaStream_t st,
+                                    Consumer consume = Consumer()) {
     if (n <= 0) return cudaSuccess;
     const int64_t nt = sort_tiles(n);
     for (int p = 0; p < key_passes<K>(); ++p) {
@@ -260,8 +281,8 @@ inline cudaError_t radix_sort_pairs(const SortWorkspaceT<K>& w, int64_t n, cudaS
         radix_hist_kernel<K><<<(unsigned)nt, kSortThreads, 0, st>>>(w.keys[0], w.keys[1], n, shift, p, nt, w.state,
                                                                     w.hist);
         hist_scan_digits<K><<<kBins, kScanThreads, 0, st>>>(w.hist, nt, w.tile_sums, w.state, shift, p);
-        radix_scatter_kernel<K><<<(unsigned)nt, kSortThreads, 0, st>>>(w.keys[0], w.keys[1], w.vals[0], w.vals[1], n,
-                                                                      shift, p, nt, w.state, w.hist, w.tile_sums);
+        radix_scatter_kernel<K, Consumer><<<(unsigned)nt, kSortThreads, 0, st>>>(
+            w.keys[0], w.keys[1], w.vals[0], w.vals[1], n, shift, p, nt, w.state, w.hist, w.tile_sums, consume);
         note_launches(3);
     }
     return cudaGetLastError();
