@@ -23,6 +23,7 @@ the neighbour list against its HBM roofline.
 """
 import argparse
 import json
+import math
 import os
 import re
 import statistics
@@ -142,6 +143,38 @@ def measured_peak():
             return float(json.load(f)["hbm_gbs"]), "measured"
     except Exception:
         return 6650.0, "fallback"
+
+
+def candidate_tests(pos, sup):
+    """(query, candidate) pairs the count walk tests on the 1M workload: every query against every
+    point of its cell's 3^3 stencil, on the reference's grid (compute_h of util.py:28-79 over the
+    domain [-1, 1]^3 and the largest support); computed with torch on the points' device."""
+    import torch
+    ext, hmax = 2.0, float(sup.max())
+    n = int(ext / hmax)
+    if ext / hmax - n > 0:
+        n -= 1
+    n = max(n, 1)
+    h = ext / n
+    if math.ceil(ext / h) > ext / h:
+        h *= 1 + 1e-4
+    cnt = int(math.ceil(ext / h))
+    c = torch.clamp(torch.floor((pos + 1.0) / h).long(), 0, cnt - 1)
+    occ = torch.bincount((c[:, 0] * cnt + c[:, 1]) * cnt + c[:, 2], minlength=cnt ** 3).view(1, 1, cnt, cnt, cnt)
+    stencil = torch.nn.functional.conv3d(occ.double(), torch.ones(1, 1, 3, 3, 3, dtype=torch.float64, device=occ.device),
+                                         padding=1)
+    return int((occ.double() * stencil).sum())
+
+
+def ncu_issue_active():
+    """smsp__issue_active (percent of peak) of the count walk from the committed ncu summary."""
+    p = os.path.join(REPO, "profiles", "walk_count_3d_1m.txt")
+    try:
+        with open(p) as f:
+            m = re.search(r"smsp__issue_active\.avg\.pct_of_peak_sustained_active\s+([0-9.]+)", f.read())
+        return float(m.group(1)) / 100 if m else None
+    except OSError:
+        return None
 
 
 def ncu_traffic():
@@ -1041,6 +1074,7 @@ def run_b200(args):
     search_bytes = 16 * N_POINTS + 8 * pairs + 4 * (N_POINTS + 1) + 8 * N_POINTS
     search_s = statistics.mean(step_ms) / 1e3
     traffic = ncu_traffic()
+    tests = candidate_tests(pos_d, sup_d)
     line = {
         "metric": METRIC, "value": value, "unit": "pairs/s", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True, "scaling": "weak",
@@ -1056,7 +1090,9 @@ def run_b200(args):
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                      "traffic": traffic, "kernel": "walk_count_kernel<3,false,symmetric> (every pair test)",
                      "algorithmic_bytes_per_launch": walk_bytes, "launch_ms": statistics.mean(walk_ms),
-                     "pair_tests_note": "bound by candidate tests, not HBM: see candidate_tests_per_s",
+                     "pair_tests_note": "bound by candidate tests (instruction issue), not HBM",
+                     "candidate_tests_per_launch": tests, "candidate_tests_per_s": tests / walk_s,
+                     "issue_active_frac_ncu": ncu_issue_active(),
                      "peak_kind": peak_kind},
         "search_roofline": {"bound": "hbm", "algorithmic_bytes_per_search": search_bytes,
                             "achieved": search_bytes / search_s / 1e9, "peak": peak, "unit": "GB/s",

@@ -428,7 +428,8 @@ __global__ void __launch_bounds__(kThreads) mark_runs_kernel(const KT* k0, const
             int64_t prev = base == 0 ? -1 : key_slot(pk, nslots);
 #pragma unroll
             for (int k = 0; k < kMarkKeys; ++k) {
-                if (k < nk) {
+                // a key equal to the one before it starts no run (same slot): one compare
+                if (k < nk && (v[k] != (k == 0 ? pk : v[k - 1]) || (k == 0 && base == 0))) {
                     const int64_t cur = key_slot(v[k], nslots);
                     mark_range(prev + 1 < 0 ? 0 : prev + 1, cur, base + k, off, gaps, ngaps, gap_cap, dsc);
                     prev = cur;
