@@ -30,7 +30,7 @@ def _rank_main(rank, world, port, out):
 
 def test_two_rank_value_uses_the_slowest_rank():
     port = 29500 + (os.getpid() % 1000)
-    with mp.Manager() as m:
+    with mp.get_context("spawn").Manager() as m:  # no fork of a process that runs threads
         out = m.dict()
         mp.spawn(_rank_main, args=(2, port, out), nprocs=2, join=True)
         res = dict(out)
