@@ -8,7 +8,7 @@ from typing import Optional, Tuple, Union
 
 import torch
 
-from .search import CompactHashMap, _as_f32, _domain_host, _require_cuda, compact_search
+from .search import CompactHashMap, _as_f32, _domain_host, _require_cuda, _to_host, compact_search
 from .util import DomainDescription, PointCloud, SparseCOO, SparseCSR
 
 ALGORITHMS = ("naive", "small", "compact", "cluster", "mlm")
@@ -79,7 +79,8 @@ def radiusSearch(queryPointCloud: PointCloud, referencePointCloud: Optional[Poin
             out, ds = _radius_search_f64(queryPointCloud, referencePointCloud, supportOverride, mode, domain, lo, hi,
                                          mask, hashMapLength, format, self_cloud, returnStructure, device)
             if in_device.type != "cuda":
-                out = tuple(None if t is None else t.to(in_device) for t in out)
+                out = _to_host(out) if in_device.type == "cpu" else tuple(
+                    None if t is None else t.to(in_device) for t in out)
             adj = SparseCOO(out[0], out[1], nq, nr) if format == "coo" else SparseCSR(out[0], out[1], out[2], nq, nr)
             return (adj, ds) if returnStructure else adj
         xq = _as_f32(qpos, device)
@@ -111,7 +112,8 @@ def radiusSearch(queryPointCloud: PointCloud, referencePointCloud: Optional[Poin
                                      return_structure=returnStructure, ref_pos_user=rpos,
                                      ref_sup_user=referencePointCloud.supports, fixed_support=supportOverride)
         if in_device.type != "cuda":
-            out = tuple(None if t is None else t.to(in_device) for t in out)
+            out = _to_host(out) if in_device.type == "cpu" else tuple(
+                None if t is None else t.to(in_device) for t in out)
         if format == "coo":
             adj = SparseCOO(out[0], out[1], nq, nr)
         else:
@@ -194,7 +196,8 @@ def neighborSearchExisting(queryPointCloud: PointCloud, hashMap: CompactHashMap,
                                 hashMap.hashMapLength, format, False, structure=hashMap)
         nq, nr = qpos.shape[0], hashMap._n
         if qpos.device.type != "cuda":
-            out = tuple(None if t is None else t.to(qpos.device) for t in out)
+            out = _to_host(out) if qpos.device.type == "cpu" else tuple(
+                None if t is None else t.to(qpos.device) for t in out)
         if format == "coo":
             return SparseCOO(out[0], out[1], nq, nr)
         return SparseCSR(out[0], out[1], out[2], nq, nr)
@@ -220,7 +223,8 @@ def _existing_f64(q: PointCloud, hashMap: CompactHashMap, mode, fmt, dev):
                                 hashMap.hashMapLength, fmt, False, structure=hashMap)
     nq, nr = qpos.shape[0], hashMap._n
     if qpos.device.type != "cuda":
-        out = tuple(None if t is None else t.to(qpos.device) for t in out)
+        out = _to_host(out) if qpos.device.type == "cpu" else tuple(
+            None if t is None else t.to(qpos.device) for t in out)
     if fmt == "coo":
         return SparseCOO(out[0], out[1], nq, nr)
     return SparseCSR(out[0], out[1], out[2], nq, nr)
