@@ -20,7 +20,7 @@ import torch
 
 from . import _lib
 from . import context as _context
-from .search import _as_f32, _check_device_fault, _domain_host, _ptr, _require_cuda
+from .search import _as_f32, _check_device_fault, _domain_host, _ptr, _require_cuda, _to_host
 from .util import DomainDescription, PointCloud, SparseCOO, SparseCSR
 
 CLOUD_DTYPE = np.dtype([("dim", "<i4"), ("periodic_mask", "<i4"), ("domain_min", "<f4", (3,)),
@@ -413,7 +413,9 @@ def radius_batched(xq, xr, support, batch_x, batch_y, mode="gather", domain=None
     rids = qids if same_cloud else orr.to(torch.int32)
     out = run_batch(table, mode, same_cloud, "coo", device, local_index=False, query_ids=qids, ref_ids=rids)
     i, j = out["row"], out["col"]
-    if xq.device.type != "cuda":
+    if xq.device.type == "cpu":
+        i, j = _to_host((i, j))
+    elif xq.device.type != "cuda":
         i, j = i.to(xq.device), j.to(xq.device)
     return i, j
 
